@@ -1,0 +1,481 @@
+"""Benchmark: Katsevich helical cone-beam reconstruction of a 512x512x256 volume on B200.
+
+Workload (default, the plain FP32 B200 configuration): flat detector 64 rows x 736 columns
+at 0.8 mm, source radius 600 mm, source-detector 1200 mm, 1160 views/turn over 8 turns
+(9280 views), pitch 0.9x the Tam-Danielson window, 40 seeded random ellipsoids with Poisson
+noise at 1e5 photons/ray, 512x512x256 FP32 volume at 0.4 mm voxels. Synthetic data made on
+the device by the analytic FP64 projector (not timed).
+
+One step = the whole hot path over one scan: filter (derivative, forward height rebin,
+Hilbert, backward rebin) -> PI-line solve -> voxel-driven backprojection.
+
+Metric: GUPS = voxel-view updates per second, the update count being the reference's own
+loop count sum(LoopEnd - LoopBegin + 1) over written voxels (KatsevichBkProj.cpp:237),
+taken from the bisection PI solve and used for every variant. `value` is updates / step
+time of the device-resident chain (all ranks' updates / max-over-ranks time); `e2e` is the
+same through the MEX-equivalent host calls (FP64 host buffers, copies in the timed region).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--hilbert fp32|bf16x3|tf32] [--pi bisect|newton|learned]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from ctrecon_b200.geometry import config  # noqa: E402
+
+WORKLOAD_NAME = ("katsevich_helical_512x512x256_det64x736_9280views_"
+                 "40ellipsoids_poisson1e5")
+METRIC = "Katsevich 512^3 recon GUPS & s/vol: plain FP32 vs mixed+learned @ equal RMSE"
+BYTES_PER_UPDATE = 16  # four FP32 bilinear taps (KatsevichBkProj.cpp:253-256)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="c2")
+    ap.add_argument("--hilbert", default="fp32", choices=["fp32", "bf16x3", "tf32"])
+    ap.add_argument("--pi", default="bisect", choices=["bisect", "newton", "learned"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def load_traffic(kernel, workload):
+    """Per-launch DRAM bytes of `kernel` from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "traffic.txt")
+    try:
+        for line in open(path):
+            parts = line.split()
+            if len(parts) >= 3 and not line.startswith("#") and parts[0] == kernel and \
+                    parts[1] == workload:
+                return float(parts[2])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        if not self.proc:
+            return out
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sms, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sms.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.path)
+        if sms:
+            out = {"sm_mhz": statistics.median(sms), "sm_max_mhz": mx,
+                   "reasons": sorted(reasons), "samples": len(sms)}
+        return out
+
+
+def dist_setup(n):
+    import torch
+    import torch.distributed as dist
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    torch.cuda.set_device(local)
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, ws):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------------------------
+# CPU baselines (the oracle restatement, or the reference's own compiled backprojector)
+# ---------------------------------------------------------------------------------------------
+def _oracle():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    return oracle
+
+
+def block_problem(O, s, n=48):
+    """A central n^3 block of the volume at the workload's voxel pitch, posed as a geom the
+    reference's MEX accepts (it derives the pitch from ObjR as 2*ObjR/N), restricted to the
+    views [lo, hi) its PI intervals need (with a 2-view margin, so the loop bounds and
+    endpoint weights are those of the full scan)."""
+    dx = s.voxel_size[0]
+    obj = [dx * n / 2.0, float(n), float(n), float(n), dx, dx, dx]
+    g = O.bp_geom(s.locus(), s.detector(), obj, honour_extras=True)
+    pit = O.pi_table(g)
+    v = pit["valid"]
+    lo = max(0, int(np.floor(pit["B"][v].min())) - 3)
+    hi = min(s.P, int(np.ceil(pit["T"][v].max())) + 4)
+    locus = s.locus()
+    locus[4] = float(lo + 1)          # ProjBeginIndex (one-based)
+    locus[5] = float(hi)              # ProjEndIndex
+    return locus, s.detector(), obj, lo, hi
+
+
+def cpu_filter_views(O, s, proj_sub):
+    """FP64 filter restatement of a contiguous view range; the first and last view only
+    serve as derivative neighbours and are not valid outputs."""
+    fp = O.filter_params(ProjScale=float(s.views_per_turn), DecWidth=s.DecWidth,
+                         DecHeigh=s.DecHeigh, ScanR=s.ScanR, StdDis=s.StdDis, HelicP=s.HelicP,
+                         FilterCoeFF=s.filter_coeff, DeltaAngle=s.delta,
+                         FilteringMode=s.filtering_mode, YL=s.YL, ZL=s.ZL,
+                         ProjNumber=proj_sub.shape[0])
+    return O.katsevich_filter(fp, proj_sub)
+
+
+def cpu_bp_sample_port(O, s, fproj_views, lo, hi, nthreads, n=48):
+    locus, det, obj, lo2, hi2 = block_problem(O, s, n)
+    assert (lo2, hi2) == (lo, hi)
+    g = O.bp_geom(locus, det, obj, honour_extras=True)
+    img = np.zeros((n, n, n))
+    t = time.perf_counter()
+    _, nupd = O.bkproj(g, np.ascontiguousarray(fproj_views), img, nthreads=nthreads)
+    return time.perf_counter() - t, nupd
+
+
+def _ref_worker(args):
+    locus, det, obj, fproj_path = args
+    O = _oracle()
+    fproj = np.ascontiguousarray(np.load(fproj_path))
+    n = int(obj[1])
+    img = np.zeros((n, n, n))
+    geom = {"Locus": np.array(locus), "Detector": np.array(det), "Object": np.array(obj)}
+    t = time.perf_counter()
+    O.ref_bkproj(geom, fproj, img)
+    return time.perf_counter() - t
+
+
+# ---------------------------------------------------------------------------------------------
+def run_reference(args):
+    """The reference's CPU path, timed on the host cores: KatsevichBkProj.cpp compiled
+    unchanged (oracle/_ref; single-threaded code, run as one process per core on the same
+    central block) for the backprojection, and the FP64 restatement of KatsevichFiltering.m
+    (MATLAB is unavailable; OpenMP over views) for the filter. Each step is a bounded sample
+    scaled to one full scan by the exact update count and the view count."""
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    O = _oracle()
+    s = config(args.config)
+    cores = os.cpu_count() or 1
+    if not O.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref (KatsevichBkProj.cpp built from the CTRecon sources) "
+                          "is missing"}))
+        return
+    n = 48
+    locus, det, obj, lo, hi = block_problem(O, s, n)
+    # inputs: the same analytic phantom (FP64 oracle projector) on the views the block needs
+    gsub = O.bp_geom(locus, s.detector(), s.object())
+    proj = O.project_ellipsoids(gsub, s.ellipsoids())
+    fproj = cpu_filter_views(O, s, proj)
+    g = O.bp_geom(locus, det, obj, honour_extras=True)
+    _, block_updates = O.bkproj(g, fproj, np.zeros((n, n, n)))
+    full_updates = _full_update_count(s)
+    tmpdir = tempfile.mkdtemp()
+    fpath = os.path.join(tmpdir, "fproj.npy")
+    np.save(fpath, fproj)
+    import multiprocessing as mp
+    nproc = cores
+    per_step = []
+    with mp.get_context("spawn").Pool(nproc) as pool:
+        for it in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            pool.map(_ref_worker, [(locus, det, obj, fpath)] * nproc)
+            wall_bp = time.perf_counter() - t0
+            bp_rate = nproc * block_updates / wall_bp  # updates/s on all cores
+            nv = 8
+            t1 = time.perf_counter()
+            cpu_filter_views(O, s, proj[:nv + 2])
+            t_view = (time.perf_counter() - t1) / nv
+            t_scan = full_updates / bp_rate + t_view * s.P
+            if it >= args.warmup:
+                per_step.append(t_scan)
+    os.unlink(fpath)
+    os.rmdir(tmpdir)
+    t_scan = statistics.median(per_step)
+    gups = full_updates / t_scan / 1e9
+    sample = (f"per step: KatsevichBkProj.cpp (oracle/_ref) on a central {n}^3 block at the "
+              f"workload's voxel pitch ({block_updates} updates) in {nproc} processes, plus "
+              f"the FP64 filter restatement on 8 views with {cores} threads; scaled to the "
+              f"full scan ({full_updates} updates, {s.P} views)")
+    line = {"impl": "reference", "metric": METRIC, "value": gups, "unit": "GUPS",
+            "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t_scan * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD_NAME, "volume": list(s.vol_shape),
+                       "detector": [s.ZL, s.YL], "views": s.P},
+            "cpu_baseline": {"value": gups, "unit": "GUPS", "cores": cores,
+                             "kind": "reference", "sample": sample},
+            "e2e": {"value": gups, "unit": "GUPS", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+            "s_per_vol": t_scan}
+    print(json.dumps(line))
+
+
+def _full_update_count(s):
+    """sum(LoopEnd-LoopBegin+1) of the whole volume; on the GPU when there is one."""
+    try:
+        import torch
+        if torch.cuda.is_available():
+            import ctrecon_b200 as ct
+            c = ct.Context(torch.cuda.current_device())
+            d_tab = torch.empty(c.pi_table_bytes(s.geom_struct()), dtype=torch.uint8,
+                                device="cuda")
+            d_cnt = torch.zeros(1, dtype=torch.int64, device="cuda")
+            c.pi_dev(s.geom_struct(), d_tab, d_cnt)
+            torch.cuda.synchronize()
+            n = int(d_cnt.item())
+            c.close()
+            return n
+    except Exception:
+        pass
+    O = _oracle()
+    t = O.pi_table(O.bp_geom(s.locus(), s.detector(), s.object()))
+    v = t["valid"]
+    return int(np.sum(t["loop_end"][v] - t["loop_begin"][v] + 1))
+
+
+# ---------------------------------------------------------------------------------------------
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+    import ctrecon_b200 as ct
+    from ctrecon_b200 import _lib
+
+    ws, rank, local = dist_setup(args.gpus)
+    dev = torch.device("cuda", local)
+    s = config(args.config)
+    hil = {"fp32": _lib.HILBERT_FP32, "bf16x3": _lib.HILBERT_BF16X3,
+           "tf32": _lib.HILBERT_TF32}[args.hilbert]
+    pis = {"bisect": _lib.PI_BISECT, "newton": _lib.PI_NEWTON, "learned": _lib.PI_LEARNED}[args.pi]
+    ctx = ct.Context(local, hilbert=hil, pi_solver=pis)
+    geom = s.geom_struct()
+    fpar = ct.scan_filter_params(s)
+
+    # ---- inputs, resident in HBM before timing --------------------------------------------------
+    d_proj = torch.empty(s.proj_shape, dtype=torch.float32, device=dev)
+    ctx.phantom_dev(geom, s.ellipsoids(), d_proj, photons=s.photons or 0.0, seed=s.seed + rank)
+    d_fproj = torch.empty_like(d_proj)
+    d_img = torch.zeros(s.vol_shape, dtype=torch.float32, device=dev)
+    d_tab = torch.empty(ctx.pi_table_bytes(geom), dtype=torch.uint8, device=dev)
+    d_cnt = torch.zeros(1, dtype=torch.int64, device=dev)
+    # exact update count: the reference's loop count from the bisection PI solve
+    ctx.set_option(_lib.OPT_PI_SOLVER, _lib.PI_BISECT)
+    ctx.pi_dev(geom, d_tab, d_cnt)
+    torch.cuda.synchronize()
+    updates = int(d_cnt.item())
+    ctx.set_option(_lib.OPT_PI_SOLVER, pis)
+    stream = torch.cuda.current_stream()
+
+    ev = {k: [] for k in ("f0", "f1", "p1", "b1")}
+
+    def step(record):
+        if record:
+            e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+            e[0].record(stream)
+        ctx.filter_dev(fpar, d_proj, d_fproj)
+        if record:
+            e[1].record(stream)
+        ctx.pi_dev(geom, d_tab)
+        if record:
+            e[2].record(stream)
+        ctx.bkproj_dev(geom, d_fproj, d_img, d_pitab=d_tab)
+        if record:
+            e[3].record(stream)
+            for k, x in zip(("f0", "f1", "p1", "b1"), e):
+                ev[k].append(x)
+
+    for _ in range(max(3, args.warmup)):
+        step(False)
+    torch.cuda.synchronize()
+    barrier(ws)
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    torch.cuda.synchronize()
+    barrier(ws)
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    t_start.record(stream)
+    for _ in range(args.steps):
+        step(True)
+    t_end.record(stream)
+    torch.cuda.synchronize()
+    barrier(ws)
+    clocks = sampler.stop()
+    ms_total = t_start.elapsed_time(t_end)
+    ms_step = max_over_ranks(ms_total / args.steps, ws)
+    filt_ms = statistics.mean(a.elapsed_time(b) for a, b in zip(ev["f0"], ev["f1"]))
+    pi_ms = statistics.mean(a.elapsed_time(b) for a, b in zip(ev["f1"], ev["p1"]))
+    bp_ms = statistics.mean(a.elapsed_time(b) for a, b in zip(ev["p1"], ev["b1"]))
+    value = ws * updates / (ms_step / 1e3) / 1e9
+    chunk = ctx.get_option(_lib.OPT_FILTER_CHUNK)
+    nchunks = (s.P + chunk - 1) // chunk
+    launches_per_step = 2 * nchunks + 1 + 1
+    if hil != _lib.HILBERT_FP32:
+        launches_per_step += nchunks
+
+    # ---- e2e through the MEX-equivalent host calls (FP64 pinned host buffers) -----------------
+    e2e = None
+    if not args.no_e2e:
+        h_proj = torch.empty(s.proj_shape, dtype=torch.float64, pin_memory=True)
+        h_proj.copy_(d_proj.cpu().to(torch.float64))
+        h_fproj = torch.empty_like(h_proj).pin_memory()
+        h_img = torch.zeros(s.vol_shape, dtype=torch.float64).pin_memory()
+        np_proj, np_fproj, np_img = h_proj.numpy(), h_fproj.numpy(), h_img.numpy()
+        ctx.filter_host(fpar, np_proj, np_fproj)
+        ctx.bkproj_host(geom, np_fproj, np_img)
+        e2e_steps = max(1, min(args.steps, 3))
+        barrier(ws)
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            ctx.filter_host(fpar, np_proj, np_fproj)       # KatsevichFiltering_GPU
+            ctx.bkproj_host(geom, np_fproj, np_img)        # KatsevichBkProj_GPU
+        t_e2e = (time.perf_counter() - t0) / e2e_steps
+        t_e2e = max_over_ranks(t_e2e, ws)
+        nproj, nvox = int(np.prod(s.proj_shape)), int(np.prod(s.vol_shape))
+        e2e = {"value": ws * updates / t_e2e / 1e9, "unit": "GUPS",
+               "h2d_bytes_per_step": 8 * (2 * nproj + nvox),
+               "d2h_bytes_per_step": 8 * (nproj + nvox),
+               "s_per_vol": t_e2e,
+               "path": "ctrecon_filter_host_f64 + ctrecon_bkproj_host_f64 (MEX-equivalent)"}
+
+    # ---- roofline of the dominant kernel (backprojection) -----------------------------------------
+    peak, peak_kind = load_peaks()
+    achieved = BYTES_PER_UPDATE * updates / (bp_ms / 1e3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_kind,
+                "kernel": "k_bkproj", "model": "16 B per voxel-view update",
+                "traffic": load_traffic("k_bkproj", WORKLOAD_NAME)}
+
+    # ---- CPU baseline (rank 0, N = 1): the FP64 oracle restatement on a bounded sample -----------
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        try:
+            O = _oracle()
+            cores = os.cpu_count() or 1
+            n = 48
+            locus, det, obj, lo, hi = block_problem(O, s, n)
+            proj_sub = d_proj[lo:hi].cpu().numpy().astype(np.float64)
+            t1 = time.perf_counter()
+            cpu_filter_views(O, s, proj_sub[:10])
+            t_view = (time.perf_counter() - t1) / 8
+            fproj_sub = d_fproj[lo:hi].cpu().numpy().astype(np.float64)
+            t_bp, n_bp = cpu_bp_sample_port(O, s, fproj_sub, lo, hi, cores, n=n)
+            t_scan = t_view * s.P + t_bp * updates / max(n_bp, 1)
+            cpu = {"value": updates / t_scan / 1e9, "unit": "GUPS", "cores": cores,
+                   "kind": "port", "s_per_vol": t_scan,
+                   "sample": (f"FP64 oracle with {cores} OpenMP threads: filter of 8 views and "
+                              f"backprojection of a central {n}^3 block ({n_bp} updates), "
+                              f"scaled to {s.P} views and {updates} updates")}
+        except Exception as exc:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": "GUPS", "cores": 0, "kind": "port",
+                   "sample": f"failed: {exc}"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "GUPS", "n_gpus": ws,
+                "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": ms_step,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32", "data": "synthetic",
+                "config": {"workload": WORKLOAD_NAME, "volume": list(s.vol_shape),
+                           "voxel_mm": list(s.voxel_size), "detector": [s.ZL, s.YL],
+                           "views": s.P, "views_per_turn": s.views_per_turn,
+                           "hilbert": args.hilbert, "pi_solver": args.pi,
+                           "parallelism": f"replicas{ws}",
+                           "l2": "inputs larger than L2 (projections 1.75 GB)"},
+                "updates_per_step": updates, "s_per_vol": ms_step / 1e3,
+                "phase_ms": {"filter": filt_ms, "pi": pi_ms, "bkproj": bp_ms},
+                "bkproj_gups": updates / (bp_ms / 1e3) / 1e9,
+                "gpu_launches": launches_per_step * args.steps,
+                "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks}
+        print(json.dumps(line))
+    ctx.close()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

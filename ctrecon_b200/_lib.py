@@ -1,0 +1,107 @@
+"""ctypes bindings of ``libctrecon.so`` (the C ABI declared in ``include/ctrecon.h``).
+
+The library is built in-tree (``ctrecon_b200/lib/``) by ``ctrecon_b200/csrc/Makefile``;
+there is no fallback: if it is missing, loading raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_DIR = os.path.join(HERE, "lib")
+LIB_PATH = os.path.join(LIB_DIR, "libctrecon.so")
+MEX_DIR = os.path.join(LIB_DIR, "mex")
+
+# status codes (ctrecon_status)
+OK = 0
+ERR_INVALID_ARGUMENT = 1
+ERR_GEOMETRY = 2
+ERR_CUDA = 3
+ERR_OUT_OF_MEMORY = 4
+ERR_NO_DEVICE = 5
+ERR_TIMEOUT = 6
+ERR_UNSUPPORTED = 7
+ERR_INTERNAL = 8
+
+HILBERT_FP32, HILBERT_BF16X3, HILBERT_TF32 = 0, 1, 2
+PI_BISECT, PI_NEWTON, PI_LEARNED = 0, 1, 2
+OPT_HILBERT, OPT_PI_SOLVER, OPT_FILTER_CHUNK, OPT_BP_VARIANT, OPT_VERBOSE = 1, 2, 3, 4, 5
+
+
+class FilterParams(ctypes.Structure):
+    _fields_ = [("proj_scale", ctypes.c_double), ("dec_width", ctypes.c_double),
+                ("dec_height", ctypes.c_double), ("scan_r", ctypes.c_double),
+                ("std_dis", ctypes.c_double), ("helic_p", ctypes.c_double),
+                ("filter_coeff", ctypes.c_double), ("delta_angle", ctypes.c_double),
+                ("filtering_mode", ctypes.c_int), ("yl", ctypes.c_int), ("zl", ctypes.c_int),
+                ("proj_number", ctypes.c_int)]
+
+
+class BPGeom(ctypes.Structure):
+    _fields_ = [("locus", ctypes.c_double * 7), ("detector", ctypes.c_double * 6),
+                ("object", ctypes.c_double * 7), ("n_detector", ctypes.c_int),
+                ("n_object", ctypes.c_int)]
+
+
+_vp = ctypes.c_void_p
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+_st = ctypes.c_int
+
+# (name, restype, argtypes) of every exported entry point of include/ctrecon.h
+SIGNATURES = [
+    ("ctrecon_ctx_create", _st, [ctypes.c_int, ctypes.POINTER(_vp)]),
+    ("ctrecon_ctx_destroy", None, [_vp]),
+    ("ctrecon_last_error", ctypes.c_char_p, [_vp]),
+    ("ctrecon_status_string", ctypes.c_char_p, [_st]),
+    ("ctrecon_abi_version", ctypes.c_int, []),
+    ("ctrecon_set_option", _st, [_vp, ctypes.c_int, ctypes.c_int]),
+    ("ctrecon_get_option", _st, [_vp, ctypes.c_int, _ip]),
+    ("ctrecon_filter_host_f64", _st, [_vp, ctypes.POINTER(FilterParams), _dp, _dp]),
+    ("ctrecon_bkproj_host_f64", _st, [_vp, ctypes.POINTER(BPGeom), _dp, _dp]),
+    ("ctrecon_recon_host_f64", _st, [_vp, ctypes.POINTER(FilterParams), ctypes.POINTER(BPGeom),
+                                     _dp, _dp]),
+    ("ctrecon_filter_dev_f32", _st, [_vp, _vp, ctypes.POINTER(FilterParams), _vp, _vp]),
+    ("ctrecon_pi_table_bytes", _st, [ctypes.POINTER(BPGeom), ctypes.POINTER(ctypes.c_size_t)]),
+    ("ctrecon_pi_dev", _st, [_vp, _vp, ctypes.POINTER(BPGeom), _vp, _vp]),
+    ("ctrecon_bkproj_dev_f32", _st, [_vp, _vp, ctypes.POINTER(BPGeom), _vp, _vp, _vp]),
+    ("ctrecon_num_kappa", ctypes.c_int, [ctypes.c_int]),
+    ("ctrecon_filter_tables", _st, [ctypes.POINTER(FilterParams), _ip, _ip, _dp, _dp, _ip, _ip,
+                                    _dp, _dp]),
+    ("ctrecon_geometry_sizing", None, [ctypes.c_double] * 4 + [ctypes.c_int] * 2 + [_dp] * 3),
+    ("ctrecon_phantom_project_dev", _st, [_vp, _vp, ctypes.POINTER(BPGeom), _dp, ctypes.c_int,
+                                          ctypes.c_double, ctypes.c_uint64, _vp]),
+]
+
+_lib = None
+
+
+def lib():
+    """Load libctrecon.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing; build it with "
+                              f"`make -C ctrecon_b200/csrc` or __graft_entry__.build()")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, res, args in SIGNATURES:
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+class CtreconError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"[{status}] {message}")
+        self.status = status
+        self.message = message
+
+
+def check(status: int, ctx=None) -> None:
+    if status != OK:
+        msg = lib().ctrecon_last_error(ctx)
+        raise CtreconError(status, (msg or b"").decode(errors="replace") or
+                           lib().ctrecon_status_string(status).decode())

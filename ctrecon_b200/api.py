@@ -1,0 +1,261 @@
+"""Python face of the C ABI, mirroring the reference's MEX interface.
+
+Host functions take numpy arrays in the reference's MATLAB layouts (C-order shape
+``(P, ZL, YL)`` for projections, ``(NX, NY, NZ)`` for the image) and behave like the MEX
+functions they replace:
+
+* :func:`KatsevichFiltering_GPU` -- 14 arguments, filtered result written in place into
+  the 14th (``KatsevichFiltering_GPU.cu:939-978``);
+* :func:`KatsevichBkProj` / :func:`KatsevichBkProj_GPU` -- ``(geom, FProj, RecMatrix)``,
+  image updated in place (``KatsevichBkProj.cpp:314-352``).
+
+Device functions take CUDA tensors (torch is only the device-memory and stream plumbing)
+and run on the tensors' device, ordered on the current torch stream.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Mapping, Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import BPGeom, FilterParams, check, lib
+
+
+# ---- argument packing -----------------------------------------------------------------------
+def filter_params(ProjScale, DecWidth, DecHeigh, ScanR, StdDis, HelicP, FilterCoeFF, DeltaAngle,
+                  FilteringMode, YL, ZL, ProjNumber) -> FilterParams:
+    """Pack inputs 2..13 of KatsevichFiltering_GPU (ints truncated like the reference)."""
+    p = FilterParams()
+    p.proj_scale = float(int(ProjScale))
+    p.dec_width = float(DecWidth)
+    p.dec_height = float(DecHeigh)
+    p.scan_r = float(ScanR)
+    p.std_dis = float(StdDis)
+    p.helic_p = float(HelicP)
+    p.filter_coeff = float(FilterCoeFF)
+    p.delta_angle = float(DeltaAngle)
+    p.filtering_mode = int(FilteringMode)
+    p.yl = int(YL)
+    p.zl = int(ZL)
+    p.proj_number = int(ProjNumber)
+    return p
+
+
+def bp_geom(geom) -> BPGeom:
+    """Pack a geom struct (mapping with Locus, Detector, Object in that order, as built at
+    FunctionKat_v6.m:110-112) or a (locus, detector, object) triple."""
+    if isinstance(geom, BPGeom):
+        return geom
+    if isinstance(geom, Mapping):
+        vals = list(geom.values())
+    else:
+        vals = list(geom)
+    locus, det, obj = (np.asarray(v, dtype=np.float64).ravel() for v in vals[:3])
+    if locus.size < 7 or det.size < 4 or obj.size < 4:
+        raise ValueError("geom needs Locus[7], Detector[>=4], Object[>=4]")
+    g = BPGeom()
+    for i in range(7):
+        g.locus[i] = locus[i]
+    for i in range(min(6, det.size)):
+        g.detector[i] = det[i]
+    for i in range(min(7, obj.size)):
+        g.object[i] = obj[i]
+    g.n_detector = min(6, det.size)
+    g.n_object = min(7, obj.size)
+    return g
+
+
+def scan_filter_params(scan) -> FilterParams:
+    return filter_params(*scan.filter_args())
+
+
+def num_kappa(zl: int) -> int:
+    return lib().ctrecon_num_kappa(int(zl))
+
+
+def geometry_sizing(ScanR, StdDis, HelicP, ObjR, YL, ZL):
+    w, h, d = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+    lib().ctrecon_geometry_sizing(ScanR, StdDis, HelicP, ObjR, int(YL), int(ZL),
+                                  ctypes.byref(w), ctypes.byref(h), ctypes.byref(d))
+    return w.value, h.value, d.value
+
+
+def filter_tables(p: FilterParams) -> dict:
+    """The filter's FP64 host tables (see ctrecon_filter_tables); no GPU needed."""
+    AL, YL, ZL = num_kappa(p.zl), p.yl, p.zl
+    ip = ctypes.POINTER(ctypes.c_int)
+    dp = ctypes.POINTER(ctypes.c_double)
+    t = dict(r0=np.zeros((AL, YL), np.int32), r1=np.zeros((AL, YL), np.int32),
+             wa=np.zeros((AL, YL)), wb=np.zeros((AL, YL)), b=np.zeros((ZL, YL), np.int32),
+             e=np.zeros((ZL, YL), np.int32), gb=np.zeros((ZL, YL)), ge=np.zeros((ZL, YL)))
+    st = lib().ctrecon_filter_tables(
+        ctypes.byref(p), t["r0"].ctypes.data_as(ip), t["r1"].ctypes.data_as(ip),
+        t["wa"].ctypes.data_as(dp), t["wb"].ctypes.data_as(dp), t["b"].ctypes.data_as(ip),
+        t["e"].ctypes.data_as(ip), t["gb"].ctypes.data_as(dp), t["ge"].ctypes.data_as(dp))
+    check(st, None)
+    return t
+
+
+def _f64(a: np.ndarray, name: str, n: int) -> np.ndarray:
+    if not isinstance(a, np.ndarray) or a.dtype != np.float64 or not a.flags.c_contiguous:
+        raise TypeError(f"{name} must be a C-contiguous float64 numpy array")
+    if a.size < n:
+        raise ValueError(f"{name} has {a.size} elements, needs {n}")
+    return a
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _stream_handle(stream) -> int:
+    if stream is None:
+        import torch
+        return torch.cuda.current_stream().cuda_stream
+    if isinstance(stream, int):
+        return stream
+    return stream.cuda_stream
+
+
+def _tptr(t, dtype_name: str, name: str) -> int:
+    if t is None:
+        return None
+    if not t.is_cuda:
+        raise TypeError(f"{name} must be a CUDA tensor")
+    if dtype_name and str(t.dtype) != f"torch.{dtype_name}":
+        raise TypeError(f"{name} must be torch.{dtype_name}, got {t.dtype}")
+    if not t.is_contiguous():
+        raise ValueError(f"{name} must be contiguous")
+    return t.data_ptr()
+
+
+# ---- context ---------------------------------------------------------------------------------
+class Context:
+    """One ctrecon context on one device (not thread-safe; one per host thread)."""
+
+    def __init__(self, device: int = 0, hilbert: int = _lib.HILBERT_FP32,
+                 pi_solver: int = _lib.PI_BISECT):
+        h = ctypes.c_void_p()
+        check(lib().ctrecon_ctx_create(int(device), ctypes.byref(h)), None)
+        self._h = h
+        self.device = device
+        self.set_option(_lib.OPT_HILBERT, hilbert)
+        self.set_option(_lib.OPT_PI_SOLVER, pi_solver)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if self._h:
+            lib().ctrecon_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_option(self, opt: int, value: int):
+        check(lib().ctrecon_set_option(self._h, int(opt), int(value)), self._h)
+
+    def get_option(self, opt: int) -> int:
+        v = ctypes.c_int()
+        check(lib().ctrecon_get_option(self._h, int(opt), ctypes.byref(v)), self._h)
+        return v.value
+
+    # -- host FP64 (MEX-equivalent) --------------------------------------------------------
+    def filter_host(self, p: FilterParams, proj: np.ndarray, fproj: Optional[np.ndarray] = None):
+        n = p.yl * p.zl * p.proj_number
+        _f64(proj, "Proj", n)
+        if fproj is None:
+            fproj = np.empty_like(proj)
+        _f64(fproj, "FProj", n)
+        check(lib().ctrecon_filter_host_f64(self._h, ctypes.byref(p), _dptr(proj), _dptr(fproj)),
+              self._h)
+        return fproj
+
+    def bkproj_host(self, geom, fproj: np.ndarray, image: np.ndarray) -> np.ndarray:
+        g = bp_geom(geom)
+        check(lib().ctrecon_bkproj_host_f64(self._h, ctypes.byref(g), _dptr(fproj), _dptr(image)),
+              self._h)
+        return image
+
+    def recon_host(self, p: FilterParams, geom, proj: np.ndarray, image: np.ndarray):
+        g = bp_geom(geom)
+        check(lib().ctrecon_recon_host_f64(self._h, ctypes.byref(p), ctypes.byref(g), _dptr(proj),
+                                           _dptr(image)), self._h)
+        return image
+
+    # -- device FP32 (torch tensors) -----------------------------------------------------------
+    def filter_dev(self, p: FilterParams, d_proj, d_fproj, stream=None):
+        check(lib().ctrecon_filter_dev_f32(self._h, _stream_handle(stream), ctypes.byref(p),
+                                           _tptr(d_proj, "float32", "d_proj"),
+                                           _tptr(d_fproj, "float32", "d_fproj")), self._h)
+
+    @staticmethod
+    def pi_table_bytes(geom) -> int:
+        g = bp_geom(geom)
+        n = ctypes.c_size_t()
+        check(lib().ctrecon_pi_table_bytes(ctypes.byref(g), ctypes.byref(n)), None)
+        return n.value
+
+    def pi_dev(self, geom, d_pitab, d_updates=None, stream=None):
+        g = bp_geom(geom)
+        check(lib().ctrecon_pi_dev(self._h, _stream_handle(stream), ctypes.byref(g),
+                                   _tptr(d_pitab, "", "d_pitab"),
+                                   _tptr(d_updates, "int64", "d_updates")), self._h)
+
+    def bkproj_dev(self, geom, d_fproj, d_image, d_pitab=None, stream=None):
+        g = bp_geom(geom)
+        check(lib().ctrecon_bkproj_dev_f32(self._h, _stream_handle(stream), ctypes.byref(g),
+                                           _tptr(d_fproj, "float32", "d_fproj"),
+                                           _tptr(d_pitab, "", "d_pitab"),
+                                           _tptr(d_image, "float32", "d_image")), self._h)
+
+    def phantom_dev(self, geom, ell: np.ndarray, d_proj, photons: float = 0.0, seed: int = 0,
+                    stream=None):
+        g = bp_geom(geom)
+        ell = np.ascontiguousarray(ell, dtype=np.float64).reshape(-1, 10)
+        check(lib().ctrecon_phantom_project_dev(
+            self._h, _stream_handle(stream), ctypes.byref(g), _dptr(ell), ell.shape[0],
+            float(photons), int(seed) & ((1 << 64) - 1), _tptr(d_proj, "float32", "d_proj")),
+            self._h)
+
+
+_default: Optional[Context] = None
+
+
+def default_context() -> Context:
+    global _default
+    if _default is None:
+        _default = Context(0)
+    return _default
+
+
+# ---- the reference's MEX functions -------------------------------------------------------------
+def KatsevichFiltering_GPU(Proj, ProjScale, DecWidth, DecHeigh, ScanR, StdDis, HelicP,
+                           FilterCoeFF, DeltaAngle, FilteringMode, YL, ZL, ProjNumber, FProj):
+    """KatsevichFiltering_GPU.cu:939-978: filter Proj, result written in place into FProj."""
+    p = filter_params(ProjScale, DecWidth, DecHeigh, ScanR, StdDis, HelicP, FilterCoeFF,
+                      DeltaAngle, FilteringMode, YL, ZL, ProjNumber)
+    default_context().filter_host(p, Proj, FProj)
+
+
+def KatsevichBkProj(geom, FProj, RecMatrix):
+    """KatsevichBkProj.cpp:314-352: backproject FProj into RecMatrix in place."""
+    _f64(FProj, "FProj", 1)
+    _f64(RecMatrix, "RecMatrix", 1)
+    default_context().bkproj_host(geom, FProj, RecMatrix)
+
+
+KatsevichBkProj_GPU = KatsevichBkProj

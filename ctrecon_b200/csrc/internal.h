@@ -1,0 +1,153 @@
+// internal.h -- shared host/device definitions of ctrecon-b200 (not part of the C ABI).
+#pragma once
+
+#include "ctrecon.h"
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace ctr {
+
+// The reference's pi for the filter and the backprojector (KatsevichFiltering.m:32,
+// KatsevichBkProj.cpp:25); geometry must use the same constant to agree with it.
+constexpr double kRefPi = 3.14159265358979;
+
+// ---- status plumbing ---------------------------------------------------------------------
+struct Status {
+    ctrecon_status code = CTRECON_OK;
+    std::string msg;
+    bool ok() const { return code == CTRECON_OK; }
+    static Status Ok() { return {}; }
+};
+Status make_status(ctrecon_status c, const std::string& m);
+Status cuda_status(cudaError_t e, const char* what);
+#define CTR_CUDA(call)                                                   \
+    do {                                                                 \
+        cudaError_t _e = (call);                                         \
+        if (_e != cudaSuccess) return ::ctr::cuda_status(_e, #call);     \
+    } while (0)
+#define CTR_TRY(expr)                                                    \
+    do {                                                                 \
+        ::ctr::Status _s = (expr);                                       \
+        if (!_s.ok()) return _s;                                         \
+    } while (0)
+
+// ---- device memory owned by a context (grow-only cache) ------------------------------------
+struct DevBuf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf();
+    Status ensure(size_t b, const char* what);
+    void release();
+    template <class T> T* as() const { return static_cast<T*>(ptr); }
+};
+
+// ---- filter tables -----------------------------------------------------------------------
+// forward rebin entry per (kappa row a, column y): X = wa*GF[r0] + wb*GF[r1]
+struct FwEntry { int r0, r1; float wa, wb; };
+// backward rebin entry per (row z, column y): FProj = gb*H[b] + ge*H[e], H the unsigned
+// Hilbert sum (the sign and the post-weight 1/coef are folded into gb/ge)
+struct BkEntry { int b, e; float gb, ge; };
+
+struct FilterTables {
+    int YL = 0, ZL = 0, AL = 0, QQ = 0, P = 0;
+    double DeltaL = 0, DeltaU = 0, DeltaV = 0;
+    std::vector<double> y, z, AZCor, coef, Rato;
+    std::vector<int> r0, r1, b, e;          // forward [AL*YL], backward [ZL*YL]
+    std::vector<double> wa, wb, gb, ge;     // FP64 weights
+    std::vector<double> cu;                 // u-derivative coefficient per column
+    double cv = 0;                          // v-derivative coefficient 1/(2 dV D)
+    std::vector<double> h;                  // Hilbert taps h[m + YL - 1]
+};
+// Builds the tables of KatsevichFiltering.m:40-153 and :191-287 on the host in FP64.
+Status build_filter_tables(const ctrecon_filter_params& p, FilterTables& t);
+
+// Device form of the tables for one parameter set.
+struct FilterPlan {
+    ctrecon_filter_params p{};
+    FilterTables t;
+    int YLp = 0;  // padded row length of the kappa-row buffers (multiple of 64)
+    DevBuf fw, bk, cuy, zcv, h;
+    float inv2dl = 0;
+};
+
+// ---- backprojection geometry ----------------------------------------------------------------
+struct BPGeom {
+    // reference quantities (KatsevichBkProj.cpp:80-147)
+    double ScanR, StdDis, HelicP, ProjCtr, ObjR, DecWidth, DecHeigh;
+    int ProjScale, ProjBegin, ProjNum, YL, ZL, NX, NY, NZ;
+    double DeltaL, DeltaU, DeltaV, HalfY, HalfZ, dx, dy, dz, XC, YC, ZC;
+};
+Status parse_bp_geom(const ctrecon_bp_geom& g, BPGeom& out);
+
+// Per-voxel PI-interval record (16 bytes): B = bi + bf and T = ti + tf are the fractional
+// view indices of KatsevichBkProj.cpp:177-178; bi == kPiInvalid marks an unwritten voxel.
+struct PiRecord { int bi; float bf; int ti; float tf; };
+constexpr int kPiInvalid = 0x7fffffff;
+
+// Kernel parameter block of the PI solve and the backprojector.
+struct BPParams {
+    int NX, NY, NZ, P, YL, ZL;
+    double ScanR, HelicP, DeltaL, CtrMinusBeg, ObjR2;
+    double XC, YC, ZC, dx, dy, dz;
+    float Rf, DdU, DdV, HalfY, HalfZ, invPs;
+};
+BPParams make_bp_params(const BPGeom& g);
+
+struct BPPlan {
+    BPGeom g{};
+    BPParams kp{};
+    DevBuf views;   // float4 per view: cos, sin, source z, 0
+    DevBuf xyz;     // float voxel coordinates x[NX], y[NY], z[NZ]
+};
+
+}  // namespace ctr
+
+// ---- the context (opaque in the C ABI) -------------------------------------------------------
+struct ctrecon_ctx {
+    int device = 0;
+    std::string last_error;
+    int opt_hilbert = CTRECON_HILBERT_FP32;
+    int opt_pi = CTRECON_PI_BISECT;
+    int opt_filter_chunk = 512;
+    int opt_bp_variant = 0;
+    int opt_verbose = 0;
+    cudaStream_t host_stream = nullptr;  // stream for the synchronous host calls
+    // cached plans and work buffers
+    ctr::FilterPlan fplan;
+    bool fplan_valid = false;
+    ctr::BPPlan bplan;
+    bool bplan_valid = false;
+    ctr::DevBuf ws_kappa;    // kappa-row chunk buffer of the filter
+    ctr::DevBuf ws_pitab;    // PI table when the caller does not pass one
+    ctr::DevBuf ws_count;    // update counter
+    ctr::DevBuf ws_a, ws_b, ws_c, ws_d;  // host-call staging (f64 in, f32, f32 out, f64 out)
+    ctr::DevBuf ws_ell;      // phantom ellipsoids
+    ctr::DevBuf ws_flag;     // device error word
+};
+
+namespace ctr {
+Status get_filter_plan(ctrecon_ctx* ctx, const ctrecon_filter_params& p, FilterPlan** out);
+Status get_bp_plan(ctrecon_ctx* ctx, const ctrecon_bp_geom& g, BPPlan** out);
+
+// kernel launchers (filter.cu, pi.cu, bkproj.cu, phantom.cu)
+Status launch_filter(ctrecon_ctx* ctx, cudaStream_t s, FilterPlan& plan, const float* d_proj,
+                     int proj_view0, int proj_nviews, float* d_fproj, int out_view0,
+                     int view_begin, int view_end);
+Status launch_pi(ctrecon_ctx* ctx, cudaStream_t s, BPPlan& plan, PiRecord* d_pitab,
+                 unsigned long long* d_updates);
+Status launch_bkproj_f32(ctrecon_ctx* ctx, cudaStream_t s, BPPlan& plan, const float* d_fproj,
+                         const PiRecord* d_pitab, float* d_image);
+Status launch_bkproj_f64out(ctrecon_ctx* ctx, cudaStream_t s, BPPlan& plan,
+                            const float* d_fproj, const PiRecord* d_pitab, double* d_image);
+Status launch_convert_f64_to_f32(cudaStream_t s, const double* in, float* out, size_t n);
+Status launch_convert_f32_to_f64(cudaStream_t s, const float* in, double* out, size_t n);
+Status launch_phantom(cudaStream_t s, const BPGeom& g, const double* d_ell, int n_ell,
+                      double photons, uint64_t seed, float* d_proj, float* d_max);
+}  // namespace ctr

@@ -1,0 +1,193 @@
+/*
+ * ctrecon.h -- C ABI of ctrecon-b200, a single-GPU (NVIDIA B200, sm_100a) implementation of
+ * CTRecon's Katsevich exact helical cone-beam reconstruction chain:
+ *
+ *   derivative -> forward height rebin -> Hilbert filter -> backward rebin   (filter)
+ *   PI-line solve -> voxel-driven backprojection                             (backprojection)
+ *
+ * Plain C types only (no CUDA or torch types): streams are passed as `void*` (a
+ * cudaStream_t, NULL = the legacy default stream) and device buffers as plain pointers.
+ * Every call returns a ctrecon_status; on failure ctrecon_last_error() describes it. No C++
+ * exception crosses this boundary.
+ *
+ * Layouts are the reference's MATLAB column-major arrays:
+ *   projections  Proj(YL, ZL, P)   linear index (p*ZL + z)*YL + y
+ *                                  (KatsevichFiltering_GPU.cu:63, KatsevichFiltering.m:33)
+ *   image        z fastest         linear index (x*NY + y)*NZ + z   (KatsevichBkProj.cpp:264)
+ *
+ * Threading: one context per host thread; a context is not thread-safe. Host (`_host_f64`)
+ * calls are synchronous, like the reference's MEX functions; device (`_dev`) calls are
+ * ordered on the given stream and return once the work is enqueued.
+ */
+#ifndef CTRECON_H
+#define CTRECON_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CTRECON_ABI_VERSION 1
+
+typedef enum ctrecon_status {
+    CTRECON_OK = 0,
+    CTRECON_ERR_INVALID_ARGUMENT = 1, /* sizes or parameters the chain cannot run */
+    CTRECON_ERR_GEOMETRY = 2,         /* the reference would index outside an array */
+    CTRECON_ERR_CUDA = 3,             /* a CUDA runtime call or kernel failed */
+    CTRECON_ERR_OUT_OF_MEMORY = 4,    /* device or pinned-host allocation failed */
+    CTRECON_ERR_NO_DEVICE = 5,        /* no usable sm_100 device */
+    CTRECON_ERR_TIMEOUT = 6,          /* a bounded device-side wait gave up */
+    CTRECON_ERR_UNSUPPORTED = 7,      /* option or size outside what this build supports */
+    CTRECON_ERR_INTERNAL = 8
+} ctrecon_status;
+
+typedef struct ctrecon_ctx ctrecon_ctx;
+
+/* Inputs 2..13 of KatsevichFiltering_GPU (KatsevichFiltering_GPU.cu:941-959), in order. */
+typedef struct ctrecon_filter_params {
+    double proj_scale;   /* ProjScale: views per turn */
+    double dec_width;    /* DecWidth: detector width (mm) */
+    double dec_height;   /* DecHeigh: detector height (mm) */
+    double scan_r;       /* ScanR: source-to-axis distance */
+    double std_dis;      /* StdDis: source-to-detector distance */
+    double helic_p;      /* HelicP: helical pitch (table travel per turn) */
+    double filter_coeff; /* FilterCoeFF: filtering coefficient tau */
+    double delta_angle;  /* DeltaAngle: 2*acos(ObjR/ScanR) */
+    int filtering_mode;  /* FilteringMode: 2 = dual symmetric operators, else single */
+    int yl;              /* YL: detector columns */
+    int zl;              /* ZL: detector rows */
+    int proj_number;     /* ProjNumber: views */
+} ctrecon_filter_params;
+
+/* The geom struct of KatsevichBkProj (FunctionKat_v6.m:110-112, read at
+ * KatsevichBkProj.cpp:80-95 and KatsevichBkProj_GPU.cu:353-374), field by position:
+ *   locus    = [ScanR StdDis HelicP ProjScale ProjBeginIndex ProjEndIndex ProjCtr]
+ *   detector = [DecWidth YL DecHeigh ZL DetCtrU DetCtrV]      (n_detector = 4 or 6)
+ *   object   = [ObjR RecSX RecSY RecSZ DX DY DZ]              (n_object   = 4 or 7)
+ * When present, DetCtrU/V and DX/DY/DZ are honoured (every reference caller passes
+ * exactly (N-1)/2 and 2*ObjR/N, where this equals KatsevichBkProj.cpp). */
+typedef struct ctrecon_bp_geom {
+    double locus[7];
+    double detector[6];
+    double object[7];
+    int n_detector;
+    int n_object;
+} ctrecon_bp_geom;
+
+/* Hilbert-filter arithmetic (CTRECON_OPT_HILBERT). */
+enum {
+    CTRECON_HILBERT_FP32 = 0,   /* FP32 SIMT direct Toeplitz sum (the plain form) */
+    CTRECON_HILBERT_BF16X3 = 1, /* tcgen05 Toeplitz GEMM, BF16 hi/lo split, 3 products */
+    CTRECON_HILBERT_TF32 = 2    /* tcgen05 Toeplitz GEMM in TF32 */
+};
+
+/* PI-line solver (CTRECON_OPT_PI_SOLVER). All are FP64 and converge to the same tau. */
+enum {
+    CTRECON_PI_BISECT = 0,  /* bisection of KatsevichBkProj.cpp:283-312 (the judge) */
+    CTRECON_PI_NEWTON = 1,  /* safeguarded Newton from the bracket midpoint */
+    CTRECON_PI_LEARNED = 2  /* Newton seeded by the trained PI-line network */
+};
+
+typedef enum ctrecon_option {
+    CTRECON_OPT_HILBERT = 1,          /* CTRECON_HILBERT_*; default FP32 */
+    CTRECON_OPT_PI_SOLVER = 2,        /* CTRECON_PI_*; default BISECT */
+    CTRECON_OPT_FILTER_CHUNK = 3,     /* views per filter work chunk; default 512 */
+    CTRECON_OPT_BP_VARIANT = 4,       /* backprojector variant (autotuner), default 0 */
+    CTRECON_OPT_VERBOSE = 5
+} ctrecon_option;
+
+/* ---- context ---------------------------------------------------------------------- */
+ctrecon_status ctrecon_ctx_create(int device, ctrecon_ctx** out);
+void ctrecon_ctx_destroy(ctrecon_ctx* ctx);
+const char* ctrecon_last_error(const ctrecon_ctx* ctx);
+const char* ctrecon_status_string(ctrecon_status s);
+int ctrecon_abi_version(void);
+ctrecon_status ctrecon_set_option(ctrecon_ctx* ctx, ctrecon_option opt, int value);
+ctrecon_status ctrecon_get_option(const ctrecon_ctx* ctx, ctrecon_option opt, int* value);
+
+/* ---- host, FP64, MEX-equivalent (synchronous) ------------------------------------------ */
+
+/* Replaces the KatsevichFiltering_GPU MEX function (KatsevichFiltering_GPU.cu:939-978,
+ * caller KatsevichFiltering.m:37-38): filters `proj` (YL x ZL x P doubles) and writes the
+ * result into `fproj` (same shape; may alias `proj`, as the MATLAB caller's lazy copy
+ * makes it). Computes KatsevichFiltering.m:39-287. */
+ctrecon_status ctrecon_filter_host_f64(ctrecon_ctx* ctx, const ctrecon_filter_params* p,
+                                       const double* proj, double* fproj);
+
+/* Replaces the KatsevichBkProj / KatsevichBkProj_GPU MEX functions
+ * (KatsevichBkProj.cpp:314-352, KatsevichBkProj_GPU.cu:332-429; callers
+ * FunctionKat_v6.m:113, katsevichReconForGUI.m:107-109): backprojects `fproj` into
+ * `image` in place. Voxels outside the cylinder of radius ObjR or without a PI interval
+ * inside the scan keep their value, as in KatsevichBkProj.cpp. */
+ctrecon_status ctrecon_bkproj_host_f64(ctrecon_ctx* ctx, const ctrecon_bp_geom* g,
+                                       const double* fproj, double* image);
+
+/* Filter + backprojection in one call with the filtered projections kept on the device
+ * (FunctionKat_v6.m:85-113 without the intermediate FProj round trip). */
+ctrecon_status ctrecon_recon_host_f64(ctrecon_ctx* ctx, const ctrecon_filter_params* p,
+                                      const ctrecon_bp_geom* g, const double* proj,
+                                      double* image);
+
+/* ---- device, FP32, stream-ordered ------------------------------------------------------ */
+
+/* Filter of device-resident FP32 projections (KatsevichFiltering_GPU<T>,
+ * KatsevichFiltering_GPU.cu:858-935). d_fproj must not alias d_proj. */
+ctrecon_status ctrecon_filter_dev_f32(ctrecon_ctx* ctx, void* stream,
+                                      const ctrecon_filter_params* p, const float* d_proj,
+                                      float* d_fproj);
+
+/* Bytes of the per-voxel PI-interval table written by ctrecon_pi_dev. */
+ctrecon_status ctrecon_pi_table_bytes(const ctrecon_bp_geom* g, size_t* bytes);
+
+/* PI-line solve for every voxel (PISegment, KatsevichBkProj.cpp:283-312 and the interval
+ * and endpoint rules of :177-234) into d_pitab. If d_updates is not NULL it receives (on
+ * the device, as one unsigned long long) sum(LoopEnd-LoopBegin+1) over written voxels. */
+ctrecon_status ctrecon_pi_dev(ctrecon_ctx* ctx, void* stream, const ctrecon_bp_geom* g,
+                              void* d_pitab, unsigned long long* d_updates);
+
+/* Voxel-driven backprojection (KatsevichBkProj.cpp:164-265) of device-resident FP32
+ * filtered projections into the device FP32 image (in place: unwritten voxels keep their
+ * value). d_pitab from ctrecon_pi_dev, or NULL to solve the PI lines internally. */
+ctrecon_status ctrecon_bkproj_dev_f32(ctrecon_ctx* ctx, void* stream,
+                                      const ctrecon_bp_geom* g, const float* d_fproj,
+                                      const void* d_pitab, float* d_image);
+
+/* ---- tables and helpers (host only, no GPU needed) --------------------------------------- */
+
+/* Number of kappa lines AL = 2*ceil(0.65*ZL)+1 (KatsevichFiltering.m:103-104). */
+int ctrecon_num_kappa(int zl);
+
+/* The filter's FP64 host tables, as the device uses them (rounded to FP32 there):
+ * forward rebin (KatsevichFiltering.m:131-153): per (a, y) rows r0/r1 and weights
+ *   wa/wb including the pre-weight, X[a][y] = wa*GF[r0][y] + wb*GF[r1][y];
+ * backward rebin (:191-287): per (z, y) kappa rows b/e and weights gb/ge including the
+ *   Hilbert sign and the post-weight, FProj[z][y] = gb*H[b][y] + ge*H[e][y] where H is
+ *   the unsigned Hilbert sum. Arrays are [AL*YL] (index a*YL+y) and [ZL*YL] (z*YL+y);
+ *   any may be NULL. */
+ctrecon_status ctrecon_filter_tables(const ctrecon_filter_params* p, int* r0, int* r1,
+                                     double* wa, double* wb, int* b, int* e, double* gb,
+                                     double* ge);
+
+/* Detector sizing of FunctionKat_v6.m:49-57 (with its PI = 3.1415926). */
+void ctrecon_geometry_sizing(double scan_r, double std_dis, double helic_p, double obj_r,
+                             int yl, int zl, double* dec_width, double* dec_height,
+                             double* delta);
+
+/* ---- analytic ellipsoid phantom (input generator; FP64 on the device) ------------------- */
+
+/* Line integrals of n_ell ellipsoids (rows of 10 doubles: cx cy cz a b c phi theta psi
+ * density; ZXZ Euler angles) for all views of geometry g into d_proj (FP32, layout
+ * above), the chord formula of CreateProjSlice.cpp:98-134 on a flat detector. If
+ * photons > 0, Poisson noise with `photons` incident photons per ray is applied with the
+ * attenuation scale mu = 8/max(line integral) (seeded, reproducible). */
+ctrecon_status ctrecon_phantom_project_dev(ctrecon_ctx* ctx, void* stream,
+                                           const ctrecon_bp_geom* g, const double* ell,
+                                           int n_ell, double photons, uint64_t seed,
+                                           float* d_proj);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CTRECON_H */

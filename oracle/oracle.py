@@ -1,0 +1,225 @@
+"""ctypes wrapper of the FP64 CPU oracle (TEST INFRASTRUCTURE ONLY).
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg may import
+this module; the product never does. It wraps ``liborc.so`` (the C restatement in
+``katsevich_oracle.c``) and ``_ref/libkatsevich_bkproj_ref.so`` (the reference's own
+``KatsevichBkProj.cpp``, compiled unchanged by ``oracle/Makefile``).
+
+Array conventions (numpy C order == the reference's MATLAB column-major arrays):
+  proj / fproj : shape (P, ZL, YL)   -- MATLAB Proj(YL, ZL, P)
+  image        : shape (NX, NY, NZ)  -- linear index (x*NY + y)*NZ + z
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liborc.so")
+REF_BKPROJ_PATH = os.path.join(HERE, "_ref", "libkatsevich_bkproj_ref.so")
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+_up = ctypes.POINTER(ctypes.c_ubyte)
+
+
+class FilterParams(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in (
+        "ProjScale", "DecWidth", "DecHeigh", "ScanR", "StdDis", "HelicP", "FilterCoeFF",
+        "DeltaAngle")] + [(n, ctypes.c_int) for n in ("FilteringMode", "YL", "ZL", "ProjNumber")]
+
+
+class BPGeom(ctypes.Structure):
+    _fields_ = [("locus", ctypes.c_double * 7), ("detector", ctypes.c_double * 6),
+                ("object", ctypes.c_double * 7), ("n_detector", ctypes.c_int),
+                ("n_object", ctypes.c_int), ("honour_extras", ctypes.c_int)]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FileNotFoundError(f"{LIB_PATH} missing: run `make -C oracle`")
+        L = ctypes.CDLL(LIB_PATH)
+        L.orc_geometry_sizing.argtypes = [ctypes.c_double] * 4 + [ctypes.c_int] * 2 + [_dp] * 3
+        L.orc_num_kappa.argtypes = [ctypes.c_int, _ip]
+        L.orc_filter_tables.argtypes = [ctypes.POINTER(FilterParams), _dp, _dp, _dp, _ip, _dp,
+                                        _dp, _ip, _ip, _dp, _dp]
+        L.orc_hilbert_taps.argtypes = [ctypes.c_int, _dp]
+        L.orc_filter.argtypes = [ctypes.POINTER(FilterParams), _dp, _dp, ctypes.c_int,
+                                 ctypes.c_int, ctypes.c_int]
+        L.orc_filter_view_stages.argtypes = [ctypes.POINTER(FilterParams), _dp, ctypes.c_int,
+                                             _dp, _dp, _dp]
+        L.orc_pisegment.argtypes = [ctypes.c_double] * 3 + [_dp, _dp]
+        L.orc_pisegment.restype = None
+        L.orc_bkproj.argtypes = [ctypes.POINTER(BPGeom), _dp, _dp] + [ctypes.c_int] * 5 + [
+            ctypes.POINTER(ctypes.c_longlong), _up]
+        L.orc_pi_table.argtypes = [ctypes.POINTER(BPGeom), _dp, _dp, _ip, _ip, _up, ctypes.c_int]
+        L.orc_project_ellipsoids.argtypes = [ctypes.POINTER(BPGeom), _dp, ctypes.c_int, _dp,
+                                             ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        _lib = L
+    return _lib
+
+
+def _ptr(a, t=_dp):
+    return a.ctypes.data_as(t)
+
+
+class OracleError(RuntimeError):
+    pass
+
+
+def _check(rc, what):
+    if rc != 0:
+        raise OracleError(f"{what} failed with code {rc}")
+
+
+# ---------------------------------------------------------------------------------------
+def geometry_sizing(ScanR, StdDis, HelicP, ObjR, YL, ZL):
+    """FunctionKat_v6.m:49-57 -> (DecWidth, DecHeigh, delta)."""
+    w, h, d = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+    lib().orc_geometry_sizing(ScanR, StdDis, HelicP, ObjR, YL, ZL, ctypes.byref(w),
+                              ctypes.byref(h), ctypes.byref(d))
+    return w.value, h.value, d.value
+
+
+def num_kappa(ZL):
+    qq = ctypes.c_int()
+    al = lib().orc_num_kappa(ZL, ctypes.byref(qq))
+    return al, qq.value
+
+
+def filter_params(**kw) -> FilterParams:
+    fp = FilterParams()
+    for k, v in kw.items():
+        setattr(fp, k, v)
+    return fp
+
+
+def filter_tables(fp: FilterParams) -> dict:
+    AL, QQ = num_kappa(fp.ZL)
+    YL, ZL = fp.YL, fp.ZL
+    out = dict(AZCor=np.zeros((AL, YL)), coef=np.zeros((AL, YL)), Rato=np.zeros(AL),
+               lw=np.zeros((AL, YL), np.int32), w_lw=np.zeros((AL, YL)),
+               w_up=np.zeros((AL, YL)), bAL=np.zeros((ZL, YL), np.int32),
+               eAL=np.zeros((ZL, YL), np.int32), bC=np.zeros((ZL, YL)), eC=np.zeros((ZL, YL)))
+    rc = lib().orc_filter_tables(
+        ctypes.byref(fp), _ptr(out["AZCor"]), _ptr(out["coef"]), _ptr(out["Rato"]),
+        _ptr(out["lw"], _ip), _ptr(out["w_lw"]), _ptr(out["w_up"]), _ptr(out["bAL"], _ip),
+        _ptr(out["eAL"], _ip), _ptr(out["bC"]), _ptr(out["eC"]))
+    _check(rc, "orc_filter_tables")
+    out["AL"], out["QQ"] = AL, QQ
+    return out
+
+
+def hilbert_taps(YL) -> np.ndarray:
+    h = np.zeros(2 * YL - 1)
+    _check(lib().orc_hilbert_taps(YL, _ptr(h)), "orc_hilbert_taps")
+    return h
+
+
+def katsevich_filter(fp: FilterParams, proj: np.ndarray, p_begin=0, p_end=0, nthreads=0):
+    """KatsevichFiltering.m (CPU branch) on views [p_begin, p_end) -> FProj (same shape)."""
+    proj = np.ascontiguousarray(proj, dtype=np.float64)
+    assert proj.shape == (fp.ProjNumber, fp.ZL, fp.YL)
+    out = np.zeros_like(proj)
+    _check(lib().orc_filter(ctypes.byref(fp), _ptr(proj), _ptr(out), p_begin, p_end, nthreads),
+           "orc_filter")
+    return out
+
+
+def filter_view_stages(fp: FilterParams, proj: np.ndarray, p: int):
+    AL, _ = num_kappa(fp.ZL)
+    proj = np.ascontiguousarray(proj, dtype=np.float64)
+    gf = np.zeros((fp.ZL, fp.YL))
+    xin = np.zeros((AL, fp.YL))
+    xout = np.zeros((AL, fp.YL))
+    _check(lib().orc_filter_view_stages(ctypes.byref(fp), _ptr(proj), p, _ptr(gf), _ptr(xin),
+                                        _ptr(xout)), "orc_filter_view_stages")
+    return gf, xin, xout
+
+
+def pisegment(x, y, z):
+    b, t = ctypes.c_double(), ctypes.c_double()
+    lib().orc_pisegment(x, y, z, ctypes.byref(b), ctypes.byref(t))
+    return b.value, t.value
+
+
+def bp_geom(locus, detector, obj, honour_extras=True) -> BPGeom:
+    g = BPGeom()
+    for i, v in enumerate(locus):
+        g.locus[i] = v
+    for i, v in enumerate(detector):
+        g.detector[i] = v
+    for i, v in enumerate(obj):
+        g.object[i] = v
+    g.n_detector = len(detector)
+    g.n_object = len(obj)
+    g.honour_extras = 1 if honour_extras else 0
+    return g
+
+
+def _vol_shape(g: BPGeom):
+    return int(g.object[1]), int(g.object[2]), int(g.object[3])
+
+
+def bkproj(g: BPGeom, fproj: np.ndarray, image: np.ndarray | None = None, x_range=(0, 0),
+           z_range=(0, 0), nthreads=0, want_touched=False):
+    """KatsevichBkProj.cpp restated. Returns (image, n_updates[, touched])."""
+    fproj = np.ascontiguousarray(fproj, dtype=np.float64)
+    if image is None:
+        image = np.zeros(_vol_shape(g))
+    assert image.dtype == np.float64 and image.flags.c_contiguous
+    n = ctypes.c_longlong()
+    touched = np.zeros(_vol_shape(g), np.uint8) if want_touched else None
+    rc = lib().orc_bkproj(ctypes.byref(g), _ptr(fproj), _ptr(image), x_range[0], x_range[1],
+                          z_range[0], z_range[1], nthreads, ctypes.byref(n),
+                          _ptr(touched, _up) if touched is not None else None)
+    _check(rc, "orc_bkproj")
+    if want_touched:
+        return image, n.value, touched
+    return image, n.value
+
+
+def pi_table(g: BPGeom, nthreads=0):
+    shp = _vol_shape(g)
+    B, T = np.zeros(shp), np.zeros(shp)
+    lb, le = np.zeros(shp, np.int32), np.zeros(shp, np.int32)
+    valid = np.zeros(shp, np.uint8)
+    _check(lib().orc_pi_table(ctypes.byref(g), _ptr(B), _ptr(T), _ptr(lb, _ip), _ptr(le, _ip),
+                              _ptr(valid, _up), nthreads), "orc_pi_table")
+    return dict(B=B, T=T, loop_begin=lb, loop_end=le, valid=valid.astype(bool))
+
+
+def project_ellipsoids(g: BPGeom, ell: np.ndarray, p_begin=0, p_end=0, nthreads=0):
+    P = int(g.locus[5]) - int(g.locus[4]) + 1
+    YL, ZL = int(g.detector[1]), int(g.detector[3])
+    ell = np.ascontiguousarray(ell, dtype=np.float64).reshape(-1, 10)
+    proj = np.zeros((P, ZL, YL))
+    _check(lib().orc_project_ellipsoids(ctypes.byref(g), _ptr(ell), ell.shape[0], _ptr(proj),
+                                        p_begin, p_end, nthreads), "orc_project_ellipsoids")
+    return proj
+
+
+# ---------------------------------------------------------------------------------------
+def ref_available() -> bool:
+    return os.path.exists(REF_BKPROJ_PATH)
+
+
+def ref_bkproj(geom: dict, fproj: np.ndarray, image: np.ndarray):
+    """Run the reference's own KatsevichBkProj.cpp mexFunction (in place on `image`)."""
+    import sys
+    root = os.path.dirname(HERE)
+    if root not in sys.path:
+        sys.path.insert(0, root)
+    from ctrecon_b200.mexharness import MexModule
+    m = MexModule(REF_BKPROJ_PATH)
+    m.set_print(False)
+    m.call([geom, fproj, image], nlhs=0)
+    return image
