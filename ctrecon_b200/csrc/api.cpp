@@ -54,6 +54,7 @@ Status get_filter_plan(ctrecon_ctx* ctx, const ctrecon_filter_params& p, FilterP
     }
     ctx->fplan_valid = false;
     plan.p = p;
+    plan.tc_mode = -1;
     CTR_TRY(build_filter_tables(p, plan.t));
     const FilterTables& t = plan.t;
     plan.YLp = (t.YL + 63) / 64 * 64;
@@ -148,6 +149,17 @@ static ctrecon_status finish(ctrecon_ctx* ctx, const Status& s) {
 
 static Status use_device(ctrecon_ctx* ctx) {
     CTR_CUDA(cudaSetDevice(ctx->device));
+    return Status::Ok();
+}
+
+// After a synchronisation: the device error word is set by a bounded wait that gave up.
+static Status check_device_flag(ctrecon_ctx* ctx) {
+    if (!ctx->ws_flag.ptr) return Status::Ok();
+    int flag = 0;
+    CTR_CUDA(cudaMemcpy(&flag, ctx->ws_flag.ptr, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flag)
+        return make_status(CTRECON_ERR_TIMEOUT, "a device-side wait gave up (code " +
+                                                    std::to_string(flag) + ")");
     return Status::Ok();
 }
 
@@ -398,6 +410,19 @@ ctrecon_status ctrecon_phantom_project_dev(ctrecon_ctx* ctx, void* stream,
     API_END(ctx)
 }
 
+ctrecon_status ctrecon_sync(ctrecon_ctx* ctx, void* stream) {
+    if (!ctx) return CTRECON_ERR_INVALID_ARGUMENT;
+    API_BEGIN
+    Status s = use_device(ctx);
+    if (s.ok()) {
+        cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);
+        if (e != cudaSuccess) s = cuda_status(e, "cudaStreamSynchronize");
+    }
+    if (s.ok()) s = check_device_flag(ctx);
+    return finish(ctx, s);
+    API_END(ctx)
+}
+
 // ---- host (FP64, MEX-equivalent) entry points -----------------------------------------------
 static Status host_filter_to_device(ctrecon_ctx* ctx, const ctrecon_filter_params& p,
                                     const double* proj, float** d_fproj_out) {
@@ -435,7 +460,7 @@ static Status host_bkproj_from_device(ctrecon_ctx* ctx, BPPlan& plan, const floa
                                  ctx->ws_d.as<double>()));
     CTR_CUDA(cudaMemcpyAsync(image, ctx->ws_d.ptr, nvox * sizeof(double), cudaMemcpyDeviceToHost, st));
     CTR_CUDA(cudaStreamSynchronize(st));
-    return Status::Ok();
+    return check_device_flag(ctx);
 }
 
 ctrecon_status ctrecon_filter_host_f64(ctrecon_ctx* ctx, const ctrecon_filter_params* p,
@@ -455,6 +480,7 @@ ctrecon_status ctrecon_filter_host_f64(ctrecon_ctx* ctx, const ctrecon_filter_pa
         if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->host_stream);
         if (e != cudaSuccess) s = cuda_status(e, "filter result copy");
     }
+    if (s.ok()) s = check_device_flag(ctx);
     return finish(ctx, s);
     API_END(ctx)
 }

@@ -16,6 +16,8 @@
 // between K1 and K2.
 #include "internal.h"
 
+#include <cuda_bf16.h>
+
 #include <algorithm>
 
 namespace ctr {
@@ -23,19 +25,37 @@ namespace ctr {
 // ---------------------------------------------------------------------------------------------
 // K1
 // ---------------------------------------------------------------------------------------------
+// Output formats of the kappa rows: FP32 (SIMT Hilbert), BF16 hi and lo planes (BF16x3
+// tensor-core Hilbert; the lo plane starts `plane` elements after the hi plane), or FP32
+// rounded to TF32 (round to nearest) for the TF32 tensor-core Hilbert.
+__device__ __forceinline__ void store_kappa(void* X, size_t idx, size_t plane, float v, int mode) {
+    if (mode == CTRECON_HILBERT_BF16X3) {
+        __nv_bfloat16 hi = __float2bfloat16_rn(v);
+        __nv_bfloat16 lo = __float2bfloat16_rn(v - __bfloat162float(hi));
+        static_cast<__nv_bfloat16*>(X)[idx] = hi;
+        static_cast<__nv_bfloat16*>(X)[idx + plane] = lo;
+    } else if (mode == CTRECON_HILBERT_TF32) {
+        uint32_t r;
+        asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(v));
+        static_cast<float*>(X)[idx] = __uint_as_float(r);
+    } else {
+        static_cast<float*>(X)[idx] = v;
+    }
+}
+
 __global__ void k_deriv_rebin(const float* __restrict__ proj, int proj_view0, int P, int YL,
                               int ZL, int AL, int YLp, int vbeg,
                               const FwEntry* __restrict__ fw, const float2* __restrict__ cuy,
                               const float* __restrict__ zcv, float inv2dl,
-                              float* __restrict__ X) {
+                              void* __restrict__ X, size_t plane, int mode) {
     extern __shared__ float gf[];  // ZL x blockDim.x, each thread owns one column
     const int T = blockDim.x, tid = threadIdx.x;
     const int j = blockIdx.x * T + tid;
     const int p = vbeg + blockIdx.y;
-    float* Xv = X + (size_t)blockIdx.y * AL * YLp;
+    const size_t xv = (size_t)blockIdx.y * AL * YLp;
     if (j >= YLp) return;
     if (j >= YL) {  // zero padding of the kappa rows (the GEMM form reads K = YLp)
-        for (int a = 0; a < AL; ++a) Xv[(size_t)a * YLp + j] = 0.f;
+        for (int a = 0; a < AL; ++a) store_kappa(X, xv + (size_t)a * YLp + j, plane, 0.f, mode);
         return;
     }
     const size_t S = (size_t)YL * ZL;
@@ -61,7 +81,8 @@ __global__ void k_deriv_rebin(const float* __restrict__ proj, int proj_view0, in
     }
     for (int a = 0; a < AL; ++a) {
         const FwEntry f = fw[(size_t)a * YL + j];
-        Xv[(size_t)a * YLp + j] = fmaf(f.wa, gf[f.r0 * T + tid], f.wb * gf[f.r1 * T + tid]);
+        store_kappa(X, xv + (size_t)a * YLp + j, plane,
+                    fmaf(f.wa, gf[f.r0 * T + tid], f.wb * gf[f.r1 * T + tid]), mode);
     }
 }
 
@@ -176,11 +197,8 @@ Status launch_convert_f32_to_f64(cudaStream_t s, const float* in, double* out, s
 }
 
 // implemented in hilbert_tc.cu
-Status launch_hilbert_tc(ctrecon_ctx* ctx, cudaStream_t s, FilterPlan& plan, const void* Xsplit,
+Status launch_hilbert_tc(ctrecon_ctx* ctx, cudaStream_t s, FilterPlan& plan, const void* X,
                          int nviews, float* d_fproj_chunk, int mode);
-size_t hilbert_tc_kappa_bytes(const FilterPlan& plan, int nviews, int mode);
-Status launch_split_kappa(cudaStream_t s, const FilterPlan& plan, const float* X, int nviews,
-                          void* Xsplit, int mode);
 
 // ---------------------------------------------------------------------------------------------
 // Orchestration: views [view_begin, view_end) of a projection buffer holding views
@@ -195,12 +213,13 @@ Status launch_filter(ctrecon_ctx* ctx, cudaStream_t s, FilterPlan& plan, const f
     (void)proj_nviews;
     const int mode = ctx->opt_hilbert;
     const int chunk = std::max(1, ctx->opt_filter_chunk);
-    const size_t kappa_f32 = (size_t)chunk * AL * YLp * sizeof(float);
-    size_t need = kappa_f32;
-    if (mode != CTRECON_HILBERT_FP32) need += hilbert_tc_kappa_bytes(plan, chunk, mode);
-    CTR_TRY(ctx->ws_kappa.ensure(need, "filter kappa-row chunk"));
-    float* X = ctx->ws_kappa.as<float>();
-    void* Xs = (char*)ctx->ws_kappa.ptr + kappa_f32;
+    // 4 bytes per kappa sample in every format (FP32, TF32, or BF16 hi + lo planes)
+    CTR_TRY(ctx->ws_kappa.ensure((size_t)chunk * AL * YLp * sizeof(float), "filter kappa rows"));
+    void* X = ctx->ws_kappa.ptr;
+    if (mode != CTRECON_HILBERT_FP32) {
+        CTR_TRY(ctx->ws_flag.ensure(256, "device error word"));
+        CTR_CUDA(cudaMemsetAsync(ctx->ws_flag.ptr, 0, sizeof(int), s));
+    }
 
     // K1 launch shape: one thread per column, ZL floats of shared memory per thread
     int tj = 128;
@@ -225,20 +244,20 @@ Status launch_filter(ctrecon_ctx* ctx, cudaStream_t s, FilterPlan& plan, const f
     for (int c0 = view_begin; c0 < view_end; c0 += chunk) {
         const int n = std::min(chunk, view_end - c0);
         dim3 g1((YLp + tj - 1) / tj, n);
+        const size_t plane = (size_t)n * AL * YLp;
         k_deriv_rebin<<<g1, tj, smem1, s>>>(d_proj, proj_view0, P, YL, ZL, AL, YLp, c0,
                                             plan.fw.as<FwEntry>(), plan.cuy.as<float2>(),
-                                            plan.zcv.as<float>(), plan.inv2dl, X);
+                                            plan.zcv.as<float>(), plan.inv2dl, X, plane, mode);
         CTR_CUDA(cudaGetLastError());
         float* out = d_fproj + (size_t)(c0 - out_view0) * YL * ZL;
         if (mode == CTRECON_HILBERT_FP32) {
             dim3 g2((YL + kTileI - 1) / kTileI, n);
-            k_hilbert_simt<<<g2, nthreads2, smem2, s>>>(X, AL, ALpad, YL, YLp, ZL,
-                                                        plan.h.as<float>(), HOFF,
+            k_hilbert_simt<<<g2, nthreads2, smem2, s>>>(static_cast<const float*>(X), AL, ALpad,
+                                                        YL, YLp, ZL, plan.h.as<float>(), HOFF,
                                                         plan.bk.as<BkEntry>(), out);
             CTR_CUDA(cudaGetLastError());
         } else {
-            CTR_TRY(launch_split_kappa(s, plan, X, n, Xs, mode));
-            CTR_TRY(launch_hilbert_tc(ctx, s, plan, Xs, n, out, mode));
+            CTR_TRY(launch_hilbert_tc(ctx, s, plan, X, n, out, mode));
         }
     }
     return Status::Ok();

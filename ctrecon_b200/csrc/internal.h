@@ -75,6 +75,9 @@ struct FilterPlan {
     int YLp = 0;  // padded row length of the kappa-row buffers (multiple of 64)
     DevBuf fw, bk, cuy, zcv, h;
     float inv2dl = 0;
+    // tensor-core Hilbert operands (Toeplitz hi/lo in BF16, or TF32), built on first use
+    DevBuf tcT0, tcT1;
+    int tc_mode = -1;
 };
 
 // ---- backprojection geometry ----------------------------------------------------------------

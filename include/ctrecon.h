@@ -154,6 +154,10 @@ ctrecon_status ctrecon_bkproj_dev_f32(ctrecon_ctx* ctx, void* stream,
                                       const ctrecon_bp_geom* g, const float* d_fproj,
                                       const void* d_pitab, float* d_image);
 
+/* Waits for the work enqueued on `stream` and reports device-side failures: a CUDA error,
+ * or CTRECON_ERR_TIMEOUT when a bounded wait inside a kernel gave up. */
+ctrecon_status ctrecon_sync(ctrecon_ctx* ctx, void* stream);
+
 /* ---- tables and helpers (host only, no GPU needed) --------------------------------------- */
 
 /* Number of kappa lines AL = 2*ceil(0.65*ZL)+1 (KatsevichFiltering.m:103-104). */

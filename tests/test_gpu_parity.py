@@ -82,6 +82,34 @@ def test_filter_matches_oracle(ctx, tiny_case, c1_case, case):
     assert err < 1e-5
 
 
+@pytest.mark.parametrize("mode,bound", [("bf16x3", 5e-5), ("tf32", 5e-3)])
+@pytest.mark.parametrize("case", ["tiny", "c1"])
+def test_filter_tensor_core_matches_oracle(torch_mod, tiny_case, c1_case, case, mode, bound):
+    """Toeplitz-GEMM Hilbert on tcgen05: BF16x3 must stay near FP32; TF32 is reported."""
+    import ctrecon_b200 as ct
+    c = tiny_case if case == "tiny" else c1_case
+    s = c["s"]
+    m = ct.HILBERT_BF16X3 if mode == "bf16x3" else ct.HILBERT_TF32
+    with ct.Context(0, hilbert=m) as cx:
+        out = cx.filter_host(ct.scan_filter_params(s), c["proj"])
+    err = rel_rmse(out, c["fproj"])
+    print(f"filter {case} {mode}: rel RMSE {err:.3e} max-abs {max_abs(out, c['fproj']):.3e}")
+    assert err < bound
+
+
+def test_chain_c1_bf16x3_matches_oracle(torch_mod, c1_case):
+    import ctrecon_b200 as ct
+    s = c1_case["s"]
+    img = np.full(s.vol_shape, SENTINEL)
+    with ct.Context(0, hilbert=ct.HILBERT_BF16X3) as cx:
+        cx.recon_host(ct.scan_filter_params(s), s.geom_struct(), c1_case["proj"], img)
+    t = c1_case["touched"]
+    assert np.array_equal(img[~t], c1_case["img"][~t])
+    err = rel_rmse(img, c1_case["img"], t)
+    print(f"chain c1 bf16x3: rel RMSE {err:.3e}")
+    assert err < 1e-4
+
+
 def test_filter_device_path_equals_host_path(ctx, torch_mod, tiny_case):
     import ctrecon_b200 as ct
     torch = torch_mod
