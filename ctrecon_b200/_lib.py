@@ -66,6 +66,7 @@ SIGNATURES = [
     ("ctrecon_pi_table_bytes", _st, [ctypes.POINTER(BPGeom), ctypes.POINTER(ctypes.c_size_t)]),
     ("ctrecon_pi_dev", _st, [_vp, _vp, ctypes.POINTER(BPGeom), _vp, _vp]),
     ("ctrecon_bkproj_dev_f32", _st, [_vp, _vp, ctypes.POINTER(BPGeom), _vp, _vp, _vp]),
+    ("ctrecon_filter_noalloc_dev_f32", _st, [_vp, ctypes.POINTER(FilterParams), _vp, _vp]),
     ("ctrecon_sync", _st, [_vp, _vp]),
     ("ctrecon_num_kappa", ctypes.c_int, [ctypes.c_int]),
     ("ctrecon_filter_tables", _st, [ctypes.POINTER(FilterParams), _ip, _ip, _dp, _dp, _ip, _ip,

@@ -123,6 +123,11 @@ using namespace ctr;
 
 static thread_local std::string g_noctx_error;
 
+namespace ctr {
+// the message ctrecon_last_error(NULL) returns, for entry points that take no context
+void set_noctx_error(const std::string& m) { g_noctx_error = m; }
+}  // namespace ctr
+
 static ctrecon_status finish(ctrecon_ctx* ctx, const Status& s) {
     if (!s.ok()) {
         if (ctx) ctx->last_error = s.msg;

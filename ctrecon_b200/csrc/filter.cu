@@ -263,4 +263,43 @@ Status launch_filter(ctrecon_ctx* ctx, cudaStream_t s, FilterPlan& plan, const f
     return Status::Ok();
 }
 
+// The FP32 filter over all views with caller-placed device tables and kappa-row scratch
+// (`chunk` views of AL*YLp floats), for the entry point that allocates nothing (noalloc.cu).
+Status launch_filter_fp32_preplaced(cudaStream_t s, const FilterTables& t, int YLp,
+                                    const FwEntry* fw, const BkEntry* bk, const float2* cuy,
+                                    const float* zcv, const float* hpad, float inv2dl,
+                                    float* kappa, int chunk, const float* d_proj,
+                                    float* d_fproj) {
+    const int YL = t.YL, ZL = t.ZL, AL = t.AL, P = t.P;
+    int tj = 128;
+    while (tj > 32 && (size_t)ZL * tj * sizeof(float) > 96 * 1024) tj /= 2;
+    const size_t smem1 = (size_t)ZL * tj * sizeof(float);
+    if (smem1 > 200 * 1024)
+        return make_status(CTRECON_ERR_UNSUPPORTED, "too many detector rows for K1");
+    CTR_CUDA(cudaFuncSetAttribute(k_deriv_rebin, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)smem1));
+    const int ALpad = (AL + kRA - 1) / kRA * kRA;
+    const int nthreads2 = std::max(32, (ALpad / kRA) * 8);
+    if (nthreads2 > 1024)
+        return make_status(CTRECON_ERR_UNSUPPORTED, "too many kappa lines for the FP32 filter");
+    const int HOFF = YLp + 64;
+    const size_t smem2 = (2 * (size_t)HOFF + (size_t)ALpad * kXS) * sizeof(float);
+    if (smem2 > 227 * 1024)
+        return make_status(CTRECON_ERR_UNSUPPORTED, "detector too wide for the FP32 filter");
+    CTR_CUDA(cudaFuncSetAttribute(k_hilbert_simt, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)smem2));
+    for (int c0 = 0; c0 < P; c0 += chunk) {
+        const int n = std::min(chunk, P - c0);
+        dim3 g1((YLp + tj - 1) / tj, n);
+        k_deriv_rebin<<<g1, tj, smem1, s>>>(d_proj, 0, P, YL, ZL, AL, YLp, c0, fw, cuy, zcv,
+                                            inv2dl, kappa, 0, CTRECON_HILBERT_FP32);
+        CTR_CUDA(cudaGetLastError());
+        dim3 g2((YL + kTileI - 1) / kTileI, n);
+        k_hilbert_simt<<<g2, nthreads2, smem2, s>>>(kappa, AL, ALpad, YL, YLp, ZL, hpad, HOFF, bk,
+                                                    d_fproj + (size_t)c0 * YL * ZL);
+        CTR_CUDA(cudaGetLastError());
+    }
+    return Status::Ok();
+}
+
 }  // namespace ctr

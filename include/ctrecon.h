@@ -154,6 +154,21 @@ ctrecon_status ctrecon_bkproj_dev_f32(ctrecon_ctx* ctx, void* stream,
                                       const ctrecon_bp_geom* g, const float* d_fproj,
                                       const void* d_pitab, float* d_image);
 
+/* The plain FP32 filter (same result as ctrecon_filter_dev_f32 with CTRECON_HILBERT_FP32) for
+ * callers that cannot allocate GPU memory -- e.g. a plug-in inside an application that owns all
+ * device allocations, or a real-time loop that forbids cudaMalloc after start-up. No
+ * counterpart in the reference: it is an addition of this library. It allocates nothing and
+ * needs no context: its tables and kappa-row scratch live in one fixed 16 MiB device array of
+ * the library (held by every GPU that loads the library, until exit); sizes that do not fit
+ * (tables + one view of kappa rows > 16 MiB) return CTRECON_ERR_UNSUPPORTED with the sizes
+ * in ctrecon_last_error(NULL). The caller passes the input and output buffers (distinct) and
+ * a stream; the call is stream-ordered. The first call on a device looks up the array's
+ * device address (cudaGetSymbolAddress) with that device current; make that first call
+ * before any stream capture. Every call shares the array, so calls that overlap on the GPU
+ * (concurrent streams, or several host threads) race; serialise them. */
+ctrecon_status ctrecon_filter_noalloc_dev_f32(void* stream, const ctrecon_filter_params* p,
+                                              const float* d_proj, float* d_fproj);
+
 /* Waits for the work enqueued on `stream` and reports device-side failures: a CUDA error,
  * or CTRECON_ERR_TIMEOUT when a bounded wait inside a kernel gave up. */
 ctrecon_status ctrecon_sync(ctrecon_ctx* ctx, void* stream);
