@@ -36,8 +36,11 @@ sys.path.insert(0, ROOT)
 
 from ctrecon_b200.geometry import config  # noqa: E402
 
-WORKLOAD_NAME = ("katsevich_helical_512x512x256_det64x736_9280views_"
-                 "40ellipsoids_poisson1e5")
+def workload_name(s):
+    """e.g. katsevich_helical_512x512x256_det64x736_9280views_40ellipsoids_poisson1e5"""
+    noise = f"_poisson{s.photons:.0e}".replace("+0", "").replace("+", "") if s.photons else ""
+    return (f"katsevich_helical_{s.NX}x{s.NY}x{s.NZ}_det{s.ZL}x{s.YL}_{s.P}views_"
+            f"{s.n_ellipsoids}ellipsoids{noise}")
 METRIC = "Katsevich 512^3 recon GUPS & s/vol: plain FP32 vs mixed+learned @ equal RMSE"
 BYTES_PER_UPDATE = 16  # four FP32 bilinear taps (KatsevichBkProj.cpp:253-256)
 
@@ -51,6 +54,10 @@ def parse():
     ap.add_argument("--config", default="c2")
     ap.add_argument("--hilbert", default="fp32", choices=["fp32", "bf16x3", "tf32"])
     ap.add_argument("--pi", default="bisect", choices=["bisect", "newton", "learned"])
+    ap.add_argument("--bp-variant", type=int, default=0,
+                    help="backprojector form: 0-2 second form tile shapes, 100 first form")
+    ap.add_argument("--batched", action="store_true",
+                    help="16 uneven scans (c4): one-at-a-time vs one batched graph replay")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     return ap.parse_args()
@@ -281,7 +288,7 @@ def run_reference(args):
             "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": t_scan * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD_NAME, "volume": list(s.vol_shape),
+            "config": {"workload": workload_name(s), "volume": list(s.vol_shape),
                        "detector": [s.ZL, s.YL], "views": s.P},
             "cpu_baseline": {"value": gups, "unit": "GUPS", "cores": cores,
                              "kind": "reference", "sample": sample},
@@ -314,11 +321,88 @@ def _full_update_count(s):
     return int(np.sum(t["loop_end"][v] - t["loop_begin"][v] + 1))
 
 
+def run_batched(args):
+    """c4: 16 helical scans of uneven size. Times the one-at-a-time chain (filter, PI solve,
+    backprojection per scan) and the batched form (one persistent backprojection launch over
+    all scans, replayed as a CUDA graph); value = aggregate GUPS of the batched form."""
+    import torch
+    import ctrecon_b200 as ct
+    from ctrecon_b200 import _lib
+    from ctrecon_b200.geometry import batch_configs
+    scans = batch_configs()
+    hil = {"fp32": _lib.HILBERT_FP32, "bf16x3": _lib.HILBERT_BF16X3,
+           "tf32": _lib.HILBERT_TF32}[args.hilbert]
+    pis = {"bisect": _lib.PI_BISECT, "newton": _lib.PI_NEWTON, "learned": _lib.PI_LEARNED}[args.pi]
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):
+        ctx = ct.Context(0, hilbert=hil, pi_solver=_lib.PI_BISECT)
+        ctx.set_option(_lib.OPT_BP_VARIANT, args.bp_variant)
+        if pis == _lib.PI_LEARNED:
+            import ctypes
+            loss = ctypes.c_float()
+            _lib.check(_lib.lib().ctrecon_pinet_train(ctx.handle, stream.cuda_stream, 1 << 22, 8192, 8,
+                                                      0.21, 2024, ctypes.byref(loss)), ctx.handle)
+        projs, fprojs, imgs = [], [], []
+        for s in scans:
+            d = torch.empty(s.proj_shape, dtype=torch.float32, device="cuda")
+            ctx.phantom_dev(s.geom_struct(), s.ellipsoids(), d, photons=s.photons or 0.0, seed=s.seed)
+            projs.append(d)
+            fprojs.append(torch.empty_like(d))
+            imgs.append(torch.zeros(s.vol_shape, dtype=torch.float32, device="cuda"))
+        b = ct.Batch(ctx, scans)
+        b.set_variant(args.bp_variant if args.bp_variant < 100 else 0)
+        updates = b.updates()
+        ctx.set_option(_lib.OPT_PI_SOLVER, pis)
+        total = sum(updates)
+
+        def one_at_a_time():
+            for s, d, f, im in zip(scans, projs, fprojs, imgs):
+                ctx.filter_dev(ct.scan_filter_params(s), d, f)
+                ctx.bkproj_dev(s.geom_struct(), f, im)  # PI solved inside (context table)
+
+        def timed(fn, k):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            stream.synchronize()
+            e0.record(stream)
+            for _ in range(k):
+                fn()
+            e1.record(stream)
+            stream.synchronize()
+            return e0.elapsed_time(e1) / k
+
+        for _ in range(max(3, args.warmup)):
+            one_at_a_time()
+            b.run(projs, fprojs, imgs, use_graph=True)
+        sampler = ClockSampler(0)
+        sampler.start()
+        ms_seq = timed(one_at_a_time, args.steps)
+        ms_bat = timed(lambda: b.run(projs, fprojs, imgs, use_graph=True), args.steps)
+        clocks = sampler.stop()
+        b.close()
+        ctx.close()
+    line = {"metric": METRIC, "value": total / (ms_bat / 1e3) / 1e9, "unit": "GUPS",
+            "n_gpus": 1, "steps": args.steps, "warmup": max(3, args.warmup),
+            "ms_per_step": ms_bat, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "c4_batch_16_uneven_helical_scans", "scans": len(scans),
+                       "volumes": [list(s.vol_shape) for s in scans],
+                       "detectors": [[s.ZL, s.YL] for s in scans], "views": [s.P for s in scans],
+                       "hilbert": args.hilbert, "pi_solver": args.pi, "graph": True,
+                       "l2": "inputs larger than L2 (40 GB of projections and volumes)"},
+            "updates_per_step": total,
+            "one_at_a_time": {"ms_per_step": ms_seq, "gups": total / (ms_seq / 1e3) / 1e9},
+            "batched_speedup": ms_seq / ms_bat, "clocks": clocks}
+    print(json.dumps(line))
+
+
 # ---------------------------------------------------------------------------------------------
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.batched:
+        run_batched(args)
         return
     import torch
     import ctrecon_b200 as ct
@@ -330,9 +414,20 @@ def main():
     hil = {"fp32": _lib.HILBERT_FP32, "bf16x3": _lib.HILBERT_BF16X3,
            "tf32": _lib.HILBERT_TF32}[args.hilbert]
     pis = {"bisect": _lib.PI_BISECT, "newton": _lib.PI_NEWTON, "learned": _lib.PI_LEARNED}[args.pi]
-    ctx = ct.Context(local, hilbert=hil, pi_solver=pis)
+    ctx = ct.Context(local, hilbert=hil, pi_solver=_lib.PI_BISECT)
+    ctx.set_option(_lib.OPT_BP_VARIANT, args.bp_variant)
     geom = s.geom_struct()
     fpar = ct.scan_filter_params(s)
+    pinet_info = None
+    if pis == _lib.PI_LEARNED:
+        import ctypes
+        loss = ctypes.c_float()
+        t0 = time.perf_counter()
+        _lib.check(_lib.lib().ctrecon_pinet_train(
+            ctx.handle, torch.cuda.current_stream().cuda_stream, 1 << 22, 8192, 8,
+            s.ObjR / s.ScanR * 1.05, 2024, ctypes.byref(loss)), ctx.handle)
+        pinet_info = {"train_pairs": 1 << 22, "epochs": 8, "train_s": time.perf_counter() - t0,
+                      "final_loss": loss.value}
 
     # ---- inputs, resident in HBM before timing --------------------------------------------------
     d_proj = torch.empty(s.proj_shape, dtype=torch.float32, device=dev)
@@ -428,7 +523,7 @@ def main():
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_source": peak_kind,
                 "kernel": "k_bkproj", "model": "16 B per voxel-view update",
-                "traffic": load_traffic("k_bkproj", WORKLOAD_NAME)}
+                "traffic": load_traffic("k_bkproj", workload_name(s))}
 
     # ---- CPU baseline (rank 0, N = 1): the FP64 oracle restatement on a bounded sample -----------
     cpu = None
@@ -459,15 +554,17 @@ def main():
                 "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": ms_step,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f32", "data": "synthetic",
-                "config": {"workload": WORKLOAD_NAME, "volume": list(s.vol_shape),
+                "config": {"workload": workload_name(s), "volume": list(s.vol_shape),
                            "voxel_mm": list(s.voxel_size), "detector": [s.ZL, s.YL],
                            "views": s.P, "views_per_turn": s.views_per_turn,
                            "hilbert": args.hilbert, "pi_solver": args.pi,
+                           "bp_variant": args.bp_variant,
                            "parallelism": f"replicas{ws}",
                            "l2": "inputs larger than L2 (projections 1.75 GB)"},
                 "updates_per_step": updates, "s_per_vol": ms_step / 1e3,
                 "phase_ms": {"filter": filt_ms, "pi": pi_ms, "bkproj": bp_ms},
                 "bkproj_gups": updates / (bp_ms / 1e3) / 1e9,
+                "pinet": pinet_info,
                 "gpu_launches": launches_per_step * args.steps,
                 "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks}
         print(json.dumps(line))

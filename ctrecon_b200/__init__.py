@@ -7,7 +7,7 @@ call that needs it does, and raises if it was not built.
 """
 from ._lib import (HILBERT_BF16X3, HILBERT_FP32, HILBERT_TF32, PI_BISECT, PI_LEARNED, PI_NEWTON,
                    CtreconError)
-from .api import (Context, KatsevichBkProj, KatsevichBkProj_GPU, KatsevichFiltering_GPU, bp_geom,
+from .api import (Batch, Context, KatsevichBkProj, KatsevichBkProj_GPU, KatsevichFiltering_GPU, bp_geom,
                   default_context, filter_params, filter_tables, geometry_sizing, num_kappa,
                   scan_filter_params)
 

@@ -68,7 +68,25 @@ SIGNATURES = [
     ("ctrecon_bkproj_dev_f32", _st, [_vp, _vp, ctypes.POINTER(BPGeom), _vp, _vp, _vp]),
     ("ctrecon_filter_noalloc_dev_f32", _st, [_vp, ctypes.POINTER(FilterParams), _vp, _vp]),
     ("ctrecon_sync", _st, [_vp, _vp]),
+    ("ctrecon_pi_dev_stats", _st, [_vp, _vp, ctypes.POINTER(BPGeom), _vp, _vp, _vp]),
+    ("ctrecon_batch_create", _st, [_vp, ctypes.c_int, ctypes.POINTER(FilterParams),
+                                   ctypes.POINTER(BPGeom), ctypes.POINTER(_vp)]),
+    ("ctrecon_batch_destroy", None, [_vp]),
+    ("ctrecon_batch_set_variant", _st, [_vp, ctypes.c_int]),
+    ("ctrecon_batch_run_dev", _st, [_vp, _vp, ctypes.POINTER(_vp), ctypes.POINTER(_vp),
+                                    ctypes.POINTER(_vp), ctypes.c_int]),
+    ("ctrecon_batch_updates", _st, [_vp, ctypes.POINTER(ctypes.c_ulonglong)]),
+    ("ctrecon_pinet_num_params", ctypes.c_int, []),
+    ("ctrecon_pinet_train", _st, [_vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                  ctypes.c_double, ctypes.c_uint64,
+                                  ctypes.POINTER(ctypes.c_float)]),
+    ("ctrecon_pinet_get_params", _st, [_vp, ctypes.POINTER(ctypes.c_float), ctypes.c_int]),
+    ("ctrecon_pinet_set_params", _st, [_vp, ctypes.POINTER(ctypes.c_float), ctypes.c_int,
+                                       ctypes.c_double]),
+    ("ctrecon_pinet_loss_grad", _st, [_vp, _vp, _vp, _vp, ctypes.c_int, _vp, _vp]),
+    ("ctrecon_pinet_predict", _st, [_vp, _vp, _vp, ctypes.c_int, _vp]),
     ("ctrecon_num_kappa", ctypes.c_int, [ctypes.c_int]),
+    ("ctrecon_find_tau", _st, [ctypes.c_double, ctypes.c_double, _dp]),
     ("ctrecon_filter_tables", _st, [ctypes.POINTER(FilterParams), _ip, _ip, _dp, _dp, _ip, _ip,
                                     _dp, _dp]),
     ("ctrecon_geometry_sizing", None, [ctypes.c_double] * 4 + [ctypes.c_int] * 2 + [_dp] * 3),

@@ -232,6 +232,47 @@ class Context:
             self._h)
 
 
+class Batch:
+    """Many scans reconstructed together (ctrecon_batch_*): per-scan filters and PI solves, one
+    persistent backprojection launch over all scans, optionally replayed as a CUDA graph."""
+
+    def __init__(self, ctx: Context, scans):
+        self.ctx = ctx
+        self.n = len(scans)
+        fps = (FilterParams * self.n)(*[scan_filter_params(s) for s in scans])
+        gs = (BPGeom * self.n)(*[bp_geom(s.geom_struct()) for s in scans])
+        h = ctypes.c_void_p()
+        check(lib().ctrecon_batch_create(ctx.handle, self.n, fps, gs, ctypes.byref(h)), ctx.handle)
+        self._h = h
+
+    def close(self):
+        if self._h:
+            lib().ctrecon_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_variant(self, variant: int):
+        check(lib().ctrecon_batch_set_variant(self._h, int(variant)), self.ctx.handle)
+
+    def run(self, d_projs, d_fprojs, d_images, stream=None, use_graph=True):
+        arr = lambda ts, name, dt: (ctypes.c_void_p * self.n)(*[_tptr(t, dt, name) for t in ts])
+        check(lib().ctrecon_batch_run_dev(self._h, _stream_handle(stream),
+                                          arr(d_projs, "d_proj", "float32"),
+                                          arr(d_fprojs, "d_fproj", "float32"),
+                                          arr(d_images, "d_image", "float32"),
+                                          1 if use_graph else 0), self.ctx.handle)
+
+    def updates(self):
+        out = (ctypes.c_ulonglong * self.n)()
+        check(lib().ctrecon_batch_updates(self._h, out), self.ctx.handle)
+        return [int(v) for v in out]
+
+
 _default: Optional[Context] = None
 
 

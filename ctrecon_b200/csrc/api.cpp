@@ -53,6 +53,13 @@ Status get_filter_plan(ctrecon_ctx* ctx, const ctrecon_filter_params& p, FilterP
         return Status::Ok();
     }
     ctx->fplan_valid = false;
+    CTR_TRY(build_filter_plan(p, plan));
+    ctx->fplan_valid = true;
+    *out = &plan;
+    return Status::Ok();
+}
+
+Status build_filter_plan(const ctrecon_filter_params& p, FilterPlan& plan) {
     plan.p = p;
     plan.tc_mode = -1;
     CTR_TRY(build_filter_tables(p, plan.t));
@@ -77,8 +84,6 @@ Status get_filter_plan(ctrecon_ctx* ctx, const ctrecon_filter_params& p, FilterP
     CTR_TRY(upload(plan.zcv, zcv, "derivative coefficients"));
     CTR_TRY(upload(plan.h, hpad, "Hilbert taps"));
     plan.inv2dl = (float)(1.0 / (2 * t.DeltaL));
-    ctx->fplan_valid = true;
-    *out = &plan;
     return Status::Ok();
 }
 
@@ -94,6 +99,13 @@ Status get_bp_plan(ctrecon_ctx* ctx, const ctrecon_bp_geom& gin, BPPlan** out) {
         return Status::Ok();
     }
     ctx->bplan_valid = false;
+    CTR_TRY(build_bp_plan(g, plan));
+    ctx->bplan_valid = true;
+    *out = &plan;
+    return Status::Ok();
+}
+
+Status build_bp_plan(const BPGeom& g, BPPlan& plan) {
     plan.g = g;
     plan.kp = make_bp_params(g);
     const double PI = kRefPi;
@@ -109,8 +121,6 @@ Status get_bp_plan(ctrecon_ctx* ctx, const ctrecon_bp_geom& gin, BPPlan** out) {
     for (int i = 0; i < g.NZ; ++i) xyz[(size_t)g.NX + g.NY + i] = (float)((i - g.ZC) * g.dz);
     CTR_TRY(upload(plan.views, views, "view geometry"));
     CTR_TRY(upload(plan.xyz, xyz, "voxel coordinates"));
-    ctx->bplan_valid = true;
-    *out = &plan;
     return Status::Ok();
 }
 
@@ -276,6 +286,25 @@ ctrecon_status ctrecon_get_option(const ctrecon_ctx* ctx, ctrecon_option opt, in
 }
 
 int ctrecon_num_kappa(int zl) { return 2 * (int)std::ceil(zl * 1.3 * 0.5) + 1; }
+
+ctrecon_status ctrecon_find_tau(double ratio, double tol, double* tau) {
+    if (!tau || !(ratio > 0 && ratio < 1) || !(tol > 0))
+        return finish(nullptr, make_status(CTRECON_ERR_INVALID_ARGUMENT,
+                                           "find_tau: need 0 < ratio < 1 and tol > 0"));
+    const double pi = 3.141592653589793;  // MATLAB's pi (FindTau.m:7 uses the built-in)
+    const double am = 2 * pi - 2 * std::acos(ratio);
+    double tu = 0.5, td = 0, delta = 1, t = 0;
+    int guard = 0;
+    while (delta > tol && guard++ < 200) {  // FindTau.m:13-22
+        t = (td + tu) / 2;
+        const double f = t * std::cos(am) - std::cos(t * am) + 1 - t;
+        delta = std::fabs(f);
+        if (f > 0) tu = t;
+        else td = t;
+    }
+    *tau = t;
+    return CTRECON_OK;
+}
 
 void ctrecon_geometry_sizing(double ScanR, double StdDis, double HelicP, double ObjR, int YL,
                              int ZL, double* DecWidth, double* DecHeigh, double* delta) {

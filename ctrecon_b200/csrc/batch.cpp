@@ -1,0 +1,242 @@
+// batch.cpp -- many helical scans of uneven size reconstructed together.
+//
+// A batch holds one filter plan and one backprojection plan per scan, the PI tables of all
+// scans, and a device array describing every scan to the persistent backprojector
+// (k_bkproj2_batch): per run, the scans' filters and PI solves are enqueued one after the
+// other, then ONE persistent launch backprojects the tiles of all scans, CTAs pulling tiles
+// from a shared counter (scans sorted largest first, so the small ones fill the tail). With
+// use_graph, the first run is executed eagerly (it sizes every work buffer) and the second is
+// captured into a CUDA graph that later runs replay; the graph is re-captured when the buffer
+// pointers change.
+#include "internal.h"
+
+#include <algorithm>
+#include <cstring>
+#include <memory>
+#include <numeric>
+#include <vector>
+
+namespace ctr {
+Status launch_bkproj_batch(int variant, cudaStream_t s, const BatchScanDev* d_scans, int n,
+                           long long total, unsigned long long* d_counter);
+long long bkproj_batch_tiles(const BPParams& kp, int variant);
+Status launch_pi_stats(ctrecon_ctx* ctx, cudaStream_t s, BPPlan& plan, PiRecord* d_pitab,
+                       unsigned long long* d_updates, unsigned long long* d_iters);
+void set_noctx_error(const std::string& m);
+}  // namespace ctr
+
+using namespace ctr;
+
+struct ctrecon_batch {
+    ctrecon_ctx* ctx = nullptr;
+    int n = 0;
+    int variant = 0;
+    std::vector<ctrecon_filter_params> fp;
+    std::vector<std::unique_ptr<FilterPlan>> fplans;
+    std::vector<std::unique_ptr<BPPlan>> bplans;
+    std::vector<int> order;           // scans by decreasing backprojection work
+    std::vector<size_t> pit_off;      // PiRecord offset of each scan in `pitab`
+    DevBuf pitab, scans_dev, counter, updates;
+    long long total_tiles = 0;
+    std::vector<const void*> key;     // pointers the graph was captured with
+    int runs_with_key = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    ~ctrecon_batch() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+    }
+};
+
+static ctrecon_status bfinish(ctrecon_ctx* ctx, const Status& s) {
+    if (!s.ok()) {
+        if (ctx) ctx->last_error = s.msg;
+        else set_noctx_error(s.msg);
+    }
+    return s.code;
+}
+
+static Status enqueue(ctrecon_batch* b, cudaStream_t s, const float* const* d_proj,
+                      float* const* d_fproj, float* const* d_image) {
+    ctrecon_ctx* ctx = b->ctx;
+    for (int k = 0; k < b->n; ++k) {
+        const int i = b->order[k];
+        const int P = b->fp[i].proj_number;
+        CTR_TRY(launch_filter(ctx, s, *b->fplans[i], d_proj[i], 0, P, d_fproj[i], 0, 0, P));
+    }
+    for (int k = 0; k < b->n; ++k) {
+        const int i = b->order[k];
+        CTR_TRY(launch_pi(ctx, s, *b->bplans[i], b->pitab.as<PiRecord>() + b->pit_off[i], nullptr));
+    }
+    return launch_bkproj_batch(b->variant, s, b->scans_dev.as<BatchScanDev>(), b->n,
+                               b->total_tiles, b->counter.as<unsigned long long>());
+}
+
+static Status upload_scans(ctrecon_batch* b, cudaStream_t s, float* const* d_fproj,
+                           float* const* d_image) {
+    std::vector<BatchScanDev> h(b->n);
+    long long first = 0;
+    for (int k = 0; k < b->n; ++k) {
+        const int i = b->order[k];
+        BPPlan& bp = *b->bplans[i];
+        h[k].kp = bp.kp;
+        h[k].fproj = d_fproj[i];
+        h[k].pit = b->pitab.as<PiRecord>() + b->pit_off[i];
+        h[k].views = bp.views.as<float4>();
+        h[k].xyz = bp.xyz.as<float>();
+        h[k].image = d_image[i];
+        h[k].first_tile = first;
+        first += bkproj_batch_tiles(bp.kp, b->variant);
+    }
+    b->total_tiles = first;
+    CTR_TRY(b->scans_dev.ensure(h.size() * sizeof(BatchScanDev), "batch scan table"));
+    CTR_CUDA(cudaMemcpyAsync(b->scans_dev.ptr, h.data(), h.size() * sizeof(BatchScanDev),
+                             cudaMemcpyHostToDevice, s));
+    CTR_CUDA(cudaStreamSynchronize(s));  // `h` is pageable and local
+    return Status::Ok();
+}
+
+extern "C" {
+
+ctrecon_status ctrecon_batch_create(ctrecon_ctx* ctx, int n_scans,
+                                    const ctrecon_filter_params* fp, const ctrecon_bp_geom* g,
+                                    ctrecon_batch** out) {
+    if (!ctx || !fp || !g || !out || n_scans < 1) return CTRECON_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    try {
+        cudaSetDevice(ctx->device);
+        auto b = std::make_unique<ctrecon_batch>();
+        b->ctx = ctx;
+        b->n = n_scans;
+        b->variant = ctx->opt_bp_variant >= 100 ? 0 : ctx->opt_bp_variant;
+        b->fp.assign(fp, fp + n_scans);
+        size_t nvox = 0;
+        std::vector<double> work(n_scans);
+        for (int i = 0; i < n_scans; ++i) {
+            b->fplans.emplace_back(new FilterPlan());
+            b->bplans.emplace_back(new BPPlan());
+            Status s = build_filter_plan(fp[i], *b->fplans[i]);
+            BPGeom bg;
+            std::memset(&bg, 0, sizeof bg);
+            if (s.ok()) s = parse_bp_geom(g[i], bg);
+            if (s.ok() && (bg.YL != fp[i].yl || bg.ZL != fp[i].zl || bg.ProjNum != fp[i].proj_number))
+                s = make_status(CTRECON_ERR_INVALID_ARGUMENT,
+                                "scan " + std::to_string(i) + ": filter and geometry disagree");
+            if (s.ok()) s = build_bp_plan(bg, *b->bplans[i]);
+            if (!s.ok()) return bfinish(ctx, s);
+            b->pit_off.push_back(nvox);
+            nvox += (size_t)bg.NX * bg.NY * bg.NZ;
+            work[i] = (double)bg.NX * bg.NY * bg.NZ * bg.ProjScale;
+        }
+        b->order.resize(n_scans);
+        std::iota(b->order.begin(), b->order.end(), 0);
+        std::stable_sort(b->order.begin(), b->order.end(),
+                         [&](int a, int c) { return work[a] > work[c]; });
+        Status s = b->pitab.ensure(nvox * sizeof(PiRecord), "batch PI tables");
+        if (s.ok()) s = b->counter.ensure(64, "batch work counter");
+        if (s.ok()) s = b->updates.ensure(sizeof(unsigned long long) * n_scans, "batch counts");
+        if (!s.ok()) return bfinish(ctx, s);
+        *out = b.release();
+        return CTRECON_OK;
+    } catch (const std::exception& e) {
+        return bfinish(ctx, make_status(CTRECON_ERR_INTERNAL, e.what()));
+    }
+}
+
+void ctrecon_batch_destroy(ctrecon_batch* b) {
+    if (!b) return;
+    cudaSetDevice(b->ctx->device);
+    delete b;
+}
+
+ctrecon_status ctrecon_batch_set_variant(ctrecon_batch* b, int variant) {
+    if (!b || variant < 0 || variant > 2) return CTRECON_ERR_INVALID_ARGUMENT;
+    if (variant != b->variant) {
+        b->variant = variant;
+        b->key.clear();  // tile counts change: rebuild the scan table and the graph
+    }
+    return CTRECON_OK;
+}
+
+ctrecon_status ctrecon_batch_run_dev(ctrecon_batch* b, void* stream, const float* const* d_proj,
+                                     float* const* d_fproj, float* const* d_image,
+                                     int use_graph) {
+    if (!b || !d_proj || !d_fproj || !d_image) return CTRECON_ERR_INVALID_ARGUMENT;
+    ctrecon_ctx* ctx = b->ctx;
+    try {
+        cudaSetDevice(ctx->device);
+        cudaStream_t s = (cudaStream_t)stream;
+        if (use_graph && !s)
+            return bfinish(ctx, make_status(CTRECON_ERR_INVALID_ARGUMENT,
+                                            "graph replay needs a created stream, not stream 0"));
+        std::vector<const void*> key;
+        for (int i = 0; i < b->n; ++i) {
+            key.push_back(d_proj[i]);
+            key.push_back(d_fproj[i]);
+            key.push_back(d_image[i]);
+        }
+        if (key != b->key) {
+            Status st = upload_scans(b, s, d_fproj, d_image);
+            if (!st.ok()) return bfinish(ctx, st);
+            b->key = key;
+            b->runs_with_key = 0;
+            if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; }
+            if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
+        }
+        Status st;
+        if (!use_graph || b->runs_with_key == 0) {
+            st = enqueue(b, s, d_proj, d_fproj, d_image);
+        } else {
+            if (!b->exec) {
+                cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+                if (e != cudaSuccess) return bfinish(ctx, cuda_status(e, "cudaStreamBeginCapture"));
+                st = enqueue(b, s, d_proj, d_fproj, d_image);
+                cudaGraph_t g = nullptr;
+                e = cudaStreamEndCapture(s, &g);
+                if (st.ok() && e != cudaSuccess) st = cuda_status(e, "cudaStreamEndCapture");
+                if (st.ok()) {
+                    e = cudaGraphInstantiate(&b->exec, g, 0);
+                    if (e != cudaSuccess) st = cuda_status(e, "cudaGraphInstantiate");
+                }
+                b->graph = g;
+                if (!st.ok()) return bfinish(ctx, st);
+            }
+            cudaError_t e = cudaGraphLaunch(b->exec, s);
+            if (e != cudaSuccess) st = cuda_status(e, "cudaGraphLaunch");
+        }
+        if (st.ok()) b->runs_with_key++;
+        return bfinish(ctx, st);
+    } catch (const std::exception& e) {
+        return bfinish(ctx, make_status(CTRECON_ERR_INTERNAL, e.what()));
+    }
+}
+
+ctrecon_status ctrecon_batch_updates(ctrecon_batch* b, unsigned long long* host_updates) {
+    if (!b || !host_updates) return CTRECON_ERR_INVALID_ARGUMENT;
+    ctrecon_ctx* ctx = b->ctx;
+    try {
+        cudaSetDevice(ctx->device);
+        cudaStream_t s = ctx->host_stream;
+        const int saved = ctx->opt_pi;
+        ctx->opt_pi = CTRECON_PI_BISECT;  // the loop count of the reference's own solve
+        Status st;
+        cudaError_t e0 = cudaMemsetAsync(b->updates.ptr, 0, sizeof(unsigned long long) * b->n, s);
+        if (e0 != cudaSuccess) st = cuda_status(e0, "batch counts");
+        for (int i = 0; st.ok() && i < b->n; ++i)
+            st = launch_pi_stats(ctx, s, *b->bplans[i], b->pitab.as<PiRecord>() + b->pit_off[i],
+                                 b->updates.as<unsigned long long>() + i, nullptr);
+        ctx->opt_pi = saved;
+        if (st.ok()) {
+            cudaError_t e = cudaMemcpyAsync(host_updates, b->updates.ptr,
+                                            sizeof(unsigned long long) * b->n,
+                                            cudaMemcpyDeviceToHost, s);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+            if (e != cudaSuccess) st = cuda_status(e, "batch counts");
+        }
+        return bfinish(ctx, st);
+    } catch (const std::exception& e) {
+        return bfinish(ctx, make_status(CTRECON_ERR_INTERNAL, e.what()));
+    }
+}
+
+}  // extern "C"

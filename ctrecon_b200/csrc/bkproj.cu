@@ -227,16 +227,22 @@ static Status launch_bk(cudaStream_t s, BPPlan& plan, const float* d_fproj,
     return Status::Ok();
 }
 
+template <typename OutT>
+Status launch_bkproj_v2(int variant, cudaStream_t s, BPPlan& plan, const float* d_fproj,
+                        const PiRecord* d_pitab, OutT* d_image);
+
+// CTRECON_OPT_BP_VARIANT: 0..2 select tile shapes of the second form (bkproj2.cu), 100 the
+// first form above
 Status launch_bkproj_f32(ctrecon_ctx* ctx, cudaStream_t s, BPPlan& plan, const float* d_fproj,
                          const PiRecord* d_pitab, float* d_image) {
-    (void)ctx;
-    return launch_bk<float>(s, plan, d_fproj, d_pitab, d_image);
+    if (ctx->opt_bp_variant >= 100) return launch_bk<float>(s, plan, d_fproj, d_pitab, d_image);
+    return launch_bkproj_v2<float>(ctx->opt_bp_variant, s, plan, d_fproj, d_pitab, d_image);
 }
 
 Status launch_bkproj_f64out(ctrecon_ctx* ctx, cudaStream_t s, BPPlan& plan,
                             const float* d_fproj, const PiRecord* d_pitab, double* d_image) {
-    (void)ctx;
-    return launch_bk<double>(s, plan, d_fproj, d_pitab, d_image);
+    if (ctx->opt_bp_variant >= 100) return launch_bk<double>(s, plan, d_fproj, d_pitab, d_image);
+    return launch_bkproj_v2<double>(ctx->opt_bp_variant, s, plan, d_fproj, d_pitab, d_image);
 }
 
 }  // namespace ctr

@@ -1,0 +1,381 @@
+// bkproj2.cu -- K4, second form: the same voxel-driven backprojection as bkproj.cu
+// (KatsevichBkProj.cpp:164-265, FP32 interpolation and accumulation, identical endpoint rule),
+// reorganised for issue throughput:
+//
+//  * views are staged in blocks of NB with two shared-memory buffers: while block b is being
+//    accumulated, block b+1's footprints are already in flight (cp.async, one warp per detector
+//    row, no integer division), so each block costs three barriers instead of stalling on loads;
+//  * a thread whose TZ voxels are all strictly inside their PI intervals (away from the two
+//    ramp views at each end) for a whole block takes a branch-free path with unit weights --
+//    the common case; the others take the checked path of bkproj.cu;
+//  * voxel z coordinates are generated, not held in registers, and the launch is bounded to
+//    three CTAs of 256 threads per SM.
+#include "internal.h"
+
+#include <climits>
+
+namespace ctr {
+
+namespace {
+
+constexpr int kTXY2 = 16;
+constexpr int kCap2 = 1024;  // shared floats per staged view
+
+struct Foot2 { int u0, v0, W, H; };
+
+__device__ __forceinline__ float ramp2(float s) {
+    float c = fminf(fmaxf(s, -1.f), 1.f);
+    return 0.5f + c - 0.5f * c * fabsf(c);
+}
+
+// single-instruction reciprocal and reciprocal square root (relative error ~2^-23)
+__device__ __forceinline__ float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float rsqrt_approx(float x) {
+    float r;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+__device__ __forceinline__ void cp_async4(float* dst, const float* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(
+                     (uint32_t)__cvta_generic_to_shared(dst)),
+                 "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+}  // namespace
+
+template <int NB>
+struct BPShared {
+    Foot2 foot[2][NB];
+    float4 vg[2][NB];
+    int s_pmin, s_pmax, s_item;
+};
+
+// One CTA tile: columns [16 bx, 16 bx + 16) x [16 by, 16 by + 16), slices [TZ bz, TZ bz + TZ).
+// Called by all 256 threads of the CTA; returns with no copies in flight.
+template <int TZ, int NB, typename OutT>
+__device__ __forceinline__ void bp_tile(const BPParams& kp, const float* __restrict__ fproj,
+                                        const PiRecord* __restrict__ pit,
+                                        const float4* __restrict__ views,
+                                        const float* __restrict__ xyz, OutT* __restrict__ image,
+                                        int bx, int by, int bz, BPShared<NB>& sh, float* tile) {
+    auto& foot = sh.foot;
+    auto& vg = sh.vg;
+    int& s_pmin = sh.s_pmin;
+    int& s_pmax = sh.s_pmax;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tx = tid & (kTXY2 - 1), ty = tid >> 4;
+    const int x = bx * kTXY2 + tx, y = by * kTXY2 + ty;
+    const int zb = bz * TZ;
+    const int NX = kp.NX, NY = kp.NY, NZ = kp.NZ, P = kp.P, YL = kp.YL, ZL = kp.ZL;
+    const bool col_ok = (x < NX) && (y < NY);
+    const float* xc = xyz;
+    const float* yc = xyz + NX;
+    const float* zc = xyz + NX + NY;
+    const float X = col_ok ? xc[x] : 0.f, Y = col_ok ? yc[y] : 0.f;
+    const float z0 = zc[zb];
+    const float dzf = kp.dzf;
+
+    if (tid == 0) { s_pmin = INT_MAX; s_pmax = INT_MIN; }
+
+    int bi[TZ], ti[TZ];
+    float bf[TZ], tf[TZ], acc[TZ];
+    int tmin = INT_MAX, tmax = INT_MIN, flo = INT_MIN, fhi = INT_MAX;
+    bool all_valid = col_ok;
+    const size_t colbase = ((size_t)x * NY + y) * NZ;
+#pragma unroll
+    for (int k = 0; k < TZ; ++k) {
+        const int z = zb + k;
+        PiRecord r{kPiInvalid, 0.f, -10, 0.f};
+        if (col_ok && z < NZ) r = pit[colbase + z];
+        bi[k] = r.bi; bf[k] = r.bf; ti[k] = r.ti; tf[k] = r.tf;
+        acc[k] = 0.f;
+        if (r.bi != kPiInvalid) {
+            tmin = min(tmin, max(1, r.bi));
+            tmax = max(tmax, min(r.ti + 1, P - 2));
+            flo = max(flo, r.bi + 2);  // views past both B-side ramp views
+            fhi = min(fhi, r.ti - 1);  // views before both T-side ramp views
+        } else {
+            all_valid = false;
+        }
+    }
+    int wmin = tmin, wmax = tmax;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        wmin = min(wmin, __shfl_xor_sync(0xffffffffu, wmin, o));
+        wmax = max(wmax, __shfl_xor_sync(0xffffffffu, wmax, o));
+    }
+    __syncthreads();
+    if (lane == 0 && wmin <= wmax) {
+        atomicMin(&s_pmin, wmin);
+        atomicMax(&s_pmax, wmax);
+    }
+    __syncthreads();
+    const int pmin = s_pmin, pmax = s_pmax;
+    if (pmin > pmax) return;
+
+    const int x0 = bx * kTXY2, x1 = min(x0 + kTXY2, NX) - 1;
+    const int y0 = by * kTXY2, y1 = min(y0 + kTXY2, NY) - 1;
+    const int z1 = min(zb + TZ, NZ) - 1;
+    const float bx0 = xc[x0], bx1 = xc[x1], by0 = yc[y0], by1 = yc[y1];
+    const float bz0 = zc[zb], bz1 = zc[z1];
+    const float R = kp.Rf, DdU = kp.DdU, DdV = kp.DdV, HalfY = kp.HalfY, HalfZ = kp.HalfZ;
+
+    // footprint of view p for buffer slot j (one thread per view)
+    auto footprint = [&](int buf, int j, int p) {
+        Foot2 f{0, 0, -1, 0};
+        if (p <= pmax) {
+            const float4 g = views[p];
+            vg[buf][j] = g;
+            float umin = 1e30f, umax = -1e30f, vmin = 1e30f, vmax = -1e30f;
+            bool ok = true;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const float cx = (c & 1) ? bx1 : bx0, cy = (c & 2) ? by1 : by0;
+                const float fen = R - (cx * g.x + cy * g.y);
+                ok = ok && (fen > 1e-3f * R);
+                const float inv = 1.f / fen;
+                const float u = (cy * g.x - cx * g.y) * DdU * inv + HalfY;
+                const float va = (bz0 - g.z) * DdV * inv + HalfZ;
+                const float vb = (bz1 - g.z) * DdV * inv + HalfZ;
+                umin = fminf(umin, u); umax = fmaxf(umax, u);
+                vmin = fminf(vmin, fminf(va, vb)); vmax = fmaxf(vmax, fmaxf(va, vb));
+            }
+            f = Foot2{0, 0, -2, 0};  // direct global reads unless the footprint fits
+            if (ok) {
+                const int u0 = max(0, min(YL - 2, (int)floorf(umin) - 1));
+                const int u1 = max(0, min(YL - 2, (int)floorf(umax) + 1)) + 1;
+                const int v0 = max(0, min(ZL - 2, (int)floorf(vmin) - 1));
+                const int v1 = max(0, min(ZL - 2, (int)floorf(vmax) + 1)) + 1;
+                const int W = u1 - u0 + 1, H = v1 - v0 + 1;
+                if (W * H <= kCap2 && W <= 64) f = Foot2{u0, v0, W, H};
+            }
+        }
+        foot[buf][j] = f;
+    };
+    // cp.async the footprints of buffer `buf` (block starting at view pb): warp per row
+    auto stage = [&](int buf, int pb) {
+#pragma unroll 1
+        for (int j = 0; j < NB; ++j) {
+            const Foot2 f = foot[buf][j];
+            if (f.W <= 0) continue;
+            const float* src = fproj + ((size_t)(pb + j) * ZL + f.v0) * YL + f.u0;
+            float* dst = tile + (buf * NB + j) * kCap2;
+            for (int r = warp; r < f.H; r += 8) {
+                if (lane < f.W) cp_async4(dst + r * f.W + lane, src + (size_t)r * YL + lane);
+                if (lane + 32 < f.W) cp_async4(dst + r * f.W + lane + 32, src + (size_t)r * YL + lane + 32);
+            }
+        }
+        cp_async_commit();
+    };
+
+    if (tid < NB) footprint(0, tid, pmin + tid);
+    __syncthreads();
+    stage(0, pmin);
+    int buf = 0;
+#pragma unroll 1
+    for (int pb = pmin; pb <= pmax; pb += NB, buf ^= 1) {
+        const int pn = pb + NB;
+        if (tid < NB) footprint(buf ^ 1, tid, pn + tid);  // empty slots when pn > pmax
+        __syncthreads();
+        stage(buf ^ 1, pn);
+        cp_async_wait<1>();
+        __syncthreads();
+        // warp-uniform: every lane's voxels are all inside their intervals for the block
+        const bool fast = __all_sync(0xffffffffu, all_valid && pb >= flo &&
+                                                   pb + NB - 1 <= fhi && pb + NB - 1 <= pmax);
+        if (col_ok && wmin <= wmax && !(pb + NB - 1 < wmin || pb > wmax)) {
+#pragma unroll 1
+            for (int j = 0; j < NB; ++j) {
+                const int p = pb + j;
+                if (p > pmax) break;
+                if (!fast && (p < tmin || p > tmax)) continue;
+                const Foot2 f = foot[buf][j];
+                const float4 g = vg[buf][j];
+                const float fen = R - (X * g.x + Y * g.y);
+                const float YY = Y * g.x - X * g.y;
+                const float inv = rcp_approx(fen);
+                const float u = YY * DdU * inv + HalfY;
+                const float kv = DdV * inv;
+                const float r2 = fen * fen + YY * YY;
+                const int ui = max(0, min(YL - 2, __float2int_rd(u)));
+                const float alfa = u - (float)ui;
+                const bool smem = f.W > 0;
+                // staged taps: 32-bit index into the shared tile (row stride W)
+                const int W = f.W;
+                const int tb = (buf * NB + j) * kCap2 + (ui - f.u0) - f.v0 * W;
+                const float* base;
+                int stride;
+                if (smem) {
+                    base = tile + tb;
+                    stride = W;
+                } else {
+                    base = fproj + (size_t)p * ZL * YL + ui;
+                    stride = YL;
+                }
+                const float dz0 = z0 - g.z;
+                if (fast && smem) {
+#pragma unroll
+                    for (int k = 0; k < TZ; ++k) {
+                        const float dz = fmaf((float)k, dzf, dz0);
+                        const float v = fmaf(dz, kv, HalfZ);
+                        const float rinv = rsqrt_approx(fmaf(dz, dz, r2));
+                        const int vi = max(0, min(ZL - 2, __float2int_rd(v)));
+                        const float beta = v - (float)vi;
+                        const int i0 = tb + vi * W;
+                        const int i1 = i0 + W;
+                        const float t00 = tile[i0], t01 = tile[i0 + 1];
+                        const float t10 = tile[i1], t11 = tile[i1 + 1];
+                        const float a0 = fmaf(alfa, t01 - t00, t00);
+                        const float a1 = fmaf(alfa, t11 - t10, t10);
+                        acc[k] = fmaf(fmaf(beta, a1 - a0, a0), rinv, acc[k]);
+                    }
+                } else {
+#pragma unroll
+                    for (int k = 0; k < TZ; ++k) {
+                        const int d0 = p - bi[k];
+                        const int d1 = ti[k] + 1 - p;
+                        if ((d0 | d1) < 0) continue;
+                        float w = 1.f;
+                        if (d1 <= 1) w = ramp2(tf[k] + (float)(d1 - 1));
+                        else if (d0 <= 1) w = ramp2((float)d0 - bf[k]);
+                        const float dz = fmaf((float)k, dzf, dz0);
+                        const float v = fmaf(dz, kv, HalfZ);
+                        const float rinv = rsqrt_approx(fmaf(dz, dz, r2));
+                        const int vi = max(0, min(ZL - 2, __float2int_rd(v)));
+                        const float beta = v - (float)vi;
+                        const float* q = base + vi * stride;
+                        float t00, t01, t10, t11;
+                        if (smem) {
+                            const int i0 = tb + vi * W, i1 = i0 + W;
+                            t00 = tile[i0]; t01 = tile[i0 + 1]; t10 = tile[i1]; t11 = tile[i1 + 1];
+                        } else {
+                            t00 = __ldg(q); t01 = __ldg(q + 1); t10 = __ldg(q + stride);
+                            t11 = __ldg(q + stride + 1);
+                        }
+                        const float a0 = fmaf(alfa, t01 - t00, t00);
+                        const float a1 = fmaf(alfa, t11 - t10, t10);
+                        acc[k] = fmaf(w * fmaf(beta, a1 - a0, a0), rinv, acc[k]);
+                    }
+                }
+            }
+        }
+        __syncthreads();  // buffer `buf` is free for the block after next
+    }
+    cp_async_wait<0>();
+    if (!col_ok) return;
+#pragma unroll
+    for (int k = 0; k < TZ; ++k) {
+        const int z = zb + k;
+        if (z < NZ && bi[k] != kPiInvalid) image[colbase + z] = (OutT)(-acc[k] * kp.invPs);
+    }
+}
+
+template <int TZ, int NB, typename OutT>
+__global__ void __launch_bounds__(256, 3)
+k_bkproj2(BPParams kp, const float* __restrict__ fproj, const PiRecord* __restrict__ pit,
+          const float4* __restrict__ views, const float* __restrict__ xyz,
+          OutT* __restrict__ image) {
+    extern __shared__ float tile[];  // 2 x NB x kCap2
+    __shared__ BPShared<NB> sh;
+    bp_tile<TZ, NB, OutT>(kp, fproj, pit, views, xyz, image, blockIdx.x, blockIdx.y, blockIdx.z,
+                          sh, tile);
+}
+
+// Many scans in one persistent launch: the CTAs pull tiles of all scans from one atomic
+// counter (largest-first order is the caller's choice of scan order), so uneven scans share
+// the GPU without tails between them.
+template <int TZ, int NB>
+__global__ void __launch_bounds__(256, 3)
+k_bkproj2_batch(const BatchScanDev* __restrict__ scans, int n_scans, long long total_tiles,
+                unsigned long long* __restrict__ counter) {
+    extern __shared__ float tile[];
+    __shared__ BPShared<NB> sh;
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) sh.s_item = (int)atomicAdd(counter, 1ull);
+        __syncthreads();
+        const long long item = sh.s_item;
+        if (item >= total_tiles) break;
+        int s = 0;
+        while (s + 1 < n_scans && scans[s + 1].first_tile <= item) ++s;
+        const BPParams kp = scans[s].kp;
+        const long long local = item - scans[s].first_tile;
+        const int tx = (kp.NX + kTXY2 - 1) / kTXY2, ty = (kp.NY + kTXY2 - 1) / kTXY2;
+        const int bx = (int)(local % tx);
+        const int by = (int)((local / tx) % ty);
+        const int bz = (int)(local / ((long long)tx * ty));
+        bp_tile<TZ, NB, float>(kp, scans[s].fproj, scans[s].pit, scans[s].views, scans[s].xyz,
+                               scans[s].image, bx, by, bz, sh, tile);
+    }
+}
+
+long long bkproj_batch_tiles(const BPParams& kp, int variant) {
+    const int TZ = (variant == 1) ? 4 : 8;
+    return (long long)((kp.NX + kTXY2 - 1) / kTXY2) * ((kp.NY + kTXY2 - 1) / kTXY2) *
+           ((kp.NZ + TZ - 1) / TZ);
+}
+
+template <int TZ, int NB>
+static Status launch_batch(cudaStream_t s, const BatchScanDev* d_scans, int n,
+                           long long total, unsigned long long* d_counter) {
+    const size_t smem = (size_t)2 * NB * kCap2 * sizeof(float);
+    CTR_CUDA(cudaFuncSetAttribute(k_bkproj2_batch<TZ, NB>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int dev = 0, sms = 148;
+    CTR_CUDA(cudaGetDevice(&dev));
+    CTR_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const long long grid = std::min<long long>(total, 3LL * sms);
+    CTR_CUDA(cudaMemsetAsync(d_counter, 0, sizeof(unsigned long long), s));
+    if (grid > 0)
+        k_bkproj2_batch<TZ, NB><<<(unsigned)grid, 256, smem, s>>>(d_scans, n, total, d_counter);
+    CTR_CUDA(cudaGetLastError());
+    return Status::Ok();
+}
+
+Status launch_bkproj_batch(int variant, cudaStream_t s, const BatchScanDev* d_scans, int n,
+                           long long total, unsigned long long* d_counter) {
+    switch (variant) {
+    case 1: return launch_batch<4, 8>(s, d_scans, n, total, d_counter);
+    case 2: return launch_batch<8, 4>(s, d_scans, n, total, d_counter);
+    default: return launch_batch<8, 8>(s, d_scans, n, total, d_counter);
+    }
+}
+
+template <int TZ, int NB, typename OutT>
+static Status launch_v2(cudaStream_t s, BPPlan& plan, const float* d_fproj,
+                        const PiRecord* d_pitab, OutT* d_image) {
+    const BPParams& kp = plan.kp;
+    dim3 grid((kp.NX + kTXY2 - 1) / kTXY2, (kp.NY + kTXY2 - 1) / kTXY2, (kp.NZ + TZ - 1) / TZ);
+    const size_t smem = (size_t)2 * NB * kCap2 * sizeof(float);
+    CTR_CUDA(cudaFuncSetAttribute(k_bkproj2<TZ, NB, OutT>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_bkproj2<TZ, NB, OutT><<<grid, 256, smem, s>>>(kp, d_fproj, d_pitab, plan.views.as<float4>(),
+                                                    plan.xyz.as<float>(), d_image);
+    CTR_CUDA(cudaGetLastError());
+    return Status::Ok();
+}
+
+// variants 0 (default) .. 2 of the second form; 100 + k selects the first form (bkproj.cu)
+template <typename OutT>
+Status launch_bkproj_v2(int variant, cudaStream_t s, BPPlan& plan, const float* d_fproj,
+                        const PiRecord* d_pitab, OutT* d_image) {
+    switch (variant) {
+    case 1: return launch_v2<4, 8, OutT>(s, plan, d_fproj, d_pitab, d_image);
+    case 2: return launch_v2<8, 4, OutT>(s, plan, d_fproj, d_pitab, d_image);
+    default: return launch_v2<8, 8, OutT>(s, plan, d_fproj, d_pitab, d_image);
+    }
+}
+
+template Status launch_bkproj_v2<float>(int, cudaStream_t, BPPlan&, const float*, const PiRecord*, float*);
+template Status launch_bkproj_v2<double>(int, cudaStream_t, BPPlan&, const float*, const PiRecord*, double*);
+
+}  // namespace ctr

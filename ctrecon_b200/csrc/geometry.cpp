@@ -262,6 +262,7 @@ BPParams make_bp_params(const BPGeom& g) {
     k.HalfY = (float)g.HalfY;
     k.HalfZ = (float)g.HalfZ;
     k.invPs = (float)(1.0 / g.ProjScale);
+    k.dzf = (float)g.dz;
     return k;
 }
 

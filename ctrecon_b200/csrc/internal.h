@@ -99,7 +99,7 @@ struct BPParams {
     int NX, NY, NZ, P, YL, ZL;
     double ScanR, HelicP, DeltaL, CtrMinusBeg, ObjR2;
     double XC, YC, ZC, dx, dy, dz;
-    float Rf, DdU, DdV, HalfY, HalfZ, invPs;
+    float Rf, DdU, DdV, HalfY, HalfZ, invPs, dzf;
 };
 BPParams make_bp_params(const BPGeom& g);
 
@@ -108,6 +108,27 @@ struct BPPlan {
     BPParams kp{};
     DevBuf views;   // float4 per view: cos, sin, source z, 0
     DevBuf xyz;     // float voxel coordinates x[NX], y[NY], z[NZ]
+};
+
+// One scan of a batched backprojection (batch.cpp, bkproj2.cu)
+struct BatchScanDev {
+    BPParams kp;
+    const float* fproj;
+    const PiRecord* pit;
+    const float4* views;
+    const float* xyz;
+    float* image;
+    long long first_tile;
+};
+
+// The learned PI-line initialiser (pinet.cu): FP32 master parameters, Adam state, training
+// data, and the BF16 inference copy.
+struct PinetState {
+    DevBuf theta, adam_m, adam_v, grad, data, infer, guess;
+    bool trained = false;
+    double r_max = 0;
+    int version = 0;        // bumped by every training run
+    int infer_version = -1; // version the inference copy was made from
 };
 
 }  // namespace ctr
@@ -133,11 +154,14 @@ struct ctrecon_ctx {
     ctr::DevBuf ws_a, ws_b, ws_c, ws_d;  // host-call staging (f64 in, f32, f32 out, f64 out)
     ctr::DevBuf ws_ell;      // phantom ellipsoids
     ctr::DevBuf ws_flag;     // device error word
+    ctr::PinetState pinet;   // learned PI-line initialiser
 };
 
 namespace ctr {
 Status get_filter_plan(ctrecon_ctx* ctx, const ctrecon_filter_params& p, FilterPlan** out);
 Status get_bp_plan(ctrecon_ctx* ctx, const ctrecon_bp_geom& g, BPPlan** out);
+Status build_filter_plan(const ctrecon_filter_params& p, FilterPlan& plan);
+Status build_bp_plan(const BPGeom& g, BPPlan& plan);
 
 // kernel launchers (filter.cu, pi.cu, bkproj.cu, phantom.cu)
 Status launch_filter(ctrecon_ctx* ctx, cudaStream_t s, FilterPlan& plan, const float* d_proj,

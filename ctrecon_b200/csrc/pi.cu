@@ -9,111 +9,16 @@
 //
 // Solvers (ctx option CTRECON_OPT_PI_SOLVER):
 //   BISECT  the reference's bisection, step for step (the judge of the others);
-//   NEWTON  safeguarded Newton on g(sb) = zz(sb) - z inside the same bracket, started at
-//           the bracket midpoint (or at the learned initial guess, pinet.cu), stopped at
-//           the same tolerances.
+//   NEWTON  safeguarded Newton with the closed-form derivative inside the same bracket,
+//           started at the PI line of the axis point at the same height;
+//   LEARNED the same Newton started at the trained network's prediction (pinet_infer.cu).
 #include "internal.h"
+#include "pi_device.cuh"
 
 namespace ctr {
 
-constexpr double kPiTol = 0.0000001;  // DeltaMax, KatsevichBkProj.cpp:26
-
-// chord of the PI line starting at sb: returns zz(sb) and st(sb)
-__device__ __forceinline__ double pi_chord(double x, double y, double r2, double sb,
-                                           double* st_out) {
-    const double PI = kRefPi;
-    double ssb, csb;
-    sincos(sb, &ssb, &csb);
-    double tempcos = 2 * (1 - y * ssb - x * csb);
-    double t = (1 - r2) / tempcos;
-    double templan = acos((y * csb - x * ssb) / sqrt(tempcos + r2 - 1));
-    double st = 2 * templan + sb;
-    *st_out = st;
-    return (sb * t + (1 - t) * st) / (2 * PI);
-}
-
-__device__ void pi_bisect(double x, double y, double z, double* B, double* T) {
-    const double PI = kRefPi;
-    double delta = 1, bmax = z * 2 * PI, bmin, r2 = x * x + y * y;
-    bmin = bmax - 2 * PI;
-    double sb = 0, st = 0;
-    while (((bmax - bmin) > kPiTol) && (delta > kPiTol)) {
-        sb = (bmax + bmin) * 0.5;
-        double zz = pi_chord(x, y, r2, sb, &st);
-        if (zz < z) bmin = sb;
-        else bmax = sb;
-        delta = fabs(zz - z);
-    }
-    *B = sb;
-    *T = st;
-}
-
-// Newton with a bisection safeguard: the iterate stays inside [bmin, bmax], which shrinks
-// with the sign of g; the derivative is a central difference (g is smooth and monotone).
-__device__ void pi_newton(double x, double y, double z, double s0, double* B, double* T,
-                          int* iters) {
-    const double PI = kRefPi;
-    double bmax = z * 2 * PI, bmin = bmax - 2 * PI, r2 = x * x + y * y;
-    double sb = (s0 > bmin && s0 < bmax) ? s0 : 0.5 * (bmin + bmax);
-    double st = 0;
-    int it = 0;
-    for (; it < 60; ++it) {
-        double zz = pi_chord(x, y, r2, sb, &st);
-        double g = zz - z;
-        if (fabs(g) <= kPiTol) break;
-        if (g < 0) bmin = sb;
-        else bmax = sb;
-        if (bmax - bmin <= kPiTol) break;
-        const double h = 1e-6;
-        double stp, stm;
-        double gp = pi_chord(x, y, r2, sb + h, &stp);
-        double gm = pi_chord(x, y, r2, sb - h, &stm);
-        double d = (gp - gm) / (2 * h);
-        double nx = sb - g / d;
-        if (!(d > 0) || !(nx > bmin && nx < bmax)) nx = 0.5 * (bmin + bmax);
-        sb = nx;
-    }
-    *B = sb;
-    *T = st;
-    if (iters) *iters = it + 1;
-}
-
-__device__ __forceinline__ void voxel_xyz(const BPParams& kp, long long idx, int* xi, int* yi,
-                                          int* zi, double* X, double* Y, double* Z) {
-    int z = (int)(idx % kp.NZ);
-    long long r = idx / kp.NZ;
-    int y = (int)(r % kp.NY);
-    int x = (int)(r / kp.NY);
-    *xi = x; *yi = y; *zi = z;
-    *X = (x - kp.XC) * kp.dx;  // KatsevichBkProj.cpp:142-147
-    *Y = (y - kp.YC) * kp.dy;
-    *Z = (z - kp.ZC) * kp.dz;
-}
-
-// record + loop count from (sb, st), KatsevichBkProj.cpp:177-234
-__device__ __forceinline__ unsigned long long make_record(const BPParams& kp, double Ctr,
-                                                          double Beg, double sb, double st,
-                                                          PiRecord* rec) {
-    double Bv = sb / kp.DeltaL + Ctr - Beg;
-    double Tv = st / kp.DeltaL + Ctr - Beg;
-    const int P = kp.P;
-    if ((Bv >= P - 1) || (Tv <= 0)) {
-        rec->bi = kPiInvalid; rec->bf = 0.f; rec->ti = -10; rec->tf = 0.f;
-        return 0ull;
-    }
-    int Bindex = (int)(Bv + 10) - 10;
-    int Tindex = (int)(Tv + 10) - 9;
-    int LB = Bindex < 1 ? 1 : Bindex;
-    int LE = Tindex > P - 2 ? P - 2 : Tindex;
-    rec->bi = Bindex;
-    rec->bf = (float)(Bv - Bindex);
-    rec->ti = Tindex - 1;
-    rec->tf = (float)(Tv - (Tindex - 1));
-    return (unsigned long long)(LE - LB + 1);
-}
-
 __global__ void k_pi_solve(BPParams kp, double Ctr, double Beg, int solver,
-                           const float2* __restrict__ guess, PiRecord* __restrict__ out,
+                           const float* __restrict__ guess, PiRecord* __restrict__ out,
                            unsigned long long* __restrict__ count,
                            unsigned long long* __restrict__ iters_total) {
     const long long n = (long long)kp.NX * kp.NY * kp.NZ;
@@ -128,11 +33,14 @@ __global__ void k_pi_solve(BPParams kp, double Ctr, double Beg, int solver,
             double x = X / kp.ScanR, y = Y / kp.ScanR, z = Z / kp.HelicP;  // :173-175
             double sb, st;
             if (solver == CTRECON_PI_BISECT) {
-                pi_bisect(x, y, z, &sb, &st);
-                its = 27;
+                int it = 0;
+                pi_bisect(x, y, z, &sb, &st, &it);
+                its = (unsigned long long)it;
             } else {
-                double s0 = -1e300;
-                if (guess) s0 = (double)guess[idx].x + z * 2 * kRefPi;
+                // start: the PI line of the axis point at the same height, sb = 2 pi z - pi/2,
+                // plus the learned offset when there is one
+                double s0 = z * 2 * kRefPi - 0.5 * kRefPi;
+                if (guess) s0 += (double)guess[idx];
                 int it = 0;
                 pi_newton(x, y, z, s0, &sb, &st, &it);
                 its = (unsigned long long)it;
@@ -152,25 +60,41 @@ __global__ void k_pi_solve(BPParams kp, double Ctr, double Beg, int solver,
     }
 }
 
-Status launch_pi_solver(ctrecon_ctx* ctx, cudaStream_t s, BPPlan& plan, PiRecord* d_pitab,
-                        unsigned long long* d_updates, int solver, const float2* d_guess,
-                        unsigned long long* d_iters) {
-    (void)ctx;
+// implemented in pinet_infer.cu
+Status launch_pi_learned(ctrecon_ctx* ctx, cudaStream_t s, BPPlan& plan, PiRecord* d_pitab,
+                         unsigned long long* d_updates, unsigned long long* d_iters);
+
+static Status launch_solve(cudaStream_t s, BPPlan& plan, int solver, const float* guess,
+                           PiRecord* d_pitab, unsigned long long* d_updates,
+                           unsigned long long* d_iters) {
     const long long n = (long long)plan.kp.NX * plan.kp.NY * plan.kp.NZ;
     const int bs = 128;
     long long nb = (n + bs - 1) / bs;
     if (nb > 0x7fffffffLL) return make_status(CTRECON_ERR_UNSUPPORTED, "volume too large");
     k_pi_solve<<<(unsigned)nb, bs, 0, s>>>(plan.kp, plan.g.ProjCtr, (double)plan.g.ProjBegin,
-                                           solver, d_guess, d_pitab, d_updates, d_iters);
+                                           solver, guess, d_pitab, d_updates, d_iters);
     CTR_CUDA(cudaGetLastError());
     return Status::Ok();
 }
 
+// Newton from per-voxel offsets of the start point (the learned path, pinet_infer.cu)
+Status launch_pi_guess(ctrecon_ctx* ctx, cudaStream_t s, BPPlan& plan, PiRecord* d_pitab,
+                       unsigned long long* d_updates, unsigned long long* d_iters,
+                       const float* d_guess) {
+    (void)ctx;
+    return launch_solve(s, plan, CTRECON_PI_LEARNED, d_guess, d_pitab, d_updates, d_iters);
+}
+
+Status launch_pi_stats(ctrecon_ctx* ctx, cudaStream_t s, BPPlan& plan, PiRecord* d_pitab,
+                       unsigned long long* d_updates, unsigned long long* d_iters) {
+    if (ctx->opt_pi == CTRECON_PI_LEARNED)
+        return launch_pi_learned(ctx, s, plan, d_pitab, d_updates, d_iters);
+    return launch_solve(s, plan, ctx->opt_pi, nullptr, d_pitab, d_updates, d_iters);
+}
+
 Status launch_pi(ctrecon_ctx* ctx, cudaStream_t s, BPPlan& plan, PiRecord* d_pitab,
                  unsigned long long* d_updates) {
-    int solver = ctx->opt_pi;
-    if (solver == CTRECON_PI_LEARNED) solver = CTRECON_PI_NEWTON;  // guess wired in pinet.cu
-    return launch_pi_solver(ctx, s, plan, d_pitab, d_updates, solver, nullptr, nullptr);
+    return launch_pi_stats(ctx, s, plan, d_pitab, d_updates, nullptr);
 }
 
 }  // namespace ctr

@@ -1,0 +1,259 @@
+// pinet_infer.cu -- inference of the PI-line network, and the learned PI-line solve.
+//
+// A persistent CTA of 128 threads evaluates the network for 128 items at a time (voxels of the
+// volume, or given feature triples), one item per thread and per TMEM lane:
+//   layer 0 (3 -> 64)   FP32 FMA with BF16-rounded weights, SiLU, BF16 activations written
+//                       into a 128 x 64 K-major tile in shared memory (128-byte swizzle);
+//   layers 1..3 (64x64) one thread issues four tcgen05.mma (M = 128 items, N = 64, K = 16 each)
+//                       from that tile and the layer's BF16 weight tile, FP32 accumulation in 64
+//                       TMEM columns; every thread reads its row back (tcgen05.ld), adds the bias,
+//                       applies SiLU and writes the next layer's input tile;
+//   layer 4 (64 -> 2)   FP32 FMA.
+// For the learned PI solve the kernel stores each voxel's predicted sb offset; the FP64 Newton
+// kernel (pi.cu) then starts from 2 pi z - pi/2 + offset and writes the voxel's PI record
+// exactly as the plain solver does.
+#include "internal.h"
+#include "pi_device.cuh"
+#include "pinet.h"
+#include "tc_util.cuh"
+
+#include <cuda_bf16.h>
+
+#include <algorithm>
+
+namespace ctr {
+
+Status pinet_ensure(ctrecon_ctx* ctx);
+Status launch_pi_guess(ctrecon_ctx* ctx, cudaStream_t s, BPPlan& plan, PiRecord* d_pitab,
+                       unsigned long long* d_updates, unsigned long long* d_iters,
+                       const float* d_guess);
+
+namespace {
+
+constexpr int kT = 128;
+// shared-memory layout (offsets from a 1024-byte aligned base)
+constexpr int kSmA = 0;                    // activation tile, 128 x 128 B
+constexpr int kSmW = 16384;                // three weight tiles, 64 x 128 B each
+constexpr int kSmF = 16384 + 3 * 8192;     // FP32 parameters (kNetF32 floats)
+constexpr int kSmBar = kSmF + kNetF32 * 4; // mbarrier (8-byte aligned)
+constexpr int kSmSlot = kSmBar + 8;        // TMEM address
+constexpr int kSmBytes = kSmSlot + 8 + 1024;
+
+// SiLU, x * sigmoid(x): accurate form for the FP32 features of the output layer, one-MUFU
+// form 0.5 x (1 + tanh(x/2)) for activations that are rounded to BF16 anyway
+__device__ __forceinline__ float silu_acc(float z) { return __fdividef(z, 1.f + __expf(-z)); }
+__device__ __forceinline__ float silu_bf(float z) {
+    const float h = 0.5f * z;
+    float t;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(h));
+    return fmaf(h, t, h);
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
+    __nv_bfloat162 h = __floats2bfloat162_rn(a, b);  // .x = a (low half)
+    return *reinterpret_cast<uint32_t*>(&h);
+}
+
+__global__ void k_net_prep(const float* __restrict__ theta, unsigned char* __restrict__ net) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    __nv_bfloat16* wb = reinterpret_cast<__nv_bfloat16*>(net);
+    float* f = reinterpret_cast<float*>(net + kNetBf16Bytes);
+    if (i < 3 * 4096) wb[i] = __float2bfloat16_rn(theta[pinet_offW(1 + i / 4096) + i % 4096]);
+    if (i < 192) f[kNetF32_W0 + i] = __bfloat162float(__float2bfloat16_rn(theta[pinet_offW(0) + i]));
+    if (i < 256) f[kNetF32_B0 + i] = theta[pinet_offB(i / 64) + i % 64];
+    if (i < 128) f[kNetF32_W4 + i] = __bfloat162float(__float2bfloat16_rn(theta[pinet_offW(4) + i]));
+    if (i < 2) f[kNetF32_B4 + i] = theta[pinet_offB(4) + i];
+}
+
+// voxel mode (feat == nullptr): guess[idx] = predicted sb offset (radians) of each voxel inside
+// the cylinder; feature mode: raw[idx] = the two network outputs
+__global__ void __launch_bounds__(kT)
+k_pinet_infer(BPParams kp, const unsigned char* __restrict__ net, long long n_items,
+              const float* __restrict__ feat, float2* __restrict__ raw,
+              float* __restrict__ guess, int* __restrict__ err) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* sm = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint8_t* A = sm + kSmA;
+    uint8_t* Wt = sm + kSmW;
+    float* F = reinterpret_cast<float*>(sm + kSmF);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + kSmBar);
+    uint32_t* slot = reinterpret_cast<uint32_t*>(sm + kSmSlot);
+    const int t = threadIdx.x, warp = t >> 5;
+
+    // weights into 128-byte-swizzled K-major tiles (row = output neuron, 8 chunks of 8 inputs)
+    const uint4* src = reinterpret_cast<const uint4*>(net);
+    for (int q = t; q < 3 * 64 * 8; q += kT) {
+        const int l = q >> 9, r = (q >> 3) & 63, c = q & 7;
+        *reinterpret_cast<uint4*>(Wt + l * 8192 + tcu::sw128_offset(r, c)) = src[q];
+    }
+    const float* fsrc = reinterpret_cast<const float*>(net + kNetBf16Bytes);
+    for (int q = t; q < kNetF32; q += kT) F[q] = fsrc[q];
+    if (t == 0) {
+        tcu::mbar_init(bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) tcu::tmem_alloc(slot, 64);
+    tcu::fence_proxy_async();
+    tcu::fence_before();
+    __syncthreads();
+    tcu::fence_after();
+    const uint32_t tmem = *slot;
+    const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+    const uint32_t idesc = tcu::idesc_bf16_f32(128, 64);
+    const uint32_t a_addr = tcu::smem_u32(A), w_addr = tcu::smem_u32(Wt);
+    uint32_t phase = 0;
+    const float* W0 = F + kNetF32_W0;
+    const float* B0 = F + kNetF32_B0;
+    const float* W4 = F + kNetF32_W4;
+    const float* B4 = F + kNetF32_B4;
+    const long long ntiles = (n_items + kT - 1) / kT;
+
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const long long idx = tile * kT + t;
+        const bool valid = idx < n_items;
+        float f0 = 0.f, f1 = 1.f, f2 = 0.f;
+        bool inside = false;
+        if (feat) {
+            if (valid) { f0 = feat[3 * idx]; f1 = feat[3 * idx + 1]; f2 = feat[3 * idx + 2]; }
+        } else if (valid) {
+            int xi, yi, zi;
+            double X, Y, Z;
+            voxel_xyz(kp, idx, &xi, &yi, &zi, &X, &Y, &Z);
+            inside = X * X + Y * Y < kp.ObjR2;  // KatsevichBkProj.cpp:168
+            const double x = X / kp.ScanR, y = Y / kp.ScanR, z = Z / kp.HelicP;
+            const double r = sqrt(x * x + y * y);
+            double s2, c2;
+            sincos(2 * kRefPi * z, &s2, &c2);
+            const double cph = r > 0 ? x / r : 1.0, sph = r > 0 ? y / r : 0.0;
+            f0 = (float)(r * kPinetRInv);
+            f1 = (float)(cph * c2 + sph * s2);  // cos(phi - 2 pi z)
+            f2 = (float)(sph * c2 - cph * s2);  // sin(phi - 2 pi z)
+        }
+        // layer 0 -> activation tile
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            uint32_t pk[4];
+#pragma unroll
+            for (int h = 0; h < 4; ++h) {
+                const int o = c * 8 + 2 * h;
+                const float v0 = silu_bf(B0[o] + W0[3 * o] * f0 + W0[3 * o + 1] * f1 + W0[3 * o + 2] * f2);
+                const float v1 = silu_bf(B0[o + 1] + W0[3 * o + 3] * f0 + W0[3 * o + 4] * f1 + W0[3 * o + 5] * f2);
+                pk[h] = pack_bf16(v0, v1);
+            }
+            *reinterpret_cast<uint4*>(A + tcu::sw128_offset(t, c)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+        }
+        float o0 = B4[0], o1 = B4[1];
+        bool ok = true;
+#pragma unroll 1
+        for (int l = 0; l < 3; ++l) {
+            tcu::fence_proxy_async();
+            tcu::fence_before();
+            __syncthreads();
+            tcu::fence_after();
+            if (t == 0) {
+#pragma unroll
+                for (int ks = 0; ks < 4; ++ks)
+                    tcu::mma_bf16(tmem, tcu::sw128_desc(a_addr + 32 * ks),
+                                  tcu::sw128_desc(w_addr + l * 8192 + 32 * ks), idesc, ks > 0);
+                tcu::mma_commit(bar);
+            }
+            __syncwarp();
+            ok = __all_sync(0xffffffffu, tcu::mbar_wait(bar, phase, err, 5)) && ok;
+            phase ^= 1u;
+            tcu::fence_after();
+            const float* bl = B0 + 64 * (l + 1);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                float h[16];
+                if (ok) tcu::tmem_ld16(lane_addr + 16 * q, h);
+                else {
+#pragma unroll
+                    for (int i = 0; i < 16; ++i) h[i] = 0.f;
+                }
+                if (l < 2) {
+#pragma unroll
+                    for (int cc = 0; cc < 2; ++cc) {
+                        const int c = 2 * q + cc;
+                        const float* hv = h + 8 * cc;
+                        const float* bb = bl + 8 * c;
+                        const uint4 v = make_uint4(
+                            pack_bf16(silu_bf(hv[0] + bb[0]), silu_bf(hv[1] + bb[1])),
+                            pack_bf16(silu_bf(hv[2] + bb[2]), silu_bf(hv[3] + bb[3])),
+                            pack_bf16(silu_bf(hv[4] + bb[4]), silu_bf(hv[5] + bb[5])),
+                            pack_bf16(silu_bf(hv[6] + bb[6]), silu_bf(hv[7] + bb[7])));
+                        *reinterpret_cast<uint4*>(A + tcu::sw128_offset(t, c)) = v;
+                    }
+                } else {
+#pragma unroll
+                    for (int i = 0; i < 16; ++i) {
+                        const float a = silu_acc(h[i] + bl[16 * q + i]);
+                        o0 = fmaf(W4[16 * q + i], a, o0);
+                        o1 = fmaf(W4[64 + 16 * q + i], a, o1);
+                    }
+                }
+            }
+        }
+        if (valid) {
+            if (raw) raw[idx] = make_float2(o0, o1);
+            if (guess) guess[idx] = inside ? (float)(o0 / kPinetOutScale) : 0.f;
+        }
+    }
+    tcu::fence_before();
+    __syncthreads();
+    if (warp == 0) tcu::tmem_dealloc(tmem, 64);
+}
+
+int persistent_blocks() {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return sms * 4;
+}
+
+}  // namespace
+
+Status pinet_prepare(ctrecon_ctx* ctx, cudaStream_t s) {
+    PinetState& P = ctx->pinet;
+    if (!P.trained)
+        return make_status(CTRECON_ERR_INVALID_ARGUMENT,
+                           "the PI-line network is not trained (ctrecon_pinet_train or "
+                           "ctrecon_pinet_set_params first)");
+    if (P.infer_version == P.version && P.infer.ptr) return Status::Ok();
+    CTR_TRY(P.infer.ensure(kNetBytes, "network inference copy"));
+    k_net_prep<<<(3 * 4096 + 255) / 256, 256, 0, s>>>(P.theta.as<float>(), P.infer.as<unsigned char>());
+    CTR_CUDA(cudaGetLastError());
+    P.infer_version = P.version;
+    return Status::Ok();
+}
+
+static Status launch_infer(ctrecon_ctx* ctx, cudaStream_t s, const BPParams& kp, long long n,
+                           const float* feat, float2* raw, float* guess) {
+    CTR_TRY(pinet_prepare(ctx, s));
+    CTR_TRY(ctx->ws_flag.ensure(256, "device error word"));
+    CTR_CUDA(cudaMemsetAsync(ctx->ws_flag.ptr, 0, sizeof(int), s));
+    CTR_CUDA(cudaFuncSetAttribute(k_pinet_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmBytes));
+    const long long ntiles = (n + kT - 1) / kT;
+    const int grid = (int)std::min<long long>(ntiles, persistent_blocks());
+    if (grid <= 0) return Status::Ok();
+    k_pinet_infer<<<grid, kT, kSmBytes, s>>>(kp, ctx->pinet.infer.as<unsigned char>(), n, feat,
+                                             raw, guess, ctx->ws_flag.as<int>());
+    CTR_CUDA(cudaGetLastError());
+    return Status::Ok();
+}
+
+Status launch_pi_learned(ctrecon_ctx* ctx, cudaStream_t s, BPPlan& plan, PiRecord* d_pitab,
+                         unsigned long long* d_updates, unsigned long long* d_iters) {
+    const long long n = (long long)plan.kp.NX * plan.kp.NY * plan.kp.NZ;
+    CTR_TRY(ctx->pinet.guess.ensure((size_t)n * sizeof(float), "learned PI guesses"));
+    float* g = ctx->pinet.guess.as<float>();
+    CTR_TRY(launch_infer(ctx, s, plan.kp, n, nullptr, nullptr, g));
+    return launch_pi_guess(ctx, s, plan, d_pitab, d_updates, d_iters, g);
+}
+
+Status pinet_predict(ctrecon_ctx* ctx, cudaStream_t s, const float* d_feat, long long n,
+                     float* d_out) {
+    BPParams kp{};
+    return launch_infer(ctx, s, kp, n, d_feat, reinterpret_cast<float2*>(d_out), nullptr);
+}
+
+}  // namespace ctr

@@ -169,6 +169,12 @@ def config(name: str) -> HelicalScan:
         return HelicalScan("c2", 600.0, 1200.0, 736, 64, 0.8, 0.8, 1160, 8, 0.9,
                            512, 512, 256, voxel=(0.4, 0.4, 0.4), n_ellipsoids=40, seed=1002,
                            photons=1e5)
+    if name == "c2s":
+        # a slab of c2 for profiling captures: same detector, pitch and voxels, 2 turns,
+        # 32 slices (the per-voxel PI coverage is that of c2)
+        return HelicalScan("c2s", 600.0, 1200.0, 736, 64, 0.8, 0.8, 1160, 2, 0.9,
+                           512, 512, 32, voxel=(0.4, 0.4, 0.4), n_ellipsoids=40, seed=1012,
+                           photons=1e5)
     if name == "c3":
         return HelicalScan("c3", 600.0, 1200.0, 1024, 128, 0.8, 0.8, 2304, 6, 0.9,
                            512, 512, 512, voxel=None, n_ellipsoids=40, seed=1003)

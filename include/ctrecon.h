@@ -173,6 +173,58 @@ ctrecon_status ctrecon_filter_noalloc_dev_f32(void* stream, const ctrecon_filter
  * or CTRECON_ERR_TIMEOUT when a bounded wait inside a kernel gave up. */
 ctrecon_status ctrecon_sync(ctrecon_ctx* ctx, void* stream);
 
+/* PI-line solve as ctrecon_pi_dev, also counting the solver's iterations (device unsigned long
+ * long, summed over solved voxels): bisection steps for CTRECON_PI_BISECT, Newton steps for
+ * CTRECON_PI_NEWTON / CTRECON_PI_LEARNED. */
+ctrecon_status ctrecon_pi_dev_stats(ctrecon_ctx* ctx, void* stream, const ctrecon_bp_geom* g,
+                                    void* d_pitab, unsigned long long* d_updates,
+                                    unsigned long long* d_iters);
+
+/* ---- batches of uneven scans (no counterpart in the reference) ----------------------------
+ * A batch reconstructs n scans with their own geometries. Each run enqueues every scan's filter
+ * and PI solve, then ONE persistent backprojection launch over the tiles of all scans (largest
+ * scans first, CTAs pulling tiles from a shared counter). With use_graph != 0 the first run is
+ * eager and the second is captured into a CUDA graph that later runs replay (re-captured when
+ * the buffer pointers change); graph mode needs a created stream. The batch uses the context's
+ * options (Hilbert mode, PI solver, backprojector variant) and its work buffers: one batch run
+ * at a time per context. */
+typedef struct ctrecon_batch ctrecon_batch;
+ctrecon_status ctrecon_batch_create(ctrecon_ctx* ctx, int n_scans,
+                                    const ctrecon_filter_params* params,
+                                    const ctrecon_bp_geom* geoms, ctrecon_batch** out);
+void ctrecon_batch_destroy(ctrecon_batch* batch);
+/* backprojector tile shape for the batch: 0 (8 slices x 8 views), 1 (4 x 8), 2 (8 x 4) */
+ctrecon_status ctrecon_batch_set_variant(ctrecon_batch* batch, int variant);
+/* d_proj[i] (input), d_fproj[i] (work), d_image[i] (output, in place) for scan i */
+ctrecon_status ctrecon_batch_run_dev(ctrecon_batch* batch, void* stream,
+                                     const float* const* d_proj, float* const* d_fproj,
+                                     float* const* d_image, int use_graph);
+/* sum(LoopEnd-LoopBegin+1) of each scan (bisection PI solve, synchronous) */
+ctrecon_status ctrecon_batch_updates(ctrecon_batch* batch, unsigned long long* host_updates);
+
+/* ---- learned PI-line initialiser (no counterpart in the reference) -----------------------
+ * A 3 -> 64 -> 64 -> 64 -> 64 -> 2 SiLU network mapping (r/0.25, cos psi, sin psi), with r and
+ * psi = phi - 2 pi z the voxel's normalised radius and helix-relative angle, to 4x the offsets
+ * of the PI-line endpoints from the on-axis solution (sb = 2 pi z - pi/2, st = 2 pi z + pi/2).
+ * The network lives in the context; CTRECON_PI_LEARNED uses it as the start of the FP64 Newton
+ * solve. Parameters: per layer W[out][in] row-major then b[out], FP32 (inference in BF16). */
+int ctrecon_pinet_num_params(void);
+/* Trains from scratch on n_pairs FP64-solved (point, endpoint) pairs, area-uniform in the disc
+ * of normalised radius r_max (ObjR/ScanR or more), with Adam; synchronous. */
+ctrecon_status ctrecon_pinet_train(ctrecon_ctx* ctx, void* stream, int n_pairs, int batch,
+                                   int epochs, double r_max, uint64_t seed, float* final_loss);
+ctrecon_status ctrecon_pinet_get_params(ctrecon_ctx* ctx, float* host_params, int n);
+ctrecon_status ctrecon_pinet_set_params(ctrecon_ctx* ctx, const float* host_params, int n,
+                                        double r_max);
+/* Mean (over n samples) squared error of the current parameters and its gradient (device
+ * buffers: d_feat n x 3, d_targ n x 2, d_grad ctrecon_pinet_num_params(), d_loss 1). */
+ctrecon_status ctrecon_pinet_loss_grad(ctrecon_ctx* ctx, void* stream, const float* d_feat,
+                                       const float* d_targ, int n, float* d_grad,
+                                       float* d_loss);
+/* Network outputs (n x 2) of the BF16 inference kernel for n feature triples. */
+ctrecon_status ctrecon_pinet_predict(ctrecon_ctx* ctx, void* stream, const float* d_feat, int n,
+                                     float* d_out);
+
 /* ---- tables and helpers (host only, no GPU needed) --------------------------------------- */
 
 /* Number of kappa lines AL = 2*ceil(0.65*ZL)+1 (KatsevichFiltering.m:103-104). */
@@ -188,6 +240,11 @@ int ctrecon_num_kappa(int zl);
 ctrecon_status ctrecon_filter_tables(const ctrecon_filter_params* p, int* r0, int* r1,
                                      double* wa, double* wb, int* b, int* e, double* gb,
                                      double* ge);
+
+/* Filtering coefficient tau of FindTau.m:6-22: the root in [0, 0.5] of
+ * t*cos(am) - cos(t*am) + 1 - t with am = 2*pi - 2*acos(ratio), ratio = ObjR/ScanR, found by
+ * the script's bisection until |f| <= tol (the script uses ratio 2/3 and tol 1e-4). */
+ctrecon_status ctrecon_find_tau(double ratio, double tol, double* tau);
 
 /* Detector sizing of FunctionKat_v6.m:49-57 (with its PI = 3.1415926). */
 void ctrecon_geometry_sizing(double scan_r, double std_dis, double helic_p, double obj_r,

@@ -423,6 +423,23 @@ int orc_filter_view_stages(const orc_filter_params* fp, const double* Proj, int 
 }
 
 /* ------------------------------------------------------------------------------ */
+/* Filtering coefficient: FindTau.m:6-22 (MATLAB's built-in pi)                       */
+/* ------------------------------------------------------------------------------ */
+double orc_find_tau(double ratio, double tol) {
+    const double pi = 3.141592653589793;
+    double am = 2 * pi - 2 * acos(ratio); /* :7 */
+    double tu = 0.5, td = 0, delta = 1, t = 0;
+    while (delta > tol) { /* :13-22 */
+        t = (td + tu) / 2;
+        double f = t * cos(am) - cos(t * am) + 1 - t;
+        delta = fabs(f);
+        if (f > 0) tu = t;
+        else td = t;
+    }
+    return t;
+}
+
+/* ------------------------------------------------------------------------------ */
 /* PI segment: KatsevichBkProj.cpp:283-312                                           */
 /* ------------------------------------------------------------------------------ */
 void orc_pisegment(double x, double y, double z, double* BAngle, double* TAngle) {

@@ -78,6 +78,11 @@ int orc_filter(const orc_filter_params* fp, const double* Proj, double* FProj, i
 int orc_filter_view_stages(const orc_filter_params* fp, const double* Proj, int p,
                            double* GF, double* conv_in, double* conv_out);
 
+/* ---- filtering coefficient: FindTau.m:6-22 ----
+ * Bisection on [0, 0.5] for t*cos(am) - cos(t*am) + 1 - t = 0 with am = 2*pi - 2*acos(ratio)
+ * (ratio = ObjR/ScanR; the script uses 2/3), stopping when |f| <= tol (the script: 1e-4). */
+double orc_find_tau(double ratio, double tol);
+
 /* ---- PI line: KatsevichBkProj.cpp:283-312 ---- */
 void orc_pisegment(double x, double y, double z, double* BAngle, double* TAngle);
 

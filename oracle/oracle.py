@@ -145,6 +145,14 @@ def filter_view_stages(fp: FilterParams, proj: np.ndarray, p: int):
     return gf, xin, xout
 
 
+def find_tau(ratio=2.0 / 3.0, tol=1e-4):
+    """FindTau.m:6-22."""
+    L = lib()
+    L.orc_find_tau.restype = ctypes.c_double
+    L.orc_find_tau.argtypes = [ctypes.c_double, ctypes.c_double]
+    return L.orc_find_tau(ratio, tol)
+
+
 def pisegment(x, y, z):
     b, t = ctypes.c_double(), ctypes.c_double()
     lib().orc_pisegment(x, y, z, ctypes.byref(b), ctypes.byref(t))

@@ -29,7 +29,7 @@ def test_library_exports_every_declared_symbol():
     missing = [s for s in syms if not hasattr(L, s)]
     assert not missing, missing
     bound = {n for n, _, _ in _lib.SIGNATURES}
-    assert set(syms) <= bound | {"ctrecon_no_alloc"} or not (set(syms) - bound), set(syms) - bound
+    assert set(syms) <= bound, set(syms) - bound
 
 
 def test_abi_version_and_status_strings():
@@ -71,6 +71,17 @@ def test_filter_tables_match_oracle(oracle_mod, name):
     coef_e = np.take_along_axis(o["coef"], o["eAL"], axis=0)
     np.testing.assert_allclose(t["gb"], -o["bC"] / coef_b, rtol=1e-15)
     np.testing.assert_allclose(t["ge"], -o["eC"] / coef_e, rtol=1e-15)
+
+
+@pytest.mark.parametrize("ratio,tol", [(2.0 / 3.0, 1e-4), (0.2, 1e-4), (0.5, 1e-10)])
+def test_find_tau_matches_oracle(oracle_mod, ratio, tol):
+    """FindTau.m:6-22 (the script's own case is ratio 2/3, tolerance 1e-4)."""
+    t = ctypes.c_double()
+    assert _lib.lib().ctrecon_find_tau(ratio, tol, ctypes.byref(t)) == _lib.OK
+    assert t.value == oracle_mod.find_tau(ratio, tol)
+    am = 2 * np.pi - 2 * np.arccos(ratio)
+    assert abs(t.value * np.cos(am) - np.cos(t.value * am) + 1 - t.value) <= tol
+    assert 0 < t.value < 0.5
 
 
 def test_num_kappa_matches_reference():
