@@ -2,6 +2,8 @@
 // MEX-equivalent) and device (FP32) entry points.
 #include "internal.h"
 
+#include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -19,9 +21,19 @@ void DevBuf::release() {
     bytes = 0;
 }
 
+static std::atomic<unsigned long long> g_devbuf_epoch{0};
+unsigned long long devbuf_epoch() { return g_devbuf_epoch.load(); }
+
+Status upload_now(void* dst, const void* src, size_t bytes) {
+    CTR_CUDA(cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice));
+    CTR_CUDA(cudaDeviceSynchronize());
+    return Status::Ok();
+}
+
 Status DevBuf::ensure(size_t b, const char* what) {
     if (b <= bytes && ptr) return Status::Ok();
     release();
+    g_devbuf_epoch.fetch_add(1);
     if (b == 0) b = 16;
     cudaError_t e = cudaMalloc(&ptr, b);
     if (e != cudaSuccess) {
@@ -38,7 +50,30 @@ Status DevBuf::ensure(size_t b, const char* what) {
 template <class T>
 static Status upload(DevBuf& buf, const std::vector<T>& host, const char* what) {
     CTR_TRY(buf.ensure(host.size() * sizeof(T), what));
-    CTR_CUDA(cudaMemcpy(buf.ptr, host.data(), host.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return upload_now(buf.ptr, host.data(), host.size() * sizeof(T));
+}
+
+// Most-recently-used lookup in a plan list; `make` builds a new plan on a miss. The least
+// recently used plan is dropped when the list is full, after a device synchronisation (work
+// already queued may still read its tables).
+template <class Plan, class Match, class Make>
+static Status plan_lookup(std::vector<std::unique_ptr<Plan>>& list, Match match, Make make,
+                          Plan** out) {
+    for (size_t i = 0; i < list.size(); ++i) {
+        if (match(*list[i])) {
+            std::rotate(list.begin(), list.begin() + i, list.begin() + i + 1);
+            *out = list.front().get();
+            return Status::Ok();
+        }
+    }
+    std::unique_ptr<Plan> plan(new Plan());
+    CTR_TRY(make(*plan));
+    if (list.size() >= kPlanCacheSize) {
+        CTR_CUDA(cudaDeviceSynchronize());
+        list.pop_back();
+    }
+    list.insert(list.begin(), std::move(plan));
+    *out = list.front().get();
     return Status::Ok();
 }
 
@@ -47,16 +82,9 @@ static bool same_filter_params(const ctrecon_filter_params& a, const ctrecon_fil
 }
 
 Status get_filter_plan(ctrecon_ctx* ctx, const ctrecon_filter_params& p, FilterPlan** out) {
-    FilterPlan& plan = ctx->fplan;
-    if (ctx->fplan_valid && same_filter_params(plan.p, p)) {
-        *out = &plan;
-        return Status::Ok();
-    }
-    ctx->fplan_valid = false;
-    CTR_TRY(build_filter_plan(p, plan));
-    ctx->fplan_valid = true;
-    *out = &plan;
-    return Status::Ok();
+    return plan_lookup(
+        ctx->fplans, [&](const FilterPlan& f) { return same_filter_params(f.p, p); },
+        [&](FilterPlan& f) { return build_filter_plan(p, f); }, out);
 }
 
 Status build_filter_plan(const ctrecon_filter_params& p, FilterPlan& plan) {
@@ -93,16 +121,9 @@ Status get_bp_plan(ctrecon_ctx* ctx, const ctrecon_bp_geom& gin, BPPlan** out) {
     BPGeom g;
     std::memset(&g, 0, sizeof g);
     CTR_TRY(parse_bp_geom(gin, g));
-    BPPlan& plan = ctx->bplan;
-    if (ctx->bplan_valid && same_geom(plan.g, g)) {
-        *out = &plan;
-        return Status::Ok();
-    }
-    ctx->bplan_valid = false;
-    CTR_TRY(build_bp_plan(g, plan));
-    ctx->bplan_valid = true;
-    *out = &plan;
-    return Status::Ok();
+    return plan_lookup(
+        ctx->bplans, [&](const BPPlan& b) { return same_geom(b.g, g); },
+        [&](BPPlan& b) { return build_bp_plan(g, b); }, out);
 }
 
 Status build_bp_plan(const BPGeom& g, BPPlan& plan) {
@@ -167,6 +188,12 @@ static Status use_device(ctrecon_ctx* ctx) {
     return Status::Ok();
 }
 
+Status ctr::reset_device_flag(ctrecon_ctx* ctx, cudaStream_t s) {
+    CTR_TRY(ctx->ws_flag.ensure(256, "device error word"));
+    CTR_CUDA(cudaMemsetAsync(ctx->ws_flag.ptr, 0, sizeof(int), s));
+    return Status::Ok();
+}
+
 // After a synchronisation: the device error word is set by a bounded wait that gave up.
 static Status check_device_flag(ctrecon_ctx* ctx) {
     if (!ctx->ws_flag.ptr) return Status::Ok();
@@ -225,11 +252,21 @@ ctrecon_status ctrecon_ctx_create(int device, ctrecon_ctx** out) {
     ctx->device = device;
     Status s = use_device(ctx);
     if (s.ok()) {
-        e = cudaStreamCreateWithFlags(&ctx->host_stream, cudaStreamNonBlocking);
-        if (e != cudaSuccess) s = cuda_status(e, "cudaStreamCreate");
+        for (cudaStream_t* st : {&ctx->host_stream, &ctx->up_stream, &ctx->down_stream}) {
+            e = cudaStreamCreateWithFlags(st, cudaStreamNonBlocking);
+            if (e != cudaSuccess) {
+                s = cuda_status(e, "cudaStreamCreate");
+                break;
+            }
+        }
+    }
+    if (s.ok()) s = reset_device_flag(ctx, ctx->host_stream);
+    if (s.ok()) {
+        e = cudaStreamSynchronize(ctx->host_stream);
+        if (e != cudaSuccess) s = cuda_status(e, "cudaStreamSynchronize");
     }
     if (!s.ok()) {
-        delete ctx;
+        ctrecon_ctx_destroy(ctx);
         return finish(nullptr, s);
     }
     *out = ctx;
@@ -240,10 +277,12 @@ ctrecon_status ctrecon_ctx_create(int device, ctrecon_ctx** out) {
 void ctrecon_ctx_destroy(ctrecon_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
-    if (ctx->host_stream) {
-        cudaStreamSynchronize(ctx->host_stream);
-        cudaStreamDestroy(ctx->host_stream);
+    for (cudaStream_t st : {ctx->host_stream, ctx->up_stream, ctx->down_stream}) {
+        if (!st) continue;
+        cudaStreamSynchronize(st);
+        cudaStreamDestroy(st);
     }
+    for (cudaEvent_t e : ctx->events) cudaEventDestroy(e);
     delete ctx;
 }
 
@@ -366,6 +405,7 @@ ctrecon_status ctrecon_filter_dev_f32(ctrecon_ctx* ctx, void* stream,
     Status s = use_device(ctx);
     FilterPlan* plan = nullptr;
     if (s.ok()) s = get_filter_plan(ctx, *p, &plan);
+    if (s.ok()) s = reset_device_flag(ctx, (cudaStream_t)stream);
     if (s.ok())
         s = launch_filter(ctx, (cudaStream_t)stream, *plan, d_proj, 0, p->proj_number, d_fproj,
                           0, 0, p->proj_number);
@@ -381,6 +421,7 @@ ctrecon_status ctrecon_pi_dev(ctrecon_ctx* ctx, void* stream, const ctrecon_bp_g
     Status s = use_device(ctx);
     BPPlan* plan = nullptr;
     if (s.ok()) s = get_bp_plan(ctx, *g, &plan);
+    if (s.ok()) s = reset_device_flag(ctx, (cudaStream_t)stream);
     if (s.ok()) s = launch_pi(ctx, (cudaStream_t)stream, *plan, (PiRecord*)d_pitab, d_updates);
     return finish(ctx, s);
     API_END(ctx)
@@ -401,6 +442,7 @@ ctrecon_status ctrecon_bkproj_dev_f32(ctrecon_ctx* ctx, void* stream, const ctre
     if (s.ok() && !pit) {
         const size_t nvox = (size_t)plan->kp.NX * plan->kp.NY * plan->kp.NZ;
         s = ctx->ws_pitab.ensure(nvox * sizeof(PiRecord), "PI table");
+        if (s.ok()) s = reset_device_flag(ctx, st);
         if (s.ok()) s = launch_pi(ctx, st, *plan, ctx->ws_pitab.as<PiRecord>(), nullptr);
         pit = ctx->ws_pitab.as<PiRecord>();
     }
@@ -458,20 +500,79 @@ ctrecon_status ctrecon_sync(ctrecon_ctx* ctx, void* stream) {
 }
 
 // ---- host (FP64, MEX-equivalent) entry points -----------------------------------------------
-static Status host_filter_to_device(ctrecon_ctx* ctx, const ctrecon_filter_params& p,
-                                    const double* proj, float** d_fproj_out) {
-    cudaStream_t st = ctx->host_stream;
+// The host calls pipeline their transfers: projections go up in chunks of views on the up
+// stream (converted to FP32 there), each chunk is filtered on the host stream as soon as it
+// and its neighbour view are resident, and results go down on the down stream while later
+// chunks are still being filtered; the PI solve overlaps the FProj upload. With pinned host
+// buffers the copies run concurrently with the kernels (and H2D with D2H); with pageable
+// buffers each copy blocks the calling thread and the call degrades to sequential order.
+constexpr int kHostChunkViews = 256;
+
+// Clears the device error word before the host call's three streams start.
+static Status host_reset(ctrecon_ctx* ctx) {
+    CTR_TRY(reset_device_flag(ctx, ctx->host_stream));
+    CTR_CUDA(cudaStreamSynchronize(ctx->host_stream));
+    return Status::Ok();
+}
+
+static Status event_at(ctrecon_ctx* ctx, size_t i, cudaEvent_t* out) {
+    while (ctx->events.size() <= i) {
+        cudaEvent_t e;
+        CTR_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        ctx->events.push_back(e);
+    }
+    *out = ctx->events[i];
+    return Status::Ok();
+}
+
+// Uploads proj (FP64 host) and filters it into ctx->ws_c (FP32, device); if fproj_host is not
+// NULL the result also comes down into it (FP64). Returns after enqueueing, except that it
+// waits for the down copies when fproj_host is given. The host stream holds the filter work.
+static Status host_filter_pipeline(ctrecon_ctx* ctx, const ctrecon_filter_params& p,
+                                   const double* proj, double* fproj_host) {
     FilterPlan* plan = nullptr;
     CTR_TRY(get_filter_plan(ctx, p, &plan));
-    const size_t n = (size_t)p.proj_number * p.yl * p.zl;
+    const int P = p.proj_number;
+    const size_t S = (size_t)p.yl * p.zl, n = S * P;
     CTR_TRY(ctx->ws_a.ensure(n * sizeof(double), "FP64 staging"));
     CTR_TRY(ctx->ws_b.ensure(n * sizeof(float), "projections"));
     CTR_TRY(ctx->ws_c.ensure(n * sizeof(float), "filtered projections"));
-    CTR_CUDA(cudaMemcpyAsync(ctx->ws_a.ptr, proj, n * sizeof(double), cudaMemcpyHostToDevice, st));
-    CTR_TRY(launch_convert_f64_to_f32(st, ctx->ws_a.as<double>(), ctx->ws_b.as<float>(), n));
-    CTR_TRY(launch_filter(ctx, st, *plan, ctx->ws_b.as<float>(), 0, p.proj_number,
-                          ctx->ws_c.as<float>(), 0, 0, p.proj_number));
-    *d_fproj_out = ctx->ws_c.as<float>();
+    if (fproj_host) CTR_TRY(ctx->ws_d.ensure(n * sizeof(double), "FP64 result staging"));
+    const int nch = (P + kHostChunkViews - 1) / kHostChunkViews;
+    cudaStream_t up = ctx->up_stream, comp = ctx->host_stream, down = ctx->down_stream;
+    for (int c = 0; c < nch; ++c) {
+        const size_t v0 = (size_t)c * kHostChunkViews, v1 = std::min<size_t>(P, v0 + kHostChunkViews);
+        CTR_CUDA(cudaMemcpyAsync(ctx->ws_a.as<double>() + v0 * S, proj + v0 * S,
+                                 (v1 - v0) * S * sizeof(double), cudaMemcpyHostToDevice, up));
+        CTR_TRY(launch_convert_f64_to_f32(up, ctx->ws_a.as<double>() + v0 * S,
+                                          ctx->ws_b.as<float>() + v0 * S, (v1 - v0) * S));
+        cudaEvent_t e = nullptr;
+        CTR_TRY(event_at(ctx, c, &e));
+        CTR_CUDA(cudaEventRecord(e, up));
+    }
+    for (int c = 0; c < nch; ++c) {
+        const int v0 = c * kHostChunkViews, v1 = std::min(P, v0 + kHostChunkViews);
+        cudaEvent_t need = nullptr;  // this chunk and the first view of the next (derivative neighbour)
+        CTR_TRY(event_at(ctx, std::min(c + 1, nch - 1), &need));
+        CTR_CUDA(cudaStreamWaitEvent(comp, need, 0));
+        CTR_TRY(launch_filter(ctx, comp, *plan, ctx->ws_b.as<float>(), 0, P,
+                              ctx->ws_c.as<float>(), 0, v0, v1));
+        if (fproj_host) {
+            const size_t o = (size_t)v0 * S, m = (size_t)(v1 - v0) * S;
+            CTR_TRY(launch_convert_f32_to_f64(comp, ctx->ws_c.as<float>() + o,
+                                              ctx->ws_d.as<double>() + o, m));
+            cudaEvent_t done = nullptr;
+            CTR_TRY(event_at(ctx, nch + c, &done));
+            CTR_CUDA(cudaEventRecord(done, comp));
+            CTR_CUDA(cudaStreamWaitEvent(down, done, 0));
+            CTR_CUDA(cudaMemcpyAsync(fproj_host + o, ctx->ws_d.as<double>() + o,
+                                     m * sizeof(double), cudaMemcpyDeviceToHost, down));
+        }
+    }
+    if (fproj_host) {
+        CTR_CUDA(cudaStreamSynchronize(down));
+        CTR_CUDA(cudaStreamSynchronize(comp));
+    }
     return Status::Ok();
 }
 
@@ -482,18 +583,31 @@ static Status check_filter_bp_shapes(const ctrecon_filter_params& p, const BPGeo
     return Status::Ok();
 }
 
-static Status host_bkproj_from_device(ctrecon_ctx* ctx, BPPlan& plan, const float* d_fproj,
-                                      double* image) {
-    cudaStream_t st = ctx->host_stream;
+// PI solve (on the down stream, overlapping the uploads), then the backprojection of d_fproj
+// into the FP64 image (uploaded, written in place, downloaded). `ready` is the event after
+// which d_fproj is complete (recorded by the caller), or NULL if it already is.
+static Status host_bkproj_pipeline(ctrecon_ctx* ctx, BPPlan& plan, const float* d_fproj,
+                                   cudaEvent_t ready, double* image) {
+    cudaStream_t up = ctx->up_stream, comp = ctx->host_stream, side = ctx->down_stream;
     const size_t nvox = (size_t)plan.kp.NX * plan.kp.NY * plan.kp.NZ;
     CTR_TRY(ctx->ws_pitab.ensure(nvox * sizeof(PiRecord), "PI table"));
-    CTR_TRY(ctx->ws_d.ensure(nvox * sizeof(double), "FP64 image"));
-    CTR_CUDA(cudaMemcpyAsync(ctx->ws_d.ptr, image, nvox * sizeof(double), cudaMemcpyHostToDevice, st));
-    CTR_TRY(launch_pi(ctx, st, plan, ctx->ws_pitab.as<PiRecord>(), nullptr));
-    CTR_TRY(launch_bkproj_f64out(ctx, st, plan, d_fproj, ctx->ws_pitab.as<PiRecord>(),
-                                 ctx->ws_d.as<double>()));
-    CTR_CUDA(cudaMemcpyAsync(image, ctx->ws_d.ptr, nvox * sizeof(double), cudaMemcpyDeviceToHost, st));
-    CTR_CUDA(cudaStreamSynchronize(st));
+    CTR_TRY(ctx->ws_e.ensure(nvox * sizeof(double), "FP64 image"));
+    CTR_TRY(launch_pi(ctx, side, plan, ctx->ws_pitab.as<PiRecord>(), nullptr));
+    cudaEvent_t pi_done = nullptr, img_up = nullptr;
+    CTR_TRY(event_at(ctx, 0, &pi_done));
+    CTR_TRY(event_at(ctx, 1, &img_up));
+    CTR_CUDA(cudaEventRecord(pi_done, side));
+    CTR_CUDA(cudaMemcpyAsync(ctx->ws_e.ptr, image, nvox * sizeof(double), cudaMemcpyHostToDevice, up));
+    CTR_CUDA(cudaEventRecord(img_up, up));
+    if (ready) CTR_CUDA(cudaStreamWaitEvent(comp, ready, 0));
+    CTR_CUDA(cudaStreamWaitEvent(comp, pi_done, 0));
+    CTR_CUDA(cudaStreamWaitEvent(comp, img_up, 0));
+    CTR_TRY(launch_bkproj_f64out(ctx, comp, plan, d_fproj, ctx->ws_pitab.as<PiRecord>(),
+                                 ctx->ws_e.as<double>()));
+    CTR_CUDA(cudaMemcpyAsync(image, ctx->ws_e.ptr, nvox * sizeof(double), cudaMemcpyDeviceToHost, comp));
+    CTR_CUDA(cudaStreamSynchronize(comp));
+    CTR_CUDA(cudaStreamSynchronize(side));
+    CTR_CUDA(cudaStreamSynchronize(up));
     return check_device_flag(ctx);
 }
 
@@ -504,16 +618,8 @@ ctrecon_status ctrecon_filter_host_f64(ctrecon_ctx* ctx, const ctrecon_filter_pa
     if (!p || !proj || !fproj)
         return finish(ctx, make_status(CTRECON_ERR_INVALID_ARGUMENT, "NULL argument"));
     Status s = use_device(ctx);
-    float* d_f = nullptr;
-    if (s.ok()) s = host_filter_to_device(ctx, *p, proj, &d_f);
-    const size_t n = (size_t)p->proj_number * p->yl * p->zl;
-    if (s.ok()) s = launch_convert_f32_to_f64(ctx->host_stream, d_f, ctx->ws_a.as<double>(), n);
-    if (s.ok()) {
-        cudaError_t e = cudaMemcpyAsync(fproj, ctx->ws_a.ptr, n * sizeof(double),
-                                        cudaMemcpyDeviceToHost, ctx->host_stream);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->host_stream);
-        if (e != cudaSuccess) s = cuda_status(e, "filter result copy");
-    }
+    if (s.ok()) s = host_reset(ctx);
+    if (s.ok()) s = host_filter_pipeline(ctx, *p, proj, fproj);
     if (s.ok()) s = check_device_flag(ctx);
     return finish(ctx, s);
     API_END(ctx)
@@ -528,18 +634,28 @@ ctrecon_status ctrecon_bkproj_host_f64(ctrecon_ctx* ctx, const ctrecon_bp_geom* 
     Status s = use_device(ctx);
     BPPlan* plan = nullptr;
     if (s.ok()) s = get_bp_plan(ctx, *g, &plan);
+    if (s.ok()) s = host_reset(ctx);
     if (s.ok()) {
-        const size_t n = (size_t)plan->g.ProjNum * plan->g.YL * plan->g.ZL;
-        cudaStream_t st = ctx->host_stream;
+        const size_t S = (size_t)plan->g.YL * plan->g.ZL, n = S * plan->g.ProjNum;
+        cudaStream_t up = ctx->up_stream;
         s = ctx->ws_a.ensure(n * sizeof(double), "FP64 staging");
         if (s.ok()) s = ctx->ws_c.ensure(n * sizeof(float), "filtered projections");
-        if (s.ok()) {
-            cudaError_t e = cudaMemcpyAsync(ctx->ws_a.ptr, fproj, n * sizeof(double),
-                                            cudaMemcpyHostToDevice, st);
+        for (size_t v0 = 0; s.ok() && v0 < (size_t)plan->g.ProjNum; v0 += kHostChunkViews) {
+            const size_t m = std::min<size_t>(kHostChunkViews, plan->g.ProjNum - v0) * S;
+            cudaError_t e = cudaMemcpyAsync(ctx->ws_a.as<double>() + v0 * S, fproj + v0 * S,
+                                            m * sizeof(double), cudaMemcpyHostToDevice, up);
             if (e != cudaSuccess) s = cuda_status(e, "FProj upload");
+            if (s.ok())
+                s = launch_convert_f64_to_f32(up, ctx->ws_a.as<double>() + v0 * S,
+                                              ctx->ws_c.as<float>() + v0 * S, m);
         }
-        if (s.ok()) s = launch_convert_f64_to_f32(st, ctx->ws_a.as<double>(), ctx->ws_c.as<float>(), n);
-        if (s.ok()) s = host_bkproj_from_device(ctx, *plan, ctx->ws_c.as<float>(), image);
+        cudaEvent_t ready = nullptr;
+        if (s.ok()) s = event_at(ctx, 2, &ready);
+        if (s.ok()) {
+            cudaError_t e = cudaEventRecord(ready, up);
+            if (e != cudaSuccess) s = cuda_status(e, "cudaEventRecord");
+        }
+        if (s.ok()) s = host_bkproj_pipeline(ctx, *plan, ctx->ws_c.as<float>(), ready, image);
     }
     return finish(ctx, s);
     API_END(ctx)
@@ -556,9 +672,10 @@ ctrecon_status ctrecon_recon_host_f64(ctrecon_ctx* ctx, const ctrecon_filter_par
     BPPlan* plan = nullptr;
     if (s.ok()) s = get_bp_plan(ctx, *g, &plan);
     if (s.ok()) s = check_filter_bp_shapes(*p, plan->g);
-    float* d_f = nullptr;
-    if (s.ok()) s = host_filter_to_device(ctx, *p, proj, &d_f);
-    if (s.ok()) s = host_bkproj_from_device(ctx, *plan, d_f, image);
+    if (s.ok()) s = host_reset(ctx);
+    if (s.ok()) s = host_filter_pipeline(ctx, *p, proj, nullptr);
+    // the filter's work is ordered on the host stream, where the backprojection runs too
+    if (s.ok()) s = host_bkproj_pipeline(ctx, *plan, ctx->ws_c.as<float>(), nullptr, image);
     return finish(ctx, s);
     API_END(ctx)
 }

@@ -38,7 +38,9 @@ struct ctrecon_batch {
     std::vector<size_t> pit_off;      // PiRecord offset of each scan in `pitab`
     DevBuf pitab, scans_dev, counter, updates;
     long long total_tiles = 0;
-    std::vector<const void*> key;     // pointers the graph was captured with
+    // what the graph was captured with: the buffer pointers, the context options, the
+    // learned-initialiser version and the work-buffer allocation epoch
+    std::vector<unsigned long long> key;
     int runs_with_key = 0;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -59,6 +61,7 @@ static ctrecon_status bfinish(ctrecon_ctx* ctx, const Status& s) {
 static Status enqueue(ctrecon_batch* b, cudaStream_t s, const float* const* d_proj,
                       float* const* d_fproj, float* const* d_image) {
     ctrecon_ctx* ctx = b->ctx;
+    CTR_TRY(reset_device_flag(ctx, s));
     for (int k = 0; k < b->n; ++k) {
         const int i = b->order[k];
         const int P = b->fp[i].proj_number;
@@ -169,12 +172,17 @@ ctrecon_status ctrecon_batch_run_dev(ctrecon_batch* b, void* stream, const float
         if (use_graph && !s)
             return bfinish(ctx, make_status(CTRECON_ERR_INVALID_ARGUMENT,
                                             "graph replay needs a created stream, not stream 0"));
-        std::vector<const void*> key;
+        std::vector<unsigned long long> key;
         for (int i = 0; i < b->n; ++i) {
-            key.push_back(d_proj[i]);
-            key.push_back(d_fproj[i]);
-            key.push_back(d_image[i]);
+            key.push_back((uintptr_t)d_proj[i]);
+            key.push_back((uintptr_t)d_fproj[i]);
+            key.push_back((uintptr_t)d_image[i]);
         }
+        key.push_back((unsigned long long)ctx->opt_hilbert);
+        key.push_back((unsigned long long)ctx->opt_pi);
+        key.push_back((unsigned long long)ctx->opt_filter_chunk);
+        key.push_back((unsigned long long)ctx->pinet.version);
+        key.push_back(devbuf_epoch());
         if (key != b->key) {
             Status st = upload_scans(b, s, d_fproj, d_image);
             if (!st.ok()) return bfinish(ctx, st);
@@ -219,8 +227,10 @@ ctrecon_status ctrecon_batch_updates(ctrecon_batch* b, unsigned long long* host_
         cudaStream_t s = ctx->host_stream;
         const int saved = ctx->opt_pi;
         ctx->opt_pi = CTRECON_PI_BISECT;  // the loop count of the reference's own solve
-        Status st;
-        cudaError_t e0 = cudaMemsetAsync(b->updates.ptr, 0, sizeof(unsigned long long) * b->n, s);
+        Status st = reset_device_flag(ctx, s);
+        cudaError_t e0 = st.ok() ? cudaMemsetAsync(b->updates.ptr, 0,
+                                                   sizeof(unsigned long long) * b->n, s)
+                                 : cudaSuccess;
         if (e0 != cudaSuccess) st = cuda_status(e0, "batch counts");
         for (int i = 0; st.ok() && i < b->n; ++i)
             st = launch_pi_stats(ctx, s, *b->bplans[i], b->pitab.as<PiRecord>() + b->pit_off[i],

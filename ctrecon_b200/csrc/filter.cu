@@ -69,6 +69,7 @@ __global__ void k_deriv_rebin(const float* __restrict__ proj, int proj_view0, in
     if (j < 2) { jl = 0; jr = 2; }
     else if (j > YL - 3) { jl = YL - 3; jr = YL - 1; }
     const float2 cy = cuy[j];  // (u coefficient, y coordinate)
+#pragma unroll 4
     for (int k = 0; k < ZL; ++k) {
         int kl = k - 1, kr = k + 1;  // v stencil, same edge rule (:85-95)
         if (k < 2) { kl = 0; kr = 2; }
@@ -79,6 +80,7 @@ __global__ void k_deriv_rebin(const float* __restrict__ proj, int proj_view0, in
         g = fmaf(zcv[k] * cy.y, Pv[(size_t)kr * YL + j] - Pv[(size_t)kl * YL + j], g);
         gf[k * T + tid] = g;
     }
+#pragma unroll 4
     for (int a = 0; a < AL; ++a) {
         const FwEntry f = fw[(size_t)a * YL + j];
         store_kappa(X, xv + (size_t)a * YLp + j, plane,
@@ -216,10 +218,6 @@ Status launch_filter(ctrecon_ctx* ctx, cudaStream_t s, FilterPlan& plan, const f
     // 4 bytes per kappa sample in every format (FP32, TF32, or BF16 hi + lo planes)
     CTR_TRY(ctx->ws_kappa.ensure((size_t)chunk * AL * YLp * sizeof(float), "filter kappa rows"));
     void* X = ctx->ws_kappa.ptr;
-    if (mode != CTRECON_HILBERT_FP32) {
-        CTR_TRY(ctx->ws_flag.ensure(256, "device error word"));
-        CTR_CUDA(cudaMemsetAsync(ctx->ws_flag.ptr, 0, sizeof(int), s));
-    }
 
     // K1 launch shape: one thread per column, ZL floats of shared memory per thread
     int tj = 128;

@@ -262,6 +262,7 @@ k_hilbert_tc(const __grid_constant__ CUtensorMap tA0, const __grid_constant__ CU
             if (i < p.YL) {
                 const float* row = tr + lane * p.ALs;
                 float* o = p.out + (size_t)v * p.ZL * p.YL + i;
+#pragma unroll 8
                 for (int k = 0; k < p.ZL; ++k) {
                     const BkEntry e = p.bk[(size_t)k * p.YL + i];
                     o[(size_t)k * p.YL] = fmaf(e.gb, row[e.b], e.ge * row[e.e]);
@@ -353,8 +354,8 @@ static Status ensure_toeplitz(FilterPlan& plan, int mode, DevBuf& T0, DevBuf& T1
             }
         CTR_TRY(T0.ensure(n * 2, "Toeplitz hi"));
         CTR_TRY(T1.ensure(n * 2, "Toeplitz lo"));
-        CTR_CUDA(cudaMemcpy(T0.ptr, hi.data(), n * 2, cudaMemcpyHostToDevice));
-        CTR_CUDA(cudaMemcpy(T1.ptr, lo.data(), n * 2, cudaMemcpyHostToDevice));
+        CTR_TRY(upload_now(T0.ptr, hi.data(), n * 2));
+        CTR_TRY(upload_now(T1.ptr, lo.data(), n * 2));
     } else {
         std::vector<float> t(n, 0.f);
         for (int i = 0; i < YL; ++i)
@@ -363,7 +364,7 @@ static Status ensure_toeplitz(FilterPlan& plan, int mode, DevBuf& T0, DevBuf& T1
                 if (m & 1) t[(size_t)i * YLp + j] = tf32_rn((float)plan.t.h[(size_t)(m + YL - 1)]);
             }
         CTR_TRY(T0.ensure(n * 4, "Toeplitz tf32"));
-        CTR_CUDA(cudaMemcpy(T0.ptr, t.data(), n * 4, cudaMemcpyHostToDevice));
+        CTR_TRY(upload_now(T0.ptr, t.data(), n * 4));
     }
     have_mode = mode;
     return Status::Ok();
@@ -378,7 +379,7 @@ Status launch_hilbert_tc(ctrecon_ctx* ctx, cudaStream_t s, FilterPlan& plan, con
         return make_status(CTRECON_ERR_UNSUPPORTED,
                            "tensor-core Hilbert needs AL <= 256 kappa lines (ZL <= 196)");
     CTR_TRY(ensure_toeplitz(plan, mode, plan.tcT0, plan.tcT1, plan.tc_mode));
-    CTR_TRY(ctx->ws_flag.ensure(256, "device error word"));
+    if (!ctx->ws_flag.ptr) return make_status(CTRECON_ERR_INTERNAL, "device error word not set up");
     const bool bf = (mode == CTRECON_HILBERT_BF16X3);
     const int vpt = hilbert_tc_views_per_tile(AL);
     const int ntile = (vpt * AL + 15) / 16 * 16;

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -47,6 +48,14 @@ struct DevBuf {
     void release();
     template <class T> T* as() const { return static_cast<T*>(ptr); }
 };
+// Number of device allocations made by DevBuf::ensure so far (process-wide); a captured CUDA
+// graph that baked in work-buffer pointers is stale once this has moved.
+unsigned long long devbuf_epoch();
+// Copies host -> device and waits for the device: a synchronous cudaMemcpy from pageable
+// memory may return before its DMA lands, and the kernels reading the buffer run on other
+// (non-blocking) streams.
+Status upload_now(void* dst, const void* src, size_t bytes);
+constexpr size_t kPlanCacheSize = 32;
 
 // ---- filter tables -----------------------------------------------------------------------
 // forward rebin entry per (kappa row a, column y): X = wa*GF[r0] + wb*GF[r1]
@@ -143,15 +152,18 @@ struct ctrecon_ctx {
     int opt_bp_variant = 0;
     int opt_verbose = 0;
     cudaStream_t host_stream = nullptr;  // stream for the synchronous host calls
-    // cached plans and work buffers
-    ctr::FilterPlan fplan;
-    bool fplan_valid = false;
-    ctr::BPPlan bplan;
-    bool bplan_valid = false;
+    cudaStream_t up_stream = nullptr;    // host -> device copies of the host calls
+    cudaStream_t down_stream = nullptr;  // device -> host copies of the host calls
+    std::vector<cudaEvent_t> events;     // reusable (timing-disabled) events of the host calls
+    // plans by geometry, most recently used first; a plan is never rebuilt in place (kernels
+    // still queued may read it) and evicting one synchronises the device first
+    std::vector<std::unique_ptr<ctr::FilterPlan>> fplans;
+    std::vector<std::unique_ptr<ctr::BPPlan>> bplans;
     ctr::DevBuf ws_kappa;    // kappa-row chunk buffer of the filter
     ctr::DevBuf ws_pitab;    // PI table when the caller does not pass one
     ctr::DevBuf ws_count;    // update counter
     ctr::DevBuf ws_a, ws_b, ws_c, ws_d;  // host-call staging (f64 in, f32, f32 out, f64 out)
+    ctr::DevBuf ws_e;        // FP64 image of the host backprojection
     ctr::DevBuf ws_ell;      // phantom ellipsoids
     ctr::DevBuf ws_flag;     // device error word
     ctr::PinetState pinet;   // learned PI-line initialiser
@@ -162,6 +174,10 @@ Status get_filter_plan(ctrecon_ctx* ctx, const ctrecon_filter_params& p, FilterP
 Status get_bp_plan(ctrecon_ctx* ctx, const ctrecon_bp_geom& g, BPPlan** out);
 Status build_filter_plan(const ctrecon_filter_params& p, FilterPlan& plan);
 Status build_bp_plan(const BPGeom& g, BPPlan& plan);
+// Clears the device error word on stream s (allocating it on first use). Every entry point
+// that launches a kernel with a bounded wait calls it once before its launches, so the word
+// reports the waits that gave up since the last such call.
+Status reset_device_flag(ctrecon_ctx* ctx, cudaStream_t s);
 
 // kernel launchers (filter.cu, pi.cu, bkproj.cu, phantom.cu)
 Status launch_filter(ctrecon_ctx* ctx, cudaStream_t s, FilterPlan& plan, const float* d_proj,

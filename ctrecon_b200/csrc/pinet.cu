@@ -244,7 +244,7 @@ Status pinet_ensure(ctrecon_ctx* ctx) {
     CTR_TRY(P.grad.ensure(kPinetParamsPad * sizeof(float) + 64, "gradient"));
     std::vector<float> th;
     pinet_init_params(th, 12345);
-    CTR_CUDA(cudaMemcpy(P.theta.ptr, th.data(), kPinetParams * sizeof(float), cudaMemcpyHostToDevice));
+    CTR_TRY(upload_now(P.theta.ptr, th.data(), kPinetParams * sizeof(float)));
     P.trained = false;
     return Status::Ok();
 }
@@ -368,8 +368,11 @@ ctrecon_status ctrecon_pinet_get_params(ctrecon_ctx* ctx, float* host, int n) {
         cudaSetDevice(ctx->device);
         Status s = pinet_ensure(ctx);
         if (s.ok()) {
-            cudaError_t e = cudaMemcpy(host, ctx->pinet.theta.ptr, kPinetParams * sizeof(float),
-                                       cudaMemcpyDeviceToHost);
+            // training runs on the caller's stream: wait for all of it
+            cudaError_t e = cudaDeviceSynchronize();
+            if (e == cudaSuccess)
+                e = cudaMemcpy(host, ctx->pinet.theta.ptr, kPinetParams * sizeof(float),
+                               cudaMemcpyDeviceToHost);
             if (e != cudaSuccess) s = cuda_status(e, "network parameters");
         }
         return pinet_finish(ctx, s);
@@ -383,9 +386,9 @@ ctrecon_status ctrecon_pinet_set_params(ctrecon_ctx* ctx, const float* host, int
         cudaSetDevice(ctx->device);
         Status s = pinet_ensure(ctx);
         if (s.ok()) {
-            cudaError_t e = cudaMemcpy(ctx->pinet.theta.ptr, host, kPinetParams * sizeof(float),
-                                       cudaMemcpyHostToDevice);
+            cudaError_t e = cudaDeviceSynchronize();  // no queued kernel still reads them
             if (e != cudaSuccess) s = cuda_status(e, "network parameters");
+            else s = upload_now(ctx->pinet.theta.ptr, host, kPinetParams * sizeof(float));
         }
         if (s.ok()) {
             ctx->pinet.trained = true;
@@ -413,7 +416,9 @@ ctrecon_status ctrecon_pinet_predict(ctrecon_ctx* ctx, void* stream, const float
     if (!ctx || !d_feat || !d_out || n < 1) return CTRECON_ERR_INVALID_ARGUMENT;
     PINET_GUARD({
         cudaSetDevice(ctx->device);
-        return pinet_finish(ctx, pinet_predict(ctx, (cudaStream_t)stream, d_feat, n, d_out));
+        Status s = reset_device_flag(ctx, (cudaStream_t)stream);
+        if (s.ok()) s = pinet_predict(ctx, (cudaStream_t)stream, d_feat, n, d_out);
+        return pinet_finish(ctx, s);
     })
 }
 
@@ -425,6 +430,7 @@ ctrecon_status ctrecon_pi_dev_stats(ctrecon_ctx* ctx, void* stream, const ctreco
         cudaSetDevice(ctx->device);
         BPPlan* plan = nullptr;
         Status s = get_bp_plan(ctx, *g, &plan);
+        if (s.ok()) s = reset_device_flag(ctx, (cudaStream_t)stream);
         if (s.ok())
             s = launch_pi_stats(ctx, (cudaStream_t)stream, *plan, (PiRecord*)d_pitab, d_updates,
                                 d_iters);

@@ -229,8 +229,7 @@ Status pinet_prepare(ctrecon_ctx* ctx, cudaStream_t s) {
 static Status launch_infer(ctrecon_ctx* ctx, cudaStream_t s, const BPParams& kp, long long n,
                            const float* feat, float2* raw, float* guess) {
     CTR_TRY(pinet_prepare(ctx, s));
-    CTR_TRY(ctx->ws_flag.ensure(256, "device error word"));
-    CTR_CUDA(cudaMemsetAsync(ctx->ws_flag.ptr, 0, sizeof(int), s));
+    if (!ctx->ws_flag.ptr) return make_status(CTRECON_ERR_INTERNAL, "device error word not set up");
     CTR_CUDA(cudaFuncSetAttribute(k_pinet_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmBytes));
     const long long ntiles = (n + kT - 1) / kT;
     const int grid = (int)std::min<long long>(ntiles, persistent_blocks());
