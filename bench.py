@@ -54,8 +54,9 @@ def parse():
     ap.add_argument("--config", default="c2")
     ap.add_argument("--hilbert", default="fp32", choices=["fp32", "bf16x3", "tf32"])
     ap.add_argument("--pi", default="bisect", choices=["bisect", "newton", "learned"])
-    ap.add_argument("--bp-variant", type=int, default=0,
-                    help="backprojector form: 0-2 second form tile shapes, 100 first form")
+    ap.add_argument("--bp-variant", type=int, default=2,
+                    help="backprojector form: 0, 1 per-cell records (4 / 8 views per block), "
+                         "2-4 second form tile shapes, 100 first form")
     ap.add_argument("--batched", action="store_true",
                     help="16 uneven scans (c4): one-at-a-time vs one batched graph replay")
     ap.add_argument("--no-e2e", action="store_true")

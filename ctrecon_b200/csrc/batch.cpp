@@ -153,7 +153,7 @@ void ctrecon_batch_destroy(ctrecon_batch* b) {
 }
 
 ctrecon_status ctrecon_batch_set_variant(ctrecon_batch* b, int variant) {
-    if (!b || variant < 0 || variant > 2) return CTRECON_ERR_INVALID_ARGUMENT;
+    if (!b || variant < 0 || variant > 4) return CTRECON_ERR_INVALID_ARGUMENT;
     if (variant != b->variant) {
         b->variant = variant;
         b->key.clear();  // tile counts change: rebuild the scan table and the graph

@@ -1,7 +1,7 @@
-// bkproj2.cu -- K4, second form: the same voxel-driven backprojection as bkproj.cu
-// (KatsevichBkProj.cpp:164-265, FP32 interpolation and accumulation, identical endpoint rule),
-// reorganised for issue throughput:
+// bkproj2.cu -- K4, the tiled forms of the voxel-driven backprojection of bkproj.cu
+// (KatsevichBkProj.cpp:164-265, FP32 interpolation and accumulation, identical endpoint rule).
 //
+// Second form (bp_tile below), reorganised for issue throughput:
 //  * views are staged in blocks of NB with two shared-memory buffers: while block b is being
 //    accumulated, block b+1's footprints are already in flight (cp.async, one warp per detector
 //    row, no integer division), so each block costs three barriers instead of stalling on loads;
@@ -10,7 +10,11 @@
 //    the common case; the others take the checked path of bkproj.cu;
 //  * voxel z coordinates are generated, not held in registers, and the launch is bounded to
 //    three CTAs of 256 threads per SM.
-#include "internal.h"
+// Third form (bp_tile3.cuh): per-cell bilinear records and a rounding floor that
+// bring an update down to about a dozen instructions.
+//
+// Also the persistent batched kernel (either form) behind the batch API.
+#include "bp_tile3.cuh"
 
 #include <climits>
 
@@ -18,37 +22,11 @@ namespace ctr {
 
 namespace {
 
-constexpr int kTXY2 = 16;
+using namespace bp;
+constexpr int kTXY2 = kTXY;
 constexpr int kCap2 = 1024;  // shared floats per staged view
 
 struct Foot2 { int u0, v0, W, H; };
-
-__device__ __forceinline__ float ramp2(float s) {
-    float c = fminf(fmaxf(s, -1.f), 1.f);
-    return 0.5f + c - 0.5f * c * fabsf(c);
-}
-
-// single-instruction reciprocal and reciprocal square root (relative error ~2^-23)
-__device__ __forceinline__ float rcp_approx(float x) {
-    float r;
-    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
-    return r;
-}
-__device__ __forceinline__ float rsqrt_approx(float x) {
-    float r;
-    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
-    return r;
-}
-
-__device__ __forceinline__ void cp_async4(float* dst, const float* src) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(
-                     (uint32_t)__cvta_generic_to_shared(dst)),
-                 "l"(src)
-                 : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 }  // namespace
 
@@ -245,8 +223,8 @@ __device__ __forceinline__ void bp_tile(const BPParams& kp, const float* __restr
                         const int d1 = ti[k] + 1 - p;
                         if ((d0 | d1) < 0) continue;
                         float w = 1.f;
-                        if (d1 <= 1) w = ramp2(tf[k] + (float)(d1 - 1));
-                        else if (d0 <= 1) w = ramp2((float)d0 - bf[k]);
+                        if (d1 <= 1) w = ramp(tf[k] + (float)(d1 - 1));
+                        else if (d0 <= 1) w = ramp((float)d0 - bf[k]);
                         const float dz = fmaf((float)k, dzf, dz0);
                         const float v = fmaf(dz, kv, HalfZ);
                         const float rinv = rsqrt_approx(fmaf(dz, dz, r2));
@@ -290,53 +268,76 @@ k_bkproj2(BPParams kp, const float* __restrict__ fproj, const PiRecord* __restri
                           sh, tile);
 }
 
+template <int NB, typename OutT>
+__global__ void __launch_bounds__(256, 3)
+k_bkproj3(BPParams kp, const float* __restrict__ fproj, const PiRecord* __restrict__ pit,
+          const float4* __restrict__ views, const float* __restrict__ xyz,
+          OutT* __restrict__ image) {
+    extern __shared__ __align__(16) unsigned char dyn3[];
+    __shared__ Shared3<NB> sh;
+    tile3<NB, OutT>(kp, fproj, pit, views, xyz, image, blockIdx.x, blockIdx.y, blockIdx.z, sh,
+                    dyn3);
+}
+
+// Variants: 0, 1 = third form with blocks of 4 / 8 views; 2, 3, 4 = second form with
+// (TZ, NB) = (8, 8), (4, 8), (8, 4).
+__host__ __device__ constexpr int variant_tz(int variant) { return variant == 3 ? 4 : 8; }
+
 // Many scans in one persistent launch: the CTAs pull tiles of all scans from one atomic
 // counter (largest-first order is the caller's choice of scan order), so uneven scans share
 // the GPU without tails between them.
-template <int TZ, int NB>
+template <int FORM, int TZ, int NB>
 __global__ void __launch_bounds__(256, 3)
-k_bkproj2_batch(const BatchScanDev* __restrict__ scans, int n_scans, long long total_tiles,
-                unsigned long long* __restrict__ counter) {
-    extern __shared__ float tile[];
-    __shared__ BPShared<NB> sh;
+k_bkproj_batch(const BatchScanDev* __restrict__ scans, int n_scans, long long total_tiles,
+               unsigned long long* __restrict__ counter) {
+    extern __shared__ __align__(16) unsigned char dynb[];
+    __shared__ BPShared<NB> sh2;
+    __shared__ Shared3<NB> sh3;
+    __shared__ long long s_item;
     for (;;) {
         __syncthreads();
-        if (threadIdx.x == 0) sh.s_item = (int)atomicAdd(counter, 1ull);
+        if (threadIdx.x == 0) s_item = (long long)atomicAdd(counter, 1ull);
         __syncthreads();
-        const long long item = sh.s_item;
+        const long long item = s_item;
         if (item >= total_tiles) break;
         int s = 0;
         while (s + 1 < n_scans && scans[s + 1].first_tile <= item) ++s;
-        const BPParams kp = scans[s].kp;
-        const long long local = item - scans[s].first_tile;
-        const int tx = (kp.NX + kTXY2 - 1) / kTXY2, ty = (kp.NY + kTXY2 - 1) / kTXY2;
-        const int bx = (int)(local % tx);
-        const int by = (int)((local / tx) % ty);
-        const int bz = (int)(local / ((long long)tx * ty));
-        bp_tile<TZ, NB, float>(kp, scans[s].fproj, scans[s].pit, scans[s].views, scans[s].xyz,
-                               scans[s].image, bx, by, bz, sh, tile);
+        const BatchScanDev& sc = scans[s];
+        const int nxt = (sc.kp.NX + kTXY2 - 1) / kTXY2, nyt = (sc.kp.NY + kTXY2 - 1) / kTXY2;
+        const long long local = item - sc.first_tile;
+        const int bx = (int)(local % nxt);
+        const int by = (int)((local / nxt) % nyt);
+        const int bz = (int)(local / ((long long)nxt * nyt));
+        if constexpr (FORM == 3)
+            tile3<NB, float>(sc.kp, sc.fproj, sc.pit, sc.views, sc.xyz, sc.image, bx, by, bz, sh3,
+                             dynb);
+        else
+            bp_tile<TZ, NB, float>(sc.kp, sc.fproj, sc.pit, sc.views, sc.xyz, sc.image, bx, by,
+                                   bz, sh2, reinterpret_cast<float*>(dynb));
     }
 }
 
 long long bkproj_batch_tiles(const BPParams& kp, int variant) {
-    const int TZ = (variant == 1) ? 4 : 8;
+    const int TZ = variant_tz(variant);
     return (long long)((kp.NX + kTXY2 - 1) / kTXY2) * ((kp.NY + kTXY2 - 1) / kTXY2) *
            ((kp.NZ + TZ - 1) / TZ);
 }
 
-template <int TZ, int NB>
+template <int FORM, int TZ, int NB>
 static Status launch_batch(cudaStream_t s, const BatchScanDev* d_scans, int n,
                            long long total, unsigned long long* d_counter) {
-    const size_t smem = (size_t)2 * NB * kCap2 * sizeof(float);
-    CTR_CUDA(cudaFuncSetAttribute(k_bkproj2_batch<TZ, NB>,
+    const size_t smem = FORM == 3 ? tile3_smem_bytes<NB>() : (size_t)2 * NB * kCap2 * sizeof(float);
+    CTR_CUDA(cudaFuncSetAttribute(k_bkproj_batch<FORM, TZ, NB>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    int dev = 0, sms = 148;
+    int dev = 0, sms = 148, per_sm = 1;
     CTR_CUDA(cudaGetDevice(&dev));
     CTR_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    const long long grid = std::min<long long>(total, 3LL * sms);
+    CTR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bkproj_batch<FORM, TZ, NB>,
+                                                           256, smem));
+    const long long grid = std::min<long long>(total, (long long)std::max(1, per_sm) * sms);
     CTR_CUDA(cudaMemsetAsync(d_counter, 0, sizeof(unsigned long long), s));
     if (grid > 0)
-        k_bkproj2_batch<TZ, NB><<<(unsigned)grid, 256, smem, s>>>(d_scans, n, total, d_counter);
+        k_bkproj_batch<FORM, TZ, NB><<<(unsigned)grid, 256, smem, s>>>(d_scans, n, total, d_counter);
     CTR_CUDA(cudaGetLastError());
     return Status::Ok();
 }
@@ -344,9 +345,11 @@ static Status launch_batch(cudaStream_t s, const BatchScanDev* d_scans, int n,
 Status launch_bkproj_batch(int variant, cudaStream_t s, const BatchScanDev* d_scans, int n,
                            long long total, unsigned long long* d_counter) {
     switch (variant) {
-    case 1: return launch_batch<4, 8>(s, d_scans, n, total, d_counter);
-    case 2: return launch_batch<8, 4>(s, d_scans, n, total, d_counter);
-    default: return launch_batch<8, 8>(s, d_scans, n, total, d_counter);
+    case 1: return launch_batch<3, 8, 8>(s, d_scans, n, total, d_counter);
+    case 2: return launch_batch<2, 8, 8>(s, d_scans, n, total, d_counter);
+    case 3: return launch_batch<2, 4, 8>(s, d_scans, n, total, d_counter);
+    case 4: return launch_batch<2, 8, 4>(s, d_scans, n, total, d_counter);
+    default: return launch_batch<3, 8, 4>(s, d_scans, n, total, d_counter);
     }
 }
 
@@ -364,14 +367,30 @@ static Status launch_v2(cudaStream_t s, BPPlan& plan, const float* d_fproj,
     return Status::Ok();
 }
 
-// variants 0 (default) .. 2 of the second form; 100 + k selects the first form (bkproj.cu)
+template <int NB, typename OutT>
+static Status launch_v3(cudaStream_t s, BPPlan& plan, const float* d_fproj,
+                        const PiRecord* d_pitab, OutT* d_image) {
+    const BPParams& kp = plan.kp;
+    dim3 grid((kp.NX + kTXY2 - 1) / kTXY2, (kp.NY + kTXY2 - 1) / kTXY2, (kp.NZ + 7) / 8);
+    const size_t smem = tile3_smem_bytes<NB>();
+    CTR_CUDA(cudaFuncSetAttribute(k_bkproj3<NB, OutT>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_bkproj3<NB, OutT><<<grid, 256, smem, s>>>(kp, d_fproj, d_pitab, plan.views.as<float4>(),
+                                                plan.xyz.as<float>(), d_image);
+    CTR_CUDA(cudaGetLastError());
+    return Status::Ok();
+}
+
+// variants 0 .. 4 of the tiled forms; 100 + k selects the first form (bkproj.cu)
 template <typename OutT>
 Status launch_bkproj_v2(int variant, cudaStream_t s, BPPlan& plan, const float* d_fproj,
                         const PiRecord* d_pitab, OutT* d_image) {
     switch (variant) {
-    case 1: return launch_v2<4, 8, OutT>(s, plan, d_fproj, d_pitab, d_image);
-    case 2: return launch_v2<8, 4, OutT>(s, plan, d_fproj, d_pitab, d_image);
-    default: return launch_v2<8, 8, OutT>(s, plan, d_fproj, d_pitab, d_image);
+    case 1: return launch_v3<8, OutT>(s, plan, d_fproj, d_pitab, d_image);
+    case 2: return launch_v2<8, 8, OutT>(s, plan, d_fproj, d_pitab, d_image);
+    case 3: return launch_v2<4, 8, OutT>(s, plan, d_fproj, d_pitab, d_image);
+    case 4: return launch_v2<8, 4, OutT>(s, plan, d_fproj, d_pitab, d_image);
+    default: return launch_v3<4, OutT>(s, plan, d_fproj, d_pitab, d_image);
     }
 }
 

@@ -149,7 +149,7 @@ struct ctrecon_ctx {
     int opt_hilbert = CTRECON_HILBERT_FP32;
     int opt_pi = CTRECON_PI_BISECT;
     int opt_filter_chunk = 512;
-    int opt_bp_variant = 0;
+    int opt_bp_variant = 2;  // second form, 8 slices x 8 views
     int opt_verbose = 0;
     cudaStream_t host_stream = nullptr;  // stream for the synchronous host calls
     cudaStream_t up_stream = nullptr;    // host -> device copies of the host calls

@@ -94,7 +94,9 @@ typedef enum ctrecon_option {
     CTRECON_OPT_HILBERT = 1,          /* CTRECON_HILBERT_*; default FP32 */
     CTRECON_OPT_PI_SOLVER = 2,        /* CTRECON_PI_*; default BISECT */
     CTRECON_OPT_FILTER_CHUNK = 3,     /* views per filter work chunk; default 512 */
-    CTRECON_OPT_BP_VARIANT = 4,       /* backprojector variant (autotuner), default 0 */
+    CTRECON_OPT_BP_VARIANT = 4,       /* backprojector variant, default 2: 0, 1 = per-cell
+                                         records, blocks of 4 / 8 views; 2, 3, 4 = second
+                                         form (slices x views) 8x8, 4x8, 8x4; 100 = first form */
     CTRECON_OPT_VERBOSE = 5
 } ctrecon_option;
 
@@ -193,7 +195,7 @@ ctrecon_status ctrecon_batch_create(ctrecon_ctx* ctx, int n_scans,
                                     const ctrecon_filter_params* params,
                                     const ctrecon_bp_geom* geoms, ctrecon_batch** out);
 void ctrecon_batch_destroy(ctrecon_batch* batch);
-/* backprojector tile shape for the batch: 0 (8 slices x 8 views), 1 (4 x 8), 2 (8 x 4) */
+/* backprojector form of the batch: 0 .. 4 as CTRECON_OPT_BP_VARIANT (default: the context's) */
 ctrecon_status ctrecon_batch_set_variant(ctrecon_batch* batch, int variant);
 /* d_proj[i] (input), d_fproj[i] (work), d_image[i] (output, in place) for scan i */
 ctrecon_status ctrecon_batch_run_dev(ctrecon_batch* batch, void* stream,
