@@ -54,9 +54,11 @@ def parse():
     ap.add_argument("--config", default="c2")
     ap.add_argument("--hilbert", default="fp32", choices=["fp32", "bf16x3", "tf32"])
     ap.add_argument("--pi", default="bisect", choices=["bisect", "newton", "learned"])
-    ap.add_argument("--bp-variant", type=int, default=2,
-                    help="backprojector form: 0, 1 per-cell records (4 / 8 views per block), "
-                         "2-4 second form tile shapes, 100 first form")
+    ap.add_argument("--bp-variant", type=int, default=-1,
+                    help="backprojector form: -1 autotuned on the workload before timing "
+                         "(default), 0, 1 per-cell records (4 / 8 views per block), 2-4 second "
+                         "form tile shapes, 5-9 per-cell records staged by producer warps, "
+                         "100 first form")
     ap.add_argument("--batched", action="store_true",
                     help="16 uneven scans (c4): one-at-a-time vs one batched graph replay")
     ap.add_argument("--no-e2e", action="store_true")
@@ -337,7 +339,6 @@ def run_batched(args):
     stream = torch.cuda.Stream()
     with torch.cuda.stream(stream):
         ctx = ct.Context(0, hilbert=hil, pi_solver=_lib.PI_BISECT)
-        ctx.set_option(_lib.OPT_BP_VARIANT, args.bp_variant)
         if pis == _lib.PI_LEARNED:
             import ctypes
             loss = ctypes.c_float()
@@ -351,10 +352,18 @@ def run_batched(args):
             fprojs.append(torch.empty_like(d))
             imgs.append(torch.zeros(s.vol_shape, dtype=torch.float32, device="cuda"))
         b = ct.Batch(ctx, scans)
-        b.set_variant(args.bp_variant if args.bp_variant < 100 else 0)
         updates = b.updates()
         ctx.set_option(_lib.OPT_PI_SOLVER, pis)
         total = sum(updates)
+        tune = None
+        if args.bp_variant == -1:
+            # the autotuner picks the batch's backprojector form (tile shape, view-block
+            # depth, staging) on these scans, untimed
+            tune = b.tune(projs, fprojs, imgs, stream=stream)
+            ctx.set_option(_lib.OPT_BP_VARIANT, tune["best_variant"])  # one-at-a-time too
+        else:
+            b.set_variant(args.bp_variant if args.bp_variant < 100 else 2)
+            ctx.set_option(_lib.OPT_BP_VARIANT, args.bp_variant)
 
         def one_at_a_time():
             for s, d, f, im in zip(scans, projs, fprojs, imgs):
@@ -392,7 +401,7 @@ def run_batched(args):
                        "l2": "inputs larger than L2 (40 GB of projections and volumes)"},
             "updates_per_step": total,
             "one_at_a_time": {"ms_per_step": ms_seq, "gups": total / (ms_seq / 1e3) / 1e9},
-            "batched_speedup": ms_seq / ms_bat, "clocks": clocks}
+            "batched_speedup": ms_seq / ms_bat, "bp_tune": tune, "clocks": clocks}
     print(json.dumps(line))
 
 
@@ -444,6 +453,13 @@ def main():
     updates = int(d_cnt.item())
     ctx.set_option(_lib.OPT_PI_SOLVER, pis)
     stream = torch.cuda.current_stream()
+    tune = None
+    if args.bp_variant == -1:
+        # the autotuner picks the backprojector form on this workload (untimed setup)
+        ctx.filter_dev(fpar, d_proj, d_fproj)
+        tune = ctx.tune_bkproj(geom, d_fproj, d_img, d_pitab=d_tab)
+        ctx.set_option(_lib.OPT_BP_VARIANT, _lib.BP_AUTO)
+    bp_form = tune["best_variant"] if tune else args.bp_variant
 
     ev = {k: [] for k in ("f0", "f1", "p1", "b1")}
 
@@ -492,6 +508,8 @@ def main():
     launches_per_step = 2 * nchunks + 1 + 1
     if hil != _lib.HILBERT_FP32:
         launches_per_step += nchunks
+    if pis == _lib.PI_LEARNED:
+        launches_per_step += 1  # the network's inference kernel before the Newton solve
 
     # ---- e2e through the MEX-equivalent host calls (FP64 pinned host buffers) -----------------
     e2e = None
@@ -521,10 +539,12 @@ def main():
     # ---- roofline of the dominant kernel (backprojection) -----------------------------------------
     peak, peak_kind = load_peaks()
     achieved = BYTES_PER_UPDATE * updates / (bp_ms / 1e3) / 1e9
+    bp_kernel = ("k_bkproj" if bp_form >= 100 else "k_bkproj3" if bp_form in (0, 1)
+                 else "k_bkproj2" if bp_form in (2, 3, 4) else "k_bkproj4")
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_source": peak_kind,
-                "kernel": "k_bkproj", "model": "16 B per voxel-view update",
-                "traffic": load_traffic("k_bkproj", workload_name(s))}
+                "kernel": bp_kernel, "model": "16 B per voxel-view update",
+                "traffic": load_traffic(bp_kernel, workload_name(s))}
 
     # ---- CPU baseline (rank 0, N = 1): the FP64 oracle restatement on a bounded sample -----------
     cpu = None
@@ -559,13 +579,13 @@ def main():
                            "voxel_mm": list(s.voxel_size), "detector": [s.ZL, s.YL],
                            "views": s.P, "views_per_turn": s.views_per_turn,
                            "hilbert": args.hilbert, "pi_solver": args.pi,
-                           "bp_variant": args.bp_variant,
+                           "bp_variant": bp_form,
                            "parallelism": f"replicas{ws}",
                            "l2": "inputs larger than L2 (projections 1.75 GB)"},
                 "updates_per_step": updates, "s_per_vol": ms_step / 1e3,
                 "phase_ms": {"filter": filt_ms, "pi": pi_ms, "bkproj": bp_ms},
                 "bkproj_gups": updates / (bp_ms / 1e3) / 1e9,
-                "pinet": pinet_info,
+                "pinet": pinet_info, "bp_tune": tune,
                 "gpu_launches": launches_per_step * args.steps,
                 "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks}
         print(json.dumps(line))

@@ -38,6 +38,15 @@ class FilterParams(ctypes.Structure):
                 ("proj_number", ctypes.c_int)]
 
 
+BP_AUTO = -1
+TUNE_MAX = 16
+
+
+class TuneResult(ctypes.Structure):
+    _fields_ = [("best_variant", ctypes.c_int), ("best_ms", ctypes.c_float), ("n", ctypes.c_int),
+                ("variants", ctypes.c_int * TUNE_MAX), ("ms", ctypes.c_float * TUNE_MAX)]
+
+
 class BPGeom(ctypes.Structure):
     _fields_ = [("locus", ctypes.c_double * 7), ("detector", ctypes.c_double * 6),
                 ("object", ctypes.c_double * 7), ("n_detector", ctypes.c_int),
@@ -76,6 +85,12 @@ SIGNATURES = [
     ("ctrecon_batch_run_dev", _st, [_vp, _vp, ctypes.POINTER(_vp), ctypes.POINTER(_vp),
                                     ctypes.POINTER(_vp), ctypes.c_int]),
     ("ctrecon_batch_updates", _st, [_vp, ctypes.POINTER(ctypes.c_ulonglong)]),
+    ("ctrecon_tune_bkproj", _st, [_vp, _vp, ctypes.POINTER(BPGeom), _vp, _vp, _vp,
+                                  ctypes.POINTER(TuneResult)]),
+    ("ctrecon_batch_tune", _st, [_vp, _vp, ctypes.POINTER(_vp), ctypes.POINTER(_vp),
+                                 ctypes.POINTER(_vp), ctypes.POINTER(TuneResult)]),
+    ("ctrecon_tune_save", _st, [_vp, ctypes.c_char_p]),
+    ("ctrecon_tune_load", _st, [_vp, ctypes.c_char_p]),
     ("ctrecon_pinet_num_params", ctypes.c_int, []),
     ("ctrecon_pinet_train", _st, [_vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                   ctypes.c_double, ctypes.c_uint64,

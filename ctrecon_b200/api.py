@@ -15,6 +15,7 @@ and run on the tensors' device, ordered on the current torch stream.
 from __future__ import annotations
 
 import ctypes
+import os
 from typing import Mapping, Optional, Sequence
 
 import numpy as np
@@ -222,6 +223,25 @@ class Context:
                                            _tptr(d_pitab, "", "d_pitab"),
                                            _tptr(d_image, "float32", "d_image")), self._h)
 
+    # -- autotuner -----------------------------------------------------------------------------
+    def tune_bkproj(self, geom, d_fproj, d_image, d_pitab=None, stream=None) -> dict:
+        """Times the backprojector forms on this data, records the fastest for the geometry
+        (used under OPT_BP_VARIANT = BP_AUTO) and returns {variant: ms} plus the best."""
+        g = bp_geom(geom)
+        r = _lib.TuneResult()
+        check(lib().ctrecon_tune_bkproj(self._h, _stream_handle(stream), ctypes.byref(g),
+                                        _tptr(d_fproj, "float32", "d_fproj"),
+                                        _tptr(d_pitab, "", "d_pitab"),
+                                        _tptr(d_image, "float32", "d_image"), ctypes.byref(r)),
+              self._h)
+        return _tune_dict(r)
+
+    def tune_save(self, path: str):
+        check(lib().ctrecon_tune_save(self._h, os.fsencode(path)), self._h)
+
+    def tune_load(self, path: str):
+        check(lib().ctrecon_tune_load(self._h, os.fsencode(path)), self._h)
+
     def phantom_dev(self, geom, ell: np.ndarray, d_proj, photons: float = 0.0, seed: int = 0,
                     stream=None):
         g = bp_geom(geom)
@@ -271,6 +291,23 @@ class Batch:
         out = (ctypes.c_ulonglong * self.n)()
         check(lib().ctrecon_batch_updates(self._h, out), self.ctx.handle)
         return [int(v) for v in out]
+
+    def tune(self, d_projs, d_fprojs, d_images, stream=None) -> dict:
+        """One run of the batch, then the persistent backprojection timed for every candidate
+        form; the fastest becomes the batch's form."""
+        arr = lambda ts, name, dt: (ctypes.c_void_p * self.n)(*[_tptr(t, dt, name) for t in ts])
+        r = _lib.TuneResult()
+        check(lib().ctrecon_batch_tune(self._h, _stream_handle(stream),
+                                       arr(d_projs, "d_proj", "float32"),
+                                       arr(d_fprojs, "d_fproj", "float32"),
+                                       arr(d_images, "d_image", "float32"), ctypes.byref(r)),
+              self.ctx.handle)
+        return _tune_dict(r)
+
+
+def _tune_dict(r) -> dict:
+    return {"best_variant": r.best_variant, "best_ms": r.best_ms,
+            "ms": {int(r.variants[i]): float(r.ms[i]) for i in range(r.n)}}
 
 
 _default: Optional[Context] = None

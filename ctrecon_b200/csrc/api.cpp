@@ -304,7 +304,12 @@ ctrecon_status ctrecon_set_option(ctrecon_ctx* ctx, ctrecon_option opt, int valu
             return finish(ctx, make_status(CTRECON_ERR_INVALID_ARGUMENT, "chunk must be >= 1"));
         ctx->opt_filter_chunk = value;
         break;
-    case CTRECON_OPT_BP_VARIANT: ctx->opt_bp_variant = value; break;
+    case CTRECON_OPT_BP_VARIANT:
+        if (!(value == CTRECON_BP_AUTO || (value >= 0 && value <= 9) || value == 100))
+            return finish(ctx, make_status(CTRECON_ERR_INVALID_ARGUMENT,
+                                           "backprojector variant must be -1, 0..9 or 100"));
+        ctx->opt_bp_variant = value;
+        break;
     case CTRECON_OPT_VERBOSE: ctx->opt_verbose = value; break;
     default: return finish(ctx, make_status(CTRECON_ERR_INVALID_ARGUMENT, "unknown option"));
     }
@@ -439,10 +444,10 @@ ctrecon_status ctrecon_bkproj_dev_f32(ctrecon_ctx* ctx, void* stream, const ctre
     BPPlan* plan = nullptr;
     if (s.ok()) s = get_bp_plan(ctx, *g, &plan);
     const PiRecord* pit = (const PiRecord*)d_pitab;
+    if (s.ok()) s = reset_device_flag(ctx, st);
     if (s.ok() && !pit) {
         const size_t nvox = (size_t)plan->kp.NX * plan->kp.NY * plan->kp.NZ;
         s = ctx->ws_pitab.ensure(nvox * sizeof(PiRecord), "PI table");
-        if (s.ok()) s = reset_device_flag(ctx, st);
         if (s.ok()) s = launch_pi(ctx, st, *plan, ctx->ws_pitab.as<PiRecord>(), nullptr);
         pit = ctx->ws_pitab.as<PiRecord>();
     }

@@ -18,7 +18,8 @@
 
 namespace ctr {
 Status launch_bkproj_batch(int variant, cudaStream_t s, const BatchScanDev* d_scans, int n,
-                           long long total, unsigned long long* d_counter);
+                           long long total, unsigned long long* d_counter, int cells_cap,
+                           int raw_cap, int* err);
 long long bkproj_batch_tiles(const BPParams& kp, int variant);
 Status launch_pi_stats(ctrecon_ctx* ctx, cudaStream_t s, BPPlan& plan, PiRecord* d_pitab,
                        unsigned long long* d_updates, unsigned long long* d_iters);
@@ -58,6 +59,19 @@ static ctrecon_status bfinish(ctrecon_ctx* ctx, const Status& s) {
     return s.code;
 }
 
+// the persistent backprojection launch over all scans (the scan table must be uploaded)
+static Status batch_backproject(ctrecon_batch* b, cudaStream_t s) {
+    int cells = 0, raw = 0;  // fourth-form capacities: the largest over the scans
+    for (int i = 0; i < b->n; ++i) {
+        bp4_caps(*b->bplans[i]);
+        cells = std::max(cells, b->bplans[i]->caps_cells);
+        raw = std::max(raw, b->bplans[i]->caps_raw);
+    }
+    return launch_bkproj_batch(b->variant, s, b->scans_dev.as<BatchScanDev>(), b->n,
+                               b->total_tiles, b->counter.as<unsigned long long>(), cells, raw,
+                               b->ctx->ws_flag.as<int>());
+}
+
 static Status enqueue(ctrecon_batch* b, cudaStream_t s, const float* const* d_proj,
                       float* const* d_fproj, float* const* d_image) {
     ctrecon_ctx* ctx = b->ctx;
@@ -71,8 +85,7 @@ static Status enqueue(ctrecon_batch* b, cudaStream_t s, const float* const* d_pr
         const int i = b->order[k];
         CTR_TRY(launch_pi(ctx, s, *b->bplans[i], b->pitab.as<PiRecord>() + b->pit_off[i], nullptr));
     }
-    return launch_bkproj_batch(b->variant, s, b->scans_dev.as<BatchScanDev>(), b->n,
-                               b->total_tiles, b->counter.as<unsigned long long>());
+    return batch_backproject(b, s);
 }
 
 static Status upload_scans(ctrecon_batch* b, cudaStream_t s, float* const* d_fproj,
@@ -111,7 +124,8 @@ ctrecon_status ctrecon_batch_create(ctrecon_ctx* ctx, int n_scans,
         auto b = std::make_unique<ctrecon_batch>();
         b->ctx = ctx;
         b->n = n_scans;
-        b->variant = ctx->opt_bp_variant >= 100 ? 0 : ctx->opt_bp_variant;
+        b->variant = (ctx->opt_bp_variant >= 0 && ctx->opt_bp_variant <= 9) ? ctx->opt_bp_variant
+                                                                             : kDefaultBPVariant;
         b->fp.assign(fp, fp + n_scans);
         size_t nvox = 0;
         std::vector<double> work(n_scans);
@@ -153,7 +167,7 @@ void ctrecon_batch_destroy(ctrecon_batch* b) {
 }
 
 ctrecon_status ctrecon_batch_set_variant(ctrecon_batch* b, int variant) {
-    if (!b || variant < 0 || variant > 4) return CTRECON_ERR_INVALID_ARGUMENT;
+    if (!b || variant < 0 || variant > 9) return CTRECON_ERR_INVALID_ARGUMENT;
     if (variant != b->variant) {
         b->variant = variant;
         b->key.clear();  // tile counts change: rebuild the scan table and the graph
@@ -213,6 +227,47 @@ ctrecon_status ctrecon_batch_run_dev(ctrecon_batch* b, void* stream, const float
             if (e != cudaSuccess) st = cuda_status(e, "cudaGraphLaunch");
         }
         if (st.ok()) b->runs_with_key++;
+        return bfinish(ctx, st);
+    } catch (const std::exception& e) {
+        return bfinish(ctx, make_status(CTRECON_ERR_INTERNAL, e.what()));
+    }
+}
+
+ctrecon_status ctrecon_batch_tune(ctrecon_batch* b, void* stream, const float* const* d_proj,
+                                  float* const* d_fproj, float* const* d_image,
+                                  ctrecon_tune_result* out) {
+    if (!b || !d_proj || !d_fproj || !d_image || !out) return CTRECON_ERR_INVALID_ARGUMENT;
+    ctrecon_ctx* ctx = b->ctx;
+    try {
+        cudaSetDevice(ctx->device);
+        cudaStream_t s = (cudaStream_t)stream;
+        // one eager run: filters, PI solves and a backprojection with the current form
+        ctrecon_status rc = ctrecon_batch_run_dev(b, stream, d_proj, d_fproj, d_image, 0);
+        if (rc != CTRECON_OK) return rc;
+        const int saved = b->variant;
+        Status st = tune_candidates(
+            out, s,
+            [&](int v) {
+                b->variant = v;
+                return upload_scans(b, s, d_fproj, d_image);  // tile counts depend on the form
+            },
+            [&](int) { return batch_backproject(b, s); });
+        b->variant = st.ok() ? out->best_variant : saved;
+        if (st.ok()) {  // leave the winner's backprojection in the images
+            st = upload_scans(b, s, d_fproj, d_image);
+            if (st.ok()) st = batch_backproject(b, s);
+            if (st.ok()) {
+                cudaError_t e = cudaStreamSynchronize(s);
+                if (e != cudaSuccess) st = cuda_status(e, "cudaStreamSynchronize");
+            }
+        }
+        b->key.clear();  // the next run re-uploads the scan table and re-captures its graph
+        if (st.ok()) {
+            int flag = 0;
+            cudaError_t e = cudaMemcpy(&flag, ctx->ws_flag.ptr, sizeof(int), cudaMemcpyDeviceToHost);
+            if (e != cudaSuccess) st = cuda_status(e, "device error word");
+            else if (flag) st = make_status(CTRECON_ERR_TIMEOUT, "a device-side wait gave up");
+        }
         return bfinish(ctx, st);
     } catch (const std::exception& e) {
         return bfinish(ctx, make_status(CTRECON_ERR_INTERNAL, e.what()));

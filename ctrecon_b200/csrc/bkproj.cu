@@ -229,20 +229,27 @@ static Status launch_bk(cudaStream_t s, BPPlan& plan, const float* d_fproj,
 
 template <typename OutT>
 Status launch_bkproj_v2(int variant, cudaStream_t s, BPPlan& plan, const float* d_fproj,
-                        const PiRecord* d_pitab, OutT* d_image);
+                        const PiRecord* d_pitab, OutT* d_image, int* err);
 
-// CTRECON_OPT_BP_VARIANT: 0..2 select tile shapes of the second form (bkproj2.cu), 100 the
-// first form above
+// CTRECON_OPT_BP_VARIANT: 0..9 select the tiled forms (bkproj2.cu), 100 the first form above,
+// CTRECON_BP_AUTO the tuning table's choice. The fourth form (5..9) reports a bounded wait
+// that gave up in the context's device word.
 Status launch_bkproj_f32(ctrecon_ctx* ctx, cudaStream_t s, BPPlan& plan, const float* d_fproj,
                          const PiRecord* d_pitab, float* d_image) {
-    if (ctx->opt_bp_variant >= 100) return launch_bk<float>(s, plan, d_fproj, d_pitab, d_image);
-    return launch_bkproj_v2<float>(ctx->opt_bp_variant, s, plan, d_fproj, d_pitab, d_image);
+    const int variant = bp_variant_for(ctx, plan.g);
+    if (variant >= 100) return launch_bk<float>(s, plan, d_fproj, d_pitab, d_image);
+    if (!ctx->ws_flag.ptr) return make_status(CTRECON_ERR_INTERNAL, "device error word not set up");
+    return launch_bkproj_v2<float>(variant, s, plan, d_fproj, d_pitab, d_image,
+                                   ctx->ws_flag.as<int>());
 }
 
 Status launch_bkproj_f64out(ctrecon_ctx* ctx, cudaStream_t s, BPPlan& plan,
                             const float* d_fproj, const PiRecord* d_pitab, double* d_image) {
-    if (ctx->opt_bp_variant >= 100) return launch_bk<double>(s, plan, d_fproj, d_pitab, d_image);
-    return launch_bkproj_v2<double>(ctx->opt_bp_variant, s, plan, d_fproj, d_pitab, d_image);
+    const int variant = bp_variant_for(ctx, plan.g);
+    if (variant >= 100) return launch_bk<double>(s, plan, d_fproj, d_pitab, d_image);
+    if (!ctx->ws_flag.ptr) return make_status(CTRECON_ERR_INTERNAL, "device error word not set up");
+    return launch_bkproj_v2<double>(variant, s, plan, d_fproj, d_pitab, d_image,
+                                    ctx->ws_flag.as<int>());
 }
 
 }  // namespace ctr

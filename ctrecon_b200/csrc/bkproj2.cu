@@ -14,9 +14,11 @@
 // bring an update down to about a dozen instructions.
 //
 // Also the persistent batched kernel (either form) behind the batch API.
-#include "bp_tile3.cuh"
+#include "bp_tile4.cuh"
 
+#include <algorithm>
 #include <climits>
+#include <cmath>
 
 namespace ctr {
 
@@ -29,6 +31,11 @@ constexpr int kCap2 = 1024;  // shared floats per staged view
 struct Foot2 { int u0, v0, W, H; };
 
 }  // namespace
+
+Caps4 caps_within(int cells, int raw, int NB, int S, size_t budget);
+// dynamic shared memory per fourth-form CTA: three CTAs per SM with up to two producer warps,
+// two with more
+constexpr size_t smem4_budget(int PW) { return PW <= 2 ? 72 * 1024 : 104 * 1024; }
 
 template <int NB>
 struct BPShared {
@@ -279,9 +286,56 @@ k_bkproj3(BPParams kp, const float* __restrict__ fproj, const PiRecord* __restri
                     dyn3);
 }
 
+template <int NB, int S, int PW, typename OutT>
+__global__ void __launch_bounds__(32 * (8 + PW), PW <= 2 ? 3 : 2)
+k_bkproj4(BPParams kp, const float* __restrict__ fproj, const PiRecord* __restrict__ pit,
+          const float4* __restrict__ views, const float* __restrict__ xyz,
+          OutT* __restrict__ image, Caps4 caps, int* err) {
+    extern __shared__ __align__(16) unsigned char dyn4[];
+    __shared__ Shared4<NB, S, PW> sh;
+    tile4_init(sh);
+    tile4<NB, S, PW, OutT>(kp, fproj, pit, views, xyz, image, blockIdx.x, blockIdx.y, blockIdx.z,
+                           sh, dyn4, caps, err, 0u);
+}
+
 // Variants: 0, 1 = third form with blocks of 4 / 8 views; 2, 3, 4 = second form with
-// (TZ, NB) = (8, 8), (4, 8), (8, 4).
+// (TZ, NB) = (8, 8), (4, 8), (8, 4); 5 .. 9 = fourth form with (NB, S, PW) = (4, 2, 1),
+// (2, 4, 1), (4, 2, 2), (4, 2, 3), (4, 3, 4).
 __host__ __device__ constexpr int variant_tz(int variant) { return variant == 3 ? 4 : 8; }
+
+// The persistent batched kernel of the fourth form (its own block size).
+template <int NB, int S, int PW>
+__global__ void __launch_bounds__(32 * (8 + PW), PW <= 2 ? 3 : 2)
+k_bkproj4_batch(const BatchScanDev* __restrict__ scans, int n_scans, long long total_tiles,
+                unsigned long long* __restrict__ counter, Caps4 caps, int* err) {
+    extern __shared__ __align__(16) unsigned char dynb4[];
+    __shared__ Shared4<NB, S, PW> sh;
+    __shared__ BatchScanDev sc;  // this tile's scan record, read from shared memory
+    tile4_init(sh);
+    uint32_t iter = 0;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const long long item = (long long)atomicAdd(counter, 1ull);
+            sh.s_item = item;
+            if (item < total_tiles) {
+                int s = 0;
+                while (s + 1 < n_scans && scans[s + 1].first_tile <= item) ++s;
+                sc = scans[s];
+            }
+        }
+        __syncthreads();
+        const long long item = sh.s_item;
+        if (item >= total_tiles) break;
+        const int nxt = (sc.kp.NX + kTXY2 - 1) / kTXY2, nyt = (sc.kp.NY + kTXY2 - 1) / kTXY2;
+        const long long local = item - sc.first_tile;
+        const int bx = (int)(local % nxt);
+        const int by = (int)((local / nxt) % nyt);
+        const int bz = (int)(local / ((long long)nxt * nyt));
+        iter = tile4<NB, S, PW, float>(sc.kp, sc.fproj, sc.pit, sc.views, sc.xyz, sc.image, bx,
+                                       by, bz, sh, dynb4, caps, err, iter);
+        if (sh.s_abort) break;  // uniform: read after the tile's closing barrier
+    }
+}
 
 // Many scans in one persistent launch: the CTAs pull tiles of all scans from one atomic
 // counter (largest-first order is the caller's choice of scan order), so uneven scans share
@@ -294,15 +348,21 @@ k_bkproj_batch(const BatchScanDev* __restrict__ scans, int n_scans, long long to
     __shared__ BPShared<NB> sh2;
     __shared__ Shared3<NB> sh3;
     __shared__ long long s_item;
+    __shared__ BatchScanDev sc;  // this tile's scan record, read from shared memory
     for (;;) {
         __syncthreads();
-        if (threadIdx.x == 0) s_item = (long long)atomicAdd(counter, 1ull);
+        if (threadIdx.x == 0) {
+            const long long item = (long long)atomicAdd(counter, 1ull);
+            s_item = item;
+            if (item < total_tiles) {
+                int s = 0;
+                while (s + 1 < n_scans && scans[s + 1].first_tile <= item) ++s;
+                sc = scans[s];
+            }
+        }
         __syncthreads();
         const long long item = s_item;
         if (item >= total_tiles) break;
-        int s = 0;
-        while (s + 1 < n_scans && scans[s + 1].first_tile <= item) ++s;
-        const BatchScanDev& sc = scans[s];
         const int nxt = (sc.kp.NX + kTXY2 - 1) / kTXY2, nyt = (sc.kp.NY + kTXY2 - 1) / kTXY2;
         const long long local = item - sc.first_tile;
         const int bx = (int)(local % nxt);
@@ -342,9 +402,41 @@ static Status launch_batch(cudaStream_t s, const BatchScanDev* d_scans, int n,
     return Status::Ok();
 }
 
+template <int NB, int S, int PW>
+static Status launch_batch4(cudaStream_t s, const BatchScanDev* d_scans, int n, long long total,
+                            unsigned long long* d_counter, Caps4 caps, int* err) {
+    const size_t smem = tile4_smem_bytes<NB, S, PW>(caps);
+    const int threads = 32 * (8 + PW);
+    CTR_CUDA(cudaFuncSetAttribute(k_bkproj4_batch<NB, S, PW>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int dev = 0, sms = 148, per_sm = 1;
+    CTR_CUDA(cudaGetDevice(&dev));
+    CTR_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    CTR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bkproj4_batch<NB, S, PW>,
+                                                           threads, smem));
+    const long long grid = std::min<long long>(total, (long long)std::max(1, per_sm) * sms);
+    CTR_CUDA(cudaMemsetAsync(d_counter, 0, sizeof(unsigned long long), s));
+    if (grid > 0)
+        k_bkproj4_batch<NB, S, PW><<<(unsigned)grid, threads, smem, s>>>(d_scans, n, total,
+                                                                        d_counter, caps, err);
+    CTR_CUDA(cudaGetLastError());
+    return Status::Ok();
+}
+
 Status launch_bkproj_batch(int variant, cudaStream_t s, const BatchScanDev* d_scans, int n,
-                           long long total, unsigned long long* d_counter) {
+                           long long total, unsigned long long* d_counter, int cells_cap,
+                           int raw_cap, int* err) {
     switch (variant) {
+    case 5: return launch_batch4<4, 2, 1>(s, d_scans, n, total, d_counter,
+                                              caps_within(cells_cap, raw_cap, 4, 2, smem4_budget(1)), err);
+    case 6: return launch_batch4<2, 4, 1>(s, d_scans, n, total, d_counter,
+                                              caps_within(cells_cap, raw_cap, 2, 4, smem4_budget(1)), err);
+    case 7: return launch_batch4<4, 2, 2>(s, d_scans, n, total, d_counter,
+                                              caps_within(cells_cap, raw_cap, 4, 2, smem4_budget(2)), err);
+    case 8: return launch_batch4<4, 2, 3>(s, d_scans, n, total, d_counter,
+                                              caps_within(cells_cap, raw_cap, 4, 2, smem4_budget(3)), err);
+    case 9: return launch_batch4<4, 3, 4>(s, d_scans, n, total, d_counter,
+                                              caps_within(cells_cap, raw_cap, 4, 3, smem4_budget(4)), err);
     case 1: return launch_batch<3, 8, 8>(s, d_scans, n, total, d_counter);
     case 2: return launch_batch<2, 8, 8>(s, d_scans, n, total, d_counter);
     case 3: return launch_batch<2, 4, 8>(s, d_scans, n, total, d_counter);
@@ -381,11 +473,105 @@ static Status launch_v3(cudaStream_t s, BPPlan& plan, const float* d_fproj,
     return Status::Ok();
 }
 
-// variants 0 .. 4 of the tiled forms; 100 + k selects the first form (bkproj.cu)
+template <int NB, int S, int PW, typename OutT>
+static Status launch_v4(cudaStream_t s, BPPlan& plan, const float* d_fproj,
+                        const PiRecord* d_pitab, OutT* d_image, int* err) {
+    const BPParams& kp = plan.kp;
+    bp4_caps(plan);
+    const Caps4 caps = caps_within(plan.caps_cells, plan.caps_raw, NB, S, smem4_budget(PW));
+    dim3 grid((kp.NX + kTXY2 - 1) / kTXY2, (kp.NY + kTXY2 - 1) / kTXY2, (kp.NZ + 7) / 8);
+    const size_t smem = tile4_smem_bytes<NB, S, PW>(caps);
+    CTR_CUDA(cudaFuncSetAttribute(k_bkproj4<NB, S, PW, OutT>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_bkproj4<NB, S, PW, OutT><<<grid, 32 * (8 + PW), smem, s>>>(
+        kp, d_fproj, d_pitab, plan.views.as<float4>(), plan.xyz.as<float>(), d_image, caps, err);
+    CTR_CUDA(cudaGetLastError());
+    return Status::Ok();
+}
+
+// Capacities of the fourth form's shared buffers for a geometry: the largest footprint (cell
+// records and raw floats) over a sample of tiles and views, computed as the kernel does, with
+// a margin. A view that still does not fit is read directly; the capacities only trade
+// shared memory (occupancy) for the share of views that take the cell path.
+void bp4_caps(BPPlan& plan) {
+    if (plan.caps_cells > 0) return;
+    const BPParams& kp = plan.kp;
+    const BPGeom& g = plan.g;
+    const int ntx = (kp.NX + 15) / 16, nty = (kp.NY + 15) / 16, ntz = (kp.NZ + 7) / 8;
+    const int sx = std::max(1, ntx / 12), sy = std::max(1, nty / 12), sz = std::max(1, ntz / 8);
+    const int sp = std::max(1, kp.P / 48);
+    auto xc = [&](int i) { return (i - g.XC) * g.dx; };
+    auto yc = [&](int i) { return (i - g.YC) * g.dy; };
+    auto zc = [&](int i) { return (i - g.ZC) * g.dz; };
+    const double R = g.ScanR, DdU = g.StdDis / g.DeltaU, DdV = g.StdDis / g.DeltaV;
+    const double PI = kRefPi;
+    int max_cells = 0, max_raw = 0;
+    for (int tx = 0; tx < ntx; tx += sx)
+        for (int ty = 0; ty < nty; ty += sy)
+            for (int tz = 0; tz < ntz; tz += sz) {
+                const double bx0 = xc(tx * 16), bx1 = xc(std::min(tx * 16 + 15, kp.NX - 1));
+                const double by0 = yc(ty * 16), by1 = yc(std::min(ty * 16 + 15, kp.NY - 1));
+                const double bz0 = zc(tz * 8), bz1 = zc(std::min(tz * 8 + 7, kp.NZ - 1));
+                if (std::min(bx0 * bx0, bx1 * bx1) + std::min(by0 * by0, by1 * by1) >
+                    g.ObjR * g.ObjR * 1.05)
+                    continue;  // tile outside the reconstruction cylinder
+                for (int p = 0; p < kp.P; p += sp) {
+                    const double th = (p + g.ProjBegin - g.ProjCtr) * g.DeltaL;
+                    const double c = std::cos(th), sn = std::sin(th), szs = g.HelicP * th / (2 * PI);
+                    double umin = 1e30, umax = -1e30, vmin = 1e30, vmax = -1e30;
+                    bool ok = true;
+                    for (int k = 0; k < 4; ++k) {
+                        const double cx = (k & 1) ? bx1 : bx0, cy = (k & 2) ? by1 : by0;
+                        const double fen = R - (cx * c + cy * sn);
+                        ok = ok && fen > 1e-3 * R;
+                        const double u = (cy * c - cx * sn) * DdU / fen + g.HalfY;
+                        const double va = (bz0 - szs) * DdV / fen + g.HalfZ;
+                        const double vb = (bz1 - szs) * DdV / fen + g.HalfZ;
+                        umin = std::min(umin, u); umax = std::max(umax, u);
+                        vmin = std::min(vmin, std::min(va, vb));
+                        vmax = std::max(vmax, std::max(va, vb));
+                    }
+                    if (!ok) continue;
+                    const int u0 = (int)std::floor(umin) - 1, u1 = (int)std::floor(umax) + 2;
+                    const int v0 = (int)std::floor(vmin) - 1, v1 = (int)std::floor(vmax) + 2;
+                    const int W = u1 - u0 + 1, H = v1 - v0 + 1;
+                    if (u0 < 0 || u1 > g.YL - 1 || v0 < 0 || v1 > g.ZL - 1 || W > 64) continue;
+                    max_cells = std::max(max_cells, (W - 1) * (H - 1));
+                    max_raw = std::max(max_raw, W * H);
+                }
+            }
+    auto cap = [](int v, int lo, int hi) {
+        v = (int)(v * 1.15) + 8;
+        v = (v + 3) / 4 * 4;
+        return std::max(lo, std::min(hi, v));
+    };
+    plan.caps_cells = cap(max_cells, 64, 1024);
+    plan.caps_raw = cap(max_raw, 96, 1536);
+}
+
+// Capacities that keep a fourth-form CTA within `budget` bytes of dynamic shared memory
+// (occupancy): shrunk in proportion when the geometry's footprints would need more; larger
+// footprints then take the direct path.
+Caps4 caps_within(int cells, int raw, int NB, int S, size_t budget) {
+    auto bytes = [&](int c, int r) { return (size_t)S * NB * c * 16 + (size_t)2 * NB * r * 4; };
+    if (bytes(cells, raw) > budget) {
+        const double f = (double)budget / (double)bytes(cells, raw);
+        cells = std::max(64, (int)(cells * f) / 4 * 4);
+        raw = std::max(96, (int)(raw * f) / 4 * 4);
+    }
+    return Caps4{cells, raw};
+}
+
+// variants 0 .. 9 of the tiled forms; 100 + k selects the first form (bkproj.cu)
 template <typename OutT>
 Status launch_bkproj_v2(int variant, cudaStream_t s, BPPlan& plan, const float* d_fproj,
-                        const PiRecord* d_pitab, OutT* d_image) {
+                        const PiRecord* d_pitab, OutT* d_image, int* err) {
     switch (variant) {
+    case 5: return launch_v4<4, 2, 1, OutT>(s, plan, d_fproj, d_pitab, d_image, err);
+    case 6: return launch_v4<2, 4, 1, OutT>(s, plan, d_fproj, d_pitab, d_image, err);
+    case 7: return launch_v4<4, 2, 2, OutT>(s, plan, d_fproj, d_pitab, d_image, err);
+    case 8: return launch_v4<4, 2, 3, OutT>(s, plan, d_fproj, d_pitab, d_image, err);
+    case 9: return launch_v4<4, 3, 4, OutT>(s, plan, d_fproj, d_pitab, d_image, err);
     case 1: return launch_v3<8, OutT>(s, plan, d_fproj, d_pitab, d_image);
     case 2: return launch_v2<8, 8, OutT>(s, plan, d_fproj, d_pitab, d_image);
     case 3: return launch_v2<4, 8, OutT>(s, plan, d_fproj, d_pitab, d_image);
@@ -394,7 +580,7 @@ Status launch_bkproj_v2(int variant, cudaStream_t s, BPPlan& plan, const float* 
     }
 }
 
-template Status launch_bkproj_v2<float>(int, cudaStream_t, BPPlan&, const float*, const PiRecord*, float*);
-template Status launch_bkproj_v2<double>(int, cudaStream_t, BPPlan&, const float*, const PiRecord*, double*);
+template Status launch_bkproj_v2<float>(int, cudaStream_t, BPPlan&, const float*, const PiRecord*, float*, int*);
+template Status launch_bkproj_v2<double>(int, cudaStream_t, BPPlan&, const float*, const PiRecord*, double*, int*);
 
 }  // namespace ctr

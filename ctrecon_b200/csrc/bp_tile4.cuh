@@ -1,0 +1,371 @@
+// bp_tile4.cuh -- the fourth form of the voxel-driven backprojection tile
+// (KatsevichBkProj.cpp:164-265; FP32 interpolation and accumulation, the reference's endpoint
+// rule): the per-cell records and rounding floor of the third form (bp_tile3.cuh), with the
+// staging taken off the compute warps.
+//
+//  * Warp roles. Warps 0-7 (the 16 x 16 voxel columns of the tile, 8 slices each) only
+//    accumulate. PW producer warps compute the footprints of each block of NB views, copy the
+//    raw footprint rows with cp.async two blocks ahead, and build the 16-byte cell records
+//    {A, B, C, D} into a ring of S slots.
+//  * Hand-off. Slot s has a `full` mbarrier (every producer thread arrives after writing its
+//    records) and an `empty` one (every consumer thread arrives after its last read); phases
+//    follow a per-CTA block counter, so the ring runs on across the tiles of the persistent
+//    batched kernel. Every wait is bounded: a wait that gives up records an error code in the
+//    device word and the CTA abandons the tile (no write) after draining its copies.
+//  * Capacities (cell records and raw floats per staged view) are launch parameters sized on
+//    the host from the geometry; a view whose footprint does not fit, or reaches the detector
+//    border, is read directly from FProj with the first form's clamped indices.
+#pragma once
+
+#include "bp_tile3.cuh"
+
+namespace ctr {
+namespace bp {
+
+constexpr uint32_t kSpin4 = 1u << 22;
+
+__device__ __forceinline__ void mbar_init4(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count)
+                 : "memory");
+}
+__device__ __forceinline__ void mbar_arrive4(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+// bounded wait on the phase with the given parity; false if it gave up (error recorded) or
+// another thread already did
+__device__ __forceinline__ bool mbar_wait4(uint64_t* bar, uint32_t parity, int* err, int code) {
+    const uint32_t a = smem_addr(bar);
+    for (uint32_t it = 0; it < kSpin4; ++it) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, p;\n\t}"
+            : "=r"(ok)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (ok) return true;
+        if ((it & 255) == 255 && *(volatile int*)err) return false;
+    }
+    atomicCAS(err, 0, code);
+    return false;
+}
+
+struct Caps4 {
+    int cells;  // cell records per staged view (multiple of 4)
+    int raw;    // raw floats per staged view (multiple of 4)
+};
+
+template <int NB, int S, int PW>
+struct Shared4 {
+    uint64_t full[S], empty[S];
+    Foot3 foot[S][NB];
+    float4 vg[S][NB];
+    Foot3 pfoot[2][NB];  // producer side: footprints of the blocks being staged
+    float4 pvg[2][NB];
+    int s_pmin, s_pmax, s_abort;
+    long long s_item;
+};
+
+template <int NB, int S, int PW>
+__host__ __device__ inline size_t tile4_smem_bytes(const Caps4& c) {
+    return (size_t)S * NB * c.cells * 16 + (size_t)2 * NB * c.raw * sizeof(float);
+}
+
+template <int NB, int S, int PW>
+__device__ __forceinline__ void tile4_init(Shared4<NB, S, PW>& sh) {
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < S; ++s) {
+            mbar_init4(&sh.full[s], 32 * PW);
+            mbar_init4(&sh.empty[s], 256);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+}
+
+// One CTA tile: columns [16 bx, 16 bx + 16) x [16 by, 16 by + 16), slices [8 bz, 8 bz + 8).
+// Called by all 32 * (8 + PW) threads with the same `iter` (blocks of views this CTA has
+// processed before); returns the new count. Returns with no copies in flight. Sets
+// sh.s_abort (and leaves the tile unwritten) when a wait gave up.
+template <int NB, int S, int PW, typename OutT>
+__device__ __forceinline__ uint32_t tile4(const BPParams& kp, const float* __restrict__ fproj,
+                                          const PiRecord* __restrict__ pit,
+                                          const float4* __restrict__ views,
+                                          const float* __restrict__ xyz, OutT* __restrict__ image,
+                                          int bx, int by, int bz, Shared4<NB, S, PW>& sh,
+                                          unsigned char* dyn, Caps4 caps, int* err,
+                                          uint32_t iter) {
+    constexpr int TZ = 8;
+    const int ccap = caps.cells, rcap = caps.raw;
+    float4* cellbuf = reinterpret_cast<float4*>(dyn);                          // S * NB * ccap
+    float* raw = reinterpret_cast<float*>(dyn + (size_t)S * NB * ccap * 16);   // 2 * NB * rcap
+    const uint32_t cell_s = smem_addr(cellbuf);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const bool consumer = warp < 8;
+    const int NX = kp.NX, NY = kp.NY, NZ = kp.NZ, P = kp.P, YL = kp.YL, ZL = kp.ZL;
+    const int zb = bz * TZ;
+    const float* xc = xyz;
+    const float* yc = xyz + NX;
+    const float* zc = xyz + NX + NY;
+
+    // consumer state
+    const int tx = tid & (kTXY - 1), ty = (tid >> 4) & (kTXY - 1);
+    const int x = bx * kTXY + tx, y = by * kTXY + ty;
+    const bool col_ok = consumer && (x < NX) && (y < NY);
+    const size_t colbase = ((size_t)x * NY + y) * NZ;
+    VoxelRanges<TZ> vr;
+    load_ranges<TZ>(pit, colbase, zb, NZ, P, col_ok, vr);
+    int wmin = vr.tmin, wmax = vr.tmax;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        wmin = min(wmin, __shfl_xor_sync(0xffffffffu, wmin, o));
+        wmax = max(wmax, __shfl_xor_sync(0xffffffffu, wmax, o));
+    }
+    if (tid == 0) { sh.s_pmin = INT_MAX; sh.s_pmax = INT_MIN; sh.s_abort = 0; }
+    __syncthreads();
+    if (consumer && lane == 0 && wmin <= wmax) {
+        atomicMin(&sh.s_pmin, wmin);
+        atomicMax(&sh.s_pmax, wmax);
+    }
+    __syncthreads();
+    const int pmin = sh.s_pmin, pmax = sh.s_pmax;
+    if (pmin > pmax) return iter;
+    const int nblk = (pmax - pmin) / NB + 1;
+
+    const float R = kp.Rf, DdU = kp.DdU, DdV = kp.DdV, HalfY = kp.HalfY, HalfZ = kp.HalfZ;
+    float acc[TZ];
+#pragma unroll
+    for (int k = 0; k < TZ; ++k) acc[k] = 0.f;
+
+    if (!consumer) {
+        // ------------------------------------------------------------------ producers
+        const int pw = warp - 8;  // views j with j % PW == pw are this warp's
+        const int x0 = bx * kTXY, x1 = min(x0 + kTXY, NX) - 1;
+        const int y0 = by * kTXY, y1 = min(y0 + kTXY, NY) - 1;
+        const int z1 = min(zb + TZ, NZ) - 1;
+        const float bx0 = xc[x0], bx1 = xc[x1], by0 = yc[y0], by1 = yc[y1];
+        const float bz0 = zc[zb], bz1 = zc[z1];
+        // lane i < NB / PW owns view j = pw + i * PW of every block
+        constexpr int VPW = (NB + PW - 1) / PW;
+        const int jl = pw + lane * PW;
+        const bool vlane = lane < VPW && jl < NB;
+        // view geometry of this lane's view of block ib (zero past the range)
+        auto view_of = [&](int ib) {
+            const int p = pmin + ib * NB + jl;
+            return (vlane && ib < nblk && p <= pmax) ? views[p] : make_float4(0.f, 0.f, 0.f, 0.f);
+        };
+        // footprints of this warp's views of block ib; g = view_of(ib), loaded a block ahead
+        auto footprint = [&](int ib, float4 g) {
+            if (vlane) {
+                Foot3 f{0, 0, -1, 0};
+                const int p = pmin + ib * NB + jl;
+                if (p <= pmax) {
+                    float umin = 1e30f, umax = -1e30f, vmin = 1e30f, vmax = -1e30f;
+                    bool ok = true;
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) {
+                        const float cx = (c & 1) ? bx1 : bx0, cy = (c & 2) ? by1 : by0;
+                        const float fen = R - (cx * g.x + cy * g.y);
+                        ok = ok && (fen > 1e-3f * R);
+                        const float inv = 1.f / fen;
+                        const float u = (cy * g.x - cx * g.y) * DdU * inv + HalfY;
+                        const float va = (bz0 - g.z) * DdV * inv + HalfZ;
+                        const float vb = (bz1 - g.z) * DdV * inv + HalfZ;
+                        umin = fminf(umin, u); umax = fmaxf(umax, u);
+                        vmin = fminf(vmin, fminf(va, vb)); vmax = fmaxf(vmax, fmaxf(va, vb));
+                    }
+                    f = Foot3{0, 0, -2, 0};
+                    if (ok && fabsf(umin) < 1048576.f && fabsf(umax) < 1048576.f &&
+                        fabsf(vmin) < 1048576.f && fabsf(vmax) < 1048576.f) {
+                        const int u0 = (int)floorf(umin) - 1, u1 = (int)floorf(umax) + 2;
+                        const int v0 = (int)floorf(vmin) - 1, v1 = (int)floorf(vmax) + 2;
+                        const int W = u1 - u0 + 1, H = v1 - v0 + 1;
+                        if (u0 >= 0 && u1 <= YL - 1 && v0 >= 0 && v1 <= ZL - 1 && W <= 64 &&
+                            W * H <= rcap && (W - 1) * (H - 1) <= ccap)
+                            f = Foot3{u0, v0, W, H};
+                    }
+                }
+                sh.pfoot[ib & 1][jl] = f;
+                sh.pvg[ib & 1][jl] = g;
+            }
+            __syncwarp();
+        };
+        auto stage = [&](int ib) {  // raw rows of this warp's views of block ib
+            for (int j = pw; j < NB; j += PW) {
+                const Foot3 f = sh.pfoot[ib & 1][j];
+                if (f.W <= 0) continue;
+                const int p = pmin + ib * NB + j;
+                const float* src = fproj + ((size_t)p * ZL + f.v0) * YL + f.u0;
+                float* dst = raw + ((ib & 1) * NB + j) * rcap;
+                for (int r = 0; r < f.H; ++r) {
+                    if (lane < f.W) cp_async4(dst + r * f.W + lane, src + (size_t)r * YL + lane);
+                    if (lane + 32 < f.W)
+                        cp_async4(dst + r * f.W + lane + 32, src + (size_t)r * YL + lane + 32);
+                }
+            }
+            cp_async_commit();
+        };
+        footprint(0, view_of(0));
+        stage(0);
+        float4 gnext = view_of(1);
+        for (int ib = 0; ib < nblk; ++ib) {
+            if (ib + 1 < nblk) {
+                const float4 g = gnext;
+                gnext = view_of(ib + 2);  // in flight while this block is staged and built
+                footprint(ib + 1, g);
+                stage(ib + 1);
+            } else {
+                cp_async_commit();
+            }
+            cp_async_wait<1>();
+            __syncwarp();  // this block's raw rows of all lanes have landed
+            const uint32_t g = iter + ib, slot = g % S, use = g / S;
+            if (use >= 1 && !mbar_wait4(&sh.empty[slot], (use - 1) & 1, err, 11)) {
+                sh.s_abort = 1;
+                break;
+            }
+            for (int j = pw; j < NB; j += PW) {
+                const Foot3 f = sh.pfoot[ib & 1][j];
+                if (lane == 0) {
+                    sh.foot[slot][j] = f;
+                    sh.vg[slot][j] = sh.pvg[ib & 1][j];
+                }
+                if (f.W <= 0) continue;
+                const float* src = raw + ((ib & 1) * NB + j) * rcap;
+                float4* dst = cellbuf + ((size_t)slot * NB + j) * ccap;
+                const int Wc = f.W - 1;
+                for (int r = 0; r < f.H - 1; ++r) {
+                    for (int c = lane; c < Wc; c += 32) {
+                        const float* s0 = src + r * f.W + c;
+                        const float t00 = s0[0], t01 = s0[1], t10 = s0[f.W], t11 = s0[f.W + 1];
+                        const float h0 = t01 - t00, h1 = t11 - t10;
+                        const float g0 = t10 - t00, g1 = t11 - t01;
+                        dst[r * Wc + c] = make_float4(0.25f * ((t00 + t01) + (t10 + t11)),
+                                                      0.5f * (h0 + h1), 0.5f * (g0 + g1), h1 - h0);
+                    }
+                }
+            }
+            __syncwarp();  // raw slot (ib & 1) is free for block ib + 2
+            mbar_arrive4(&sh.full[slot]);
+        }
+        cp_async_wait<0>();
+    } else {
+        // ------------------------------------------------------------------ consumers
+        const float X = col_ok ? xc[x] : 0.f, Y = col_ok ? yc[y] : 0.f;
+        const float z0 = zc[zb];
+        const float dzf = kp.dzf;
+        const float HalfYm = HalfY - 0.5f, HalfZm = HalfZ - 0.5f;
+        for (int ib = 0; ib < nblk; ++ib) {
+            const uint32_t g = iter + ib, slot = g % S, use = g / S;
+            if (!mbar_wait4(&sh.full[slot], use & 1, err, 12)) {
+                sh.s_abort = 1;
+                break;
+            }
+            const int pb = pmin + ib * NB;
+            bool cells = true;
+#pragma unroll
+            for (int j = 0; j < NB; ++j) cells = cells && (sh.foot[slot][j].W > 0);
+            const bool fast = __all_sync(0xffffffffu, vr.all_valid && pb >= vr.flo &&
+                                                       pb + NB - 1 <= vr.fhi &&
+                                                       pb + NB - 1 <= pmax && cells);
+            if (col_ok && wmin <= wmax && !(pb + NB - 1 < wmin || pb > wmax)) {
+#pragma unroll 1
+                for (int j = 0; j < NB; ++j) {
+                    const int p = pb + j;
+                    if (p > pmax) break;
+                    if (!fast && (p < vr.tmin || p > vr.tmax)) continue;
+                    const Foot3 f = sh.foot[slot][j];
+                    const float4 gv = sh.vg[slot][j];
+                    const float fen = R - (X * gv.x + Y * gv.y);
+                    const float YY = Y * gv.x - X * gv.y;
+                    const float inv = rcp_approx(fen);
+                    const float kv = DdV * inv;
+                    const float r2 = fen * fen + YY * YY;
+                    const float dz0 = z0 - gv.z;
+                    if (f.W > 0) {
+                        const float u = fmaf(YY * DdU, inv, HalfYm);  // u - 1/2
+                        const float tu = u + kMagic;
+                        const float a = u - (tu - kMagic);           // alpha - 1/2
+                        const uint32_t W16 = (uint32_t)(f.W - 1) * 16u;
+                        const uint32_t cbase =
+                            cell_s + (uint32_t)((slot * NB + j) * ccap) * 16u +
+                            ((uint32_t)__float_as_int(tu) - (uint32_t)(kMagicBits + f.u0)) * 16u -
+                            (uint32_t)(kMagicBits + f.v0) * W16;
+                        if (fast) {
+#pragma unroll
+                            for (int k = 0; k < TZ; ++k) {
+                                const float dz = fmaf((float)k, dzf, dz0);
+                                const float v = fmaf(dz, kv, HalfZm);  // v - 1/2
+                                const float rinv = rsqrt_approx(fmaf(dz, dz, r2));
+                                const float tv = v + kMagic;
+                                const float b = v - (tv - kMagic);
+                                const float4 q = lds128((uint32_t)__float_as_int(tv) * W16 + cbase);
+                                acc[k] = fmaf(fmaf(b, fmaf(a, q.w, q.z), fmaf(a, q.y, q.x)), rinv,
+                                              acc[k]);
+                            }
+                        } else {
+#pragma unroll
+                            for (int k = 0; k < TZ; ++k) {
+                                const int d0 = p - vr.bi[k];
+                                const int d1 = vr.ti[k] + 1 - p;
+                                if ((d0 | d1) < 0) continue;
+                                float w = 1.f;
+                                if (d1 <= 1) w = ramp(vr.tf[k] + (float)(d1 - 1));
+                                else if (d0 <= 1) w = ramp((float)d0 - vr.bf[k]);
+                                const float dz = fmaf((float)k, dzf, dz0);
+                                const float v = fmaf(dz, kv, HalfZm);
+                                const float rinv = rsqrt_approx(fmaf(dz, dz, r2));
+                                const float tv = v + kMagic;
+                                const float b = v - (tv - kMagic);
+                                const float4 q = lds128((uint32_t)__float_as_int(tv) * W16 + cbase);
+                                acc[k] = fmaf(w * fmaf(b, fmaf(a, q.w, q.z), fmaf(a, q.y, q.x)),
+                                              rinv, acc[k]);
+                            }
+                        }
+                    } else {
+                        // direct reads with the clamped indices of the first form
+                        const float u = YY * DdU * inv + HalfY;
+                        const int ui = max(0, min(YL - 2, __float2int_rd(u)));
+                        const float alfa = u - (float)ui;
+                        const float* base = fproj + (size_t)p * ZL * YL + ui;
+#pragma unroll
+                        for (int k = 0; k < TZ; ++k) {
+                            const int d0 = p - vr.bi[k];
+                            const int d1 = vr.ti[k] + 1 - p;
+                            if ((d0 | d1) < 0) continue;
+                            float w = 1.f;
+                            if (d1 <= 1) w = ramp(vr.tf[k] + (float)(d1 - 1));
+                            else if (d0 <= 1) w = ramp((float)d0 - vr.bf[k]);
+                            const float dz = fmaf((float)k, dzf, dz0);
+                            const float v = fmaf(dz, kv, HalfZ);
+                            const float rinv = rsqrt_approx(fmaf(dz, dz, r2));
+                            const int vi = max(0, min(ZL - 2, __float2int_rd(v)));
+                            const float beta = v - (float)vi;
+                            const float* q = base + (size_t)vi * YL;
+                            const float t00 = __ldg(q), t01 = __ldg(q + 1);
+                            const float t10 = __ldg(q + YL), t11 = __ldg(q + YL + 1);
+                            const float a0 = fmaf(alfa, t01 - t00, t00);
+                            const float a1 = fmaf(alfa, t11 - t10, t10);
+                            acc[k] = fmaf(w * fmaf(beta, a1 - a0, a0), rinv, acc[k]);
+                        }
+                    }
+                }
+            }
+            mbar_arrive4(&sh.empty[slot]);
+        }
+    }
+    __syncthreads();  // every role is done with the ring; an abort is visible
+    if (col_ok && !sh.s_abort) {
+#pragma unroll
+        for (int k = 0; k < TZ; ++k) {
+            const int z = zb + k;
+            if (z < NZ && vr.bi[k] != kPiInvalid) image[colbase + z] = (OutT)(-acc[k] * kp.invPs);
+        }
+    }
+    __syncthreads();  // the caller may reuse the shared state for the next tile
+    return iter + nblk;
+}
+
+}  // namespace bp
+}  // namespace ctr

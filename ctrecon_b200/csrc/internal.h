@@ -6,6 +6,8 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <functional>
+#include <map>
 #include <memory>
 #include <string>
 #include <vector>
@@ -117,7 +119,22 @@ struct BPPlan {
     BPParams kp{};
     DevBuf views;   // float4 per view: cos, sin, source z, 0
     DevBuf xyz;     // float voxel coordinates x[NX], y[NY], z[NZ]
+    int caps_cells = 0, caps_raw = 0;  // fourth-form staging capacities (bp4_caps)
 };
+// Sizes the fourth form's staging capacities of a plan (once).
+void bp4_caps(BPPlan& plan);
+// Autotuner (autotune.cpp): the tuning-table key of a geometry, the form to use for a plan
+// (the option, or the table's entry under CTRECON_BP_AUTO), and the candidate forms.
+std::string tune_key(const BPGeom& g);
+int bp_variant_for(const ctrecon_ctx* ctx, const BPGeom& g);
+extern const int kTuneCandidates[];
+extern const int kNumTuneCandidates;
+constexpr int kDefaultBPVariant = 2;
+// Times every candidate form: prepare(v) (untimed, may be empty) then run_one(v) three times,
+// the last two timed with CUDA events on s; candidates that cannot launch are marked -1.
+Status tune_candidates(ctrecon_tune_result* res, cudaStream_t s,
+                       const std::function<Status(int)>& prepare,
+                       const std::function<Status(int)>& run_one);
 
 // One scan of a batched backprojection (batch.cpp, bkproj2.cu)
 struct BatchScanDev {
@@ -167,6 +184,8 @@ struct ctrecon_ctx {
     ctr::DevBuf ws_ell;      // phantom ellipsoids
     ctr::DevBuf ws_flag;     // device error word
     ctr::PinetState pinet;   // learned PI-line initialiser
+    // autotuner: backprojector form per geometry key (tune_key), with its time
+    std::map<std::string, std::pair<int, float>> tune;
 };
 
 namespace ctr {

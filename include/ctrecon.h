@@ -96,7 +96,11 @@ typedef enum ctrecon_option {
     CTRECON_OPT_FILTER_CHUNK = 3,     /* views per filter work chunk; default 512 */
     CTRECON_OPT_BP_VARIANT = 4,       /* backprojector variant, default 2: 0, 1 = per-cell
                                          records, blocks of 4 / 8 views; 2, 3, 4 = second
-                                         form (slices x views) 8x8, 4x8, 8x4; 100 = first form */
+                                         form (slices x views) 8x8, 4x8, 8x4; 5, 6, 7 = per-cell
+                                         records staged by producer warps (views per block x
+                                         ring slots x producer warps) 4x2x1, 2x4x1, 4x2x2;
+                                         8, 9 = the same with 4x2x3, 4x3x4; 100 = first
+                                         form; CTRECON_BP_AUTO = the tuning table's choice */
     CTRECON_OPT_VERBOSE = 5
 } ctrecon_option;
 
@@ -195,7 +199,7 @@ ctrecon_status ctrecon_batch_create(ctrecon_ctx* ctx, int n_scans,
                                     const ctrecon_filter_params* params,
                                     const ctrecon_bp_geom* geoms, ctrecon_batch** out);
 void ctrecon_batch_destroy(ctrecon_batch* batch);
-/* backprojector form of the batch: 0 .. 4 as CTRECON_OPT_BP_VARIANT (default: the context's) */
+/* backprojector form of the batch: 0 .. 9 as CTRECON_OPT_BP_VARIANT (default: the context's) */
 ctrecon_status ctrecon_batch_set_variant(ctrecon_batch* batch, int variant);
 /* d_proj[i] (input), d_fproj[i] (work), d_image[i] (output, in place) for scan i */
 ctrecon_status ctrecon_batch_run_dev(ctrecon_batch* batch, void* stream,
@@ -203,6 +207,36 @@ ctrecon_status ctrecon_batch_run_dev(ctrecon_batch* batch, void* stream,
                                      float* const* d_image, int use_graph);
 /* sum(LoopEnd-LoopBegin+1) of each scan (bisection PI solve, synchronous) */
 ctrecon_status ctrecon_batch_updates(ctrecon_batch* batch, unsigned long long* host_updates);
+
+/* ---- autotuner (no counterpart in the reference) -----------------------------------------
+ * Times candidate backprojector forms -- tile shapes (slices per thread) and view-block
+ * depths / staging rings, the CTRECON_OPT_BP_VARIANT values -- on the caller's own data and
+ * keeps the fastest. Timing uses CUDA events on `stream` and is synchronous. The
+ * backprojection assigns voxel values (it does not accumulate), so tuning on the caller's
+ * image leaves it as one backprojection would. */
+#define CTRECON_BP_AUTO (-1) /* CTRECON_OPT_BP_VARIANT value: use the tuning table */
+#define CTRECON_TUNE_MAX 16
+typedef struct ctrecon_tune_result {
+    int best_variant;
+    float best_ms;                      /* mean device time per launch of the best form */
+    int n;                              /* candidates tried */
+    int variants[CTRECON_TUNE_MAX];
+    float ms[CTRECON_TUNE_MAX];         /* mean time per launch; -1 = does not fit */
+} ctrecon_tune_result;
+/* Single scan: tunes the backprojection of d_fproj with the PI table d_pitab (NULL: solved
+ * first) into d_image, records the winner for this geometry in the context's tuning table
+ * (used when CTRECON_OPT_BP_VARIANT is CTRECON_BP_AUTO) and returns the timings. */
+ctrecon_status ctrecon_tune_bkproj(ctrecon_ctx* ctx, void* stream, const ctrecon_bp_geom* g,
+                                   const float* d_fproj, const void* d_pitab, float* d_image,
+                                   ctrecon_tune_result* out);
+/* Batch: runs the batch once (filters and PI solves included), then times its persistent
+ * backprojection launch for each candidate form and keeps the fastest for this batch. */
+ctrecon_status ctrecon_batch_tune(ctrecon_batch* batch, void* stream, const float* const* d_proj,
+                                  float* const* d_fproj, float* const* d_image,
+                                  ctrecon_tune_result* out);
+/* The tuning table as text (one geometry per line); load merges into the context's table. */
+ctrecon_status ctrecon_tune_save(const ctrecon_ctx* ctx, const char* path);
+ctrecon_status ctrecon_tune_load(ctrecon_ctx* ctx, const char* path);
 
 /* ---- learned PI-line initialiser (no counterpart in the reference) -----------------------
  * A 3 -> 64 -> 64 -> 64 -> 64 -> 2 SiLU network mapping (r/0.25, cos psi, sin psi), with r and
