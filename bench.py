@@ -358,9 +358,15 @@ def run_batched(args):
         tune = None
         if args.bp_variant == -1:
             # the autotuner picks the batch's backprojector form (tile shape, view-block
-            # depth, staging) on these scans, untimed
+            # depth, staging) on these scans, and each scan's own form for the one-at-a-time
+            # runs (the table behind CTRECON_BP_AUTO), untimed
             tune = b.tune(projs, fprojs, imgs, stream=stream)
-            ctx.set_option(_lib.OPT_BP_VARIANT, tune["best_variant"])  # one-at-a-time too
+            single = []
+            for s_, d, f, im in zip(scans, projs, fprojs, imgs):
+                ctx.filter_dev(ct.scan_filter_params(s_), d, f)
+                single.append(ctx.tune_bkproj(s_.geom_struct(), f, im)["best_variant"])
+            ctx.set_option(_lib.OPT_BP_VARIANT, _lib.BP_AUTO)
+            tune["single_scan_best"] = single
         else:
             b.set_variant(args.bp_variant if args.bp_variant < 100 else 2)
             ctx.set_option(_lib.OPT_BP_VARIANT, args.bp_variant)

@@ -18,37 +18,20 @@
 #pragma once
 
 #include "bp_tile3.cuh"
+#include "tc_util.cuh"
 
 namespace ctr {
 namespace bp {
 
-constexpr uint32_t kSpin4 = 1u << 22;
-
 __device__ __forceinline__ void mbar_init4(uint64_t* bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count)
-                 : "memory");
+    tcu::mbar_init(bar, count);
 }
 __device__ __forceinline__ void mbar_arrive4(uint64_t* bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
 }
-// bounded wait on the phase with the given parity; false if it gave up (error recorded) or
-// another thread already did
+// bounded wait (suspend-hinted try_wait, time limit): tc_util.cuh
 __device__ __forceinline__ bool mbar_wait4(uint64_t* bar, uint32_t parity, int* err, int code) {
-    const uint32_t a = smem_addr(bar);
-    for (uint32_t it = 0; it < kSpin4; ++it) {
-        uint32_t ok;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.b32 %0, 1, 0, p;\n\t}"
-            : "=r"(ok)
-            : "r"(a), "r"(parity)
-            : "memory");
-        if (ok) return true;
-        if ((it & 255) == 255 && *(volatile int*)err) return false;
-    }
-    atomicCAS(err, 0, code);
-    return false;
+    return tcu::mbar_wait(bar, parity, err, code);
 }
 
 struct Caps4 {

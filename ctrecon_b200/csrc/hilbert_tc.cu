@@ -19,6 +19,7 @@
 // Every mbarrier wait is bounded; a wait that gives up records an error code in a device word
 // (read by the host after the call) and the CTA skips ahead, frees its TMEM and returns.
 #include "internal.h"
+#include "tc_util.cuh"
 
 #include <cuda.h>
 #include <cudaTypedefs.h>
@@ -33,7 +34,6 @@ namespace ctr {
 namespace {
 
 constexpr int kM = 128;
-constexpr uint32_t kSpinLimit = 1u << 22;
 
 struct TcParams {
     int AL, YL, ZL, nviews, vpt, ntile, nk, ALs;
@@ -57,23 +57,9 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
                  : "memory");
 }
 
-// bounded wait on the phase with the given parity; false if it gave up (error recorded)
+// bounded wait (suspend-hinted try_wait, time limit): tc_util.cuh
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err, int code) {
-    const uint32_t a = smem_u32(bar);
-    for (uint32_t it = 0; it < kSpinLimit; ++it) {
-        uint32_t ok;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.b32 %0, 1, 0, p;\n\t}"
-            : "=r"(ok)
-            : "r"(a), "r"(parity)
-            : "memory");
-        if (ok) return true;
-        if ((it & 255) == 255 && *(volatile int*)err) return false;
-    }
-    atomicCAS(err, 0, code);
-    return false;
+    return tcu::mbar_wait(bar, parity, err, code);
 }
 
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar,

@@ -6,10 +6,22 @@
 namespace ctr {
 namespace tcu {
 
-constexpr uint32_t kSpinLimit = 1u << 22;
+// Bounded mbarrier waits: each try_wait carries a suspend-time hint, so a waiting thread sleeps
+// until the phase completes (or the hint expires) instead of spinning on the issue slots the
+// threads it waits for need; the whole wait gives up after kWaitLimitNs of %globaltimer time
+// (or kWaitIterLimit tries), recording `code` in the device error word.
+constexpr uint32_t kSuspendHintNs = 1u << 20;              // ~1 ms per try
+constexpr uint64_t kWaitLimitNs = 2000000000ull;           // 2 s
+constexpr uint32_t kWaitIterLimit = 1u << 24;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
 }
 
 __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
@@ -17,20 +29,28 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
                  : "memory");
 }
 
-// bounded wait on the phase with the given parity; false if it gave up (error recorded)
+__device__ __forceinline__ bool mbar_try_wait(uint32_t a, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(a), "r"(parity), "r"(kSuspendHintNs)
+        : "memory");
+    return ok != 0;
+}
+
+// bounded wait on the phase with the given parity; false if it gave up (error recorded) or
+// another thread of the launch already gave up
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err, int code) {
     const uint32_t a = smem_u32(bar);
-    for (uint32_t it = 0; it < kSpinLimit; ++it) {
-        uint32_t ok;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.b32 %0, 1, 0, p;\n\t}"
-            : "=r"(ok)
-            : "r"(a), "r"(parity)
-            : "memory");
-        if (ok) return true;
-        if ((it & 255) == 255 && *(volatile int*)err) return false;
+    if (mbar_try_wait(a, parity)) return true;
+    const uint64_t t0 = globaltimer_ns();
+    for (uint32_t it = 1; it < kWaitIterLimit; ++it) {
+        if (mbar_try_wait(a, parity)) return true;
+        if (*(volatile int*)err) return false;
+        if (globaltimer_ns() - t0 > kWaitLimitNs) break;
     }
     atomicCAS(err, 0, code);
     return false;
