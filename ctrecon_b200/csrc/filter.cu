@@ -25,6 +25,7 @@ namespace ctr {
 // ---------------------------------------------------------------------------------------------
 // K1
 // ---------------------------------------------------------------------------------------------
+constexpr int kRowGroups = 4;  // independent row walks per column in K1
 // Output formats of the kappa rows: FP32 (SIMT Hilbert), BF16 hi and lo planes (BF16x3
 // tensor-core Hilbert; the lo plane starts `plane` elements after the hi plane), or FP32
 // rounded to TF32 (round to nearest) for the TF32 tensor-core Hilbert.
@@ -43,48 +44,55 @@ __device__ __forceinline__ void store_kappa(void* X, size_t idx, size_t plane, f
     }
 }
 
+// Block (T columns) x (RG row groups): thread (tx, ry) owns column j = blockIdx.x * T + tx and
+// computes the derivative rows k = ry, ry + RG, ... then the kappa rows a = ry, ry + RG, ...;
+// the RG groups keep RG independent row walks in flight per column.
 __global__ void k_deriv_rebin(const float* __restrict__ proj, int proj_view0, int P, int YL,
                               int ZL, int AL, int YLp, int vbeg,
                               const FwEntry* __restrict__ fw, const float2* __restrict__ cuy,
                               const float* __restrict__ zcv, float inv2dl,
                               void* __restrict__ X, size_t plane, int mode) {
-    extern __shared__ float gf[];  // ZL x blockDim.x, each thread owns one column
-    const int T = blockDim.x, tid = threadIdx.x;
-    const int j = blockIdx.x * T + tid;
+    extern __shared__ float gf[];  // ZL x blockDim.x: the derivative of the block's columns
+    const int T = blockDim.x, tx = threadIdx.x, ry = threadIdx.y, RG = blockDim.y;
+    const int j = blockIdx.x * T + tx;
     const int p = vbeg + blockIdx.y;
     const size_t xv = (size_t)blockIdx.y * AL * YLp;
+    const bool real = j < YL;
+    if (real) {
+        const size_t S = (size_t)YL * ZL;
+        // view derivative: views 0 and P-1 reuse the derivative of views 1 and P-2 (:58-59)
+        const int pc = p < 1 ? 1 : (p > P - 2 ? P - 2 : p);
+        const float* Pm = proj + (size_t)(pc - 1 - proj_view0) * S;
+        const float* Pp = proj + (size_t)(pc + 1 - proj_view0) * S;
+        const float* Pv = proj + (size_t)(p - proj_view0) * S;
+        // u stencil with the reference's edge rule (:63-78)
+        int jl = j - 1, jr = j + 1;
+        if (j < 2) { jl = 0; jr = 2; }
+        else if (j > YL - 3) { jl = YL - 3; jr = YL - 1; }
+        const float2 cy = cuy[j];  // (u coefficient, y coordinate)
+#pragma unroll 2
+        for (int k = ry; k < ZL; k += RG) {
+            int kl = k - 1, kr = k + 1;  // v stencil, same edge rule (:85-95)
+            if (k < 2) { kl = 0; kr = 2; }
+            else if (k > ZL - 3) { kl = ZL - 3; kr = ZL - 1; }
+            const float* row = Pv + (size_t)k * YL;
+            float g = (Pp[(size_t)k * YL + j] - Pm[(size_t)k * YL + j]) * inv2dl;
+            g = fmaf(row[jr] - row[jl], cy.x, g);
+            g = fmaf(zcv[k] * cy.y, Pv[(size_t)kr * YL + j] - Pv[(size_t)kl * YL + j], g);
+            gf[k * T + tx] = g;
+        }
+    }
+    __syncthreads();
     if (j >= YLp) return;
-    if (j >= YL) {  // zero padding of the kappa rows (the GEMM form reads K = YLp)
-        for (int a = 0; a < AL; ++a) store_kappa(X, xv + (size_t)a * YLp + j, plane, 0.f, mode);
+    if (!real) {  // zero padding of the kappa rows (the GEMM form reads K = YLp)
+        for (int a = ry; a < AL; a += RG) store_kappa(X, xv + (size_t)a * YLp + j, plane, 0.f, mode);
         return;
     }
-    const size_t S = (size_t)YL * ZL;
-    // view derivative: views 0 and P-1 reuse the derivative of views 1 and P-2 (:58-59)
-    const int pc = p < 1 ? 1 : (p > P - 2 ? P - 2 : p);
-    const float* Pm = proj + (size_t)(pc - 1 - proj_view0) * S;
-    const float* Pp = proj + (size_t)(pc + 1 - proj_view0) * S;
-    const float* Pv = proj + (size_t)(p - proj_view0) * S;
-    // u stencil with the reference's edge rule (:63-78)
-    int jl = j - 1, jr = j + 1;
-    if (j < 2) { jl = 0; jr = 2; }
-    else if (j > YL - 3) { jl = YL - 3; jr = YL - 1; }
-    const float2 cy = cuy[j];  // (u coefficient, y coordinate)
-#pragma unroll 4
-    for (int k = 0; k < ZL; ++k) {
-        int kl = k - 1, kr = k + 1;  // v stencil, same edge rule (:85-95)
-        if (k < 2) { kl = 0; kr = 2; }
-        else if (k > ZL - 3) { kl = ZL - 3; kr = ZL - 1; }
-        const float* row = Pv + (size_t)k * YL;
-        float g = (Pp[(size_t)k * YL + j] - Pm[(size_t)k * YL + j]) * inv2dl;
-        g = fmaf(row[jr] - row[jl], cy.x, g);
-        g = fmaf(zcv[k] * cy.y, Pv[(size_t)kr * YL + j] - Pv[(size_t)kl * YL + j], g);
-        gf[k * T + tid] = g;
-    }
-#pragma unroll 4
-    for (int a = 0; a < AL; ++a) {
+#pragma unroll 2
+    for (int a = ry; a < AL; a += RG) {
         const FwEntry f = fw[(size_t)a * YL + j];
         store_kappa(X, xv + (size_t)a * YLp + j, plane,
-                    fmaf(f.wa, gf[f.r0 * T + tid], f.wb * gf[f.r1 * T + tid]), mode);
+                    fmaf(f.wa, gf[f.r0 * T + tx], f.wb * gf[f.r1 * T + tx]), mode);
     }
 }
 
@@ -223,6 +231,7 @@ Status launch_filter(ctrecon_ctx* ctx, cudaStream_t s, FilterPlan& plan, const f
     int tj = 128;
     while (tj > 32 && (size_t)ZL * tj * sizeof(float) > 96 * 1024) tj /= 2;
     const size_t smem1 = (size_t)ZL * tj * sizeof(float);
+    const dim3 b1(tj, kRowGroups);
     if (smem1 > 200 * 1024)
         return make_status(CTRECON_ERR_UNSUPPORTED, "too many detector rows for K1");
     CTR_CUDA(cudaFuncSetAttribute(k_deriv_rebin, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -243,7 +252,7 @@ Status launch_filter(ctrecon_ctx* ctx, cudaStream_t s, FilterPlan& plan, const f
         const int n = std::min(chunk, view_end - c0);
         dim3 g1((YLp + tj - 1) / tj, n);
         const size_t plane = (size_t)n * AL * YLp;
-        k_deriv_rebin<<<g1, tj, smem1, s>>>(d_proj, proj_view0, P, YL, ZL, AL, YLp, c0,
+        k_deriv_rebin<<<g1, b1, smem1, s>>>(d_proj, proj_view0, P, YL, ZL, AL, YLp, c0,
                                             plan.fw.as<FwEntry>(), plan.cuy.as<float2>(),
                                             plan.zcv.as<float>(), plan.inv2dl, X, plane, mode);
         CTR_CUDA(cudaGetLastError());
@@ -272,6 +281,7 @@ Status launch_filter_fp32_preplaced(cudaStream_t s, const FilterTables& t, int Y
     int tj = 128;
     while (tj > 32 && (size_t)ZL * tj * sizeof(float) > 96 * 1024) tj /= 2;
     const size_t smem1 = (size_t)ZL * tj * sizeof(float);
+    const dim3 b1(tj, kRowGroups);
     if (smem1 > 200 * 1024)
         return make_status(CTRECON_ERR_UNSUPPORTED, "too many detector rows for K1");
     CTR_CUDA(cudaFuncSetAttribute(k_deriv_rebin, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -289,7 +299,7 @@ Status launch_filter_fp32_preplaced(cudaStream_t s, const FilterTables& t, int Y
     for (int c0 = 0; c0 < P; c0 += chunk) {
         const int n = std::min(chunk, P - c0);
         dim3 g1((YLp + tj - 1) / tj, n);
-        k_deriv_rebin<<<g1, tj, smem1, s>>>(d_proj, 0, P, YL, ZL, AL, YLp, c0, fw, cuy, zcv,
+        k_deriv_rebin<<<g1, b1, smem1, s>>>(d_proj, 0, P, YL, ZL, AL, YLp, c0, fw, cuy, zcv,
                                             inv2dl, kappa, 0, CTRECON_HILBERT_FP32);
         CTR_CUDA(cudaGetLastError());
         dim3 g2((YL + kTileI - 1) / kTileI, n);

@@ -12,9 +12,10 @@
 //   BF16X3: T and X split into BF16 hi + lo; D = Thi*Xhi + Thi*Xlo + Tlo*Xhi (kind::f16,
 //           FP32 accumulation) -- the dropped Tlo*Xlo term is ~2^-16 relative;
 //   TF32:   one kind::tf32 product of RN-rounded operands (about 2^-11 relative per term).
-// Epilogue: each warp reads its 32 TMEM lanes (32 output columns), one view at a time,
-// transposes them through shared memory, and gathers FProj[v][z][i] = gb*D[i][b] + ge*D[i][e]
-// (the backward-rebin rows b, e and weights gb, ge of the host table), storing coalesced rows.
+// Epilogue (8 warps, two per TMEM lane quarter): the tile's accumulators go through a shared
+// transpose buffer, then FProj[v][z][i] = gb*D[i][b] + ge*D[i][e] (the backward-rebin rows b, e
+// and weights gb, ge of the host table) is gathered for all views of the tile per table entry,
+// storing coalesced rows.
 //
 // Every mbarrier wait is bounded; a wait that gives up records an error code in a device word
 // (read by the host after the call) and the CTA skips ahead, frees its TMEM and returns.
@@ -36,7 +37,7 @@ namespace {
 constexpr int kM = 128;
 
 struct TcParams {
-    int AL, YL, ZL, nviews, vpt, ntile, nk, ALs;
+    int AL, YL, ZL, nviews, vpt, ntile, nk, ALt;  // ALt: odd row stride >= vpt * AL
     const BkEntry* bk;
     float* out;
     int* err;
@@ -141,7 +142,7 @@ __host__ __device__ inline uint32_t tmem_cols_for(int ntile) {
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(128, 1)
+__global__ void __launch_bounds__(256, 1)
 k_hilbert_tc(const __grid_constant__ CUtensorMap tA0, const __grid_constant__ CUtensorMap tA1,
              const __grid_constant__ CUtensorMap tB0, const __grid_constant__ CUtensorMap tB1,
              TcParams p) {
@@ -225,36 +226,40 @@ k_hilbert_tc(const __grid_constant__ CUtensorMap tA0, const __grid_constant__ CU
     }
     __syncwarp();
 
-    // epilogue: all four warps; warp w owns TMEM lanes [32w, 32w+32) = output columns
+    // epilogue: eight warps. Warp w reads TMEM lanes [32 (w & 3), +32) (= output columns) for
+    // the views vl = (w >> 2), (w >> 2) + 2, ... of the tile into the shared transpose buffer
+    // of its lane quarter; after a barrier, each warp gathers rows z = (w >> 2), +2, ... of
+    // every view of the tile, so each backward-rebin table entry is loaded once per tile.
     const bool have = __all_sync(0xffffffffu, mbar_wait(done, 0, p.err, 3));
     tc_fence_after();
+    const int q = warp & 3, h = warp >> 2;
+    const int nv = min(p.vpt, p.nviews - vg0);
+    float* trq = reinterpret_cast<float*>(smem) + (size_t)q * 32 * p.ALt;
+    const int i = i0 + q * 32 + lane;
     if (have) {
-        float* tr = reinterpret_cast<float*>(smem) + (size_t)warp * 32 * p.ALs;
-        const int i = i0 + warp * 32 + lane;
-        const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
-        for (int vl = 0; vl < p.vpt; ++vl) {
-            const int v = vg0 + vl;
-            if (v >= p.nviews) break;
+        const uint32_t lane_addr = tmem + ((uint32_t)(q * 32) << 16);
+        for (int vl = h; vl < nv; vl += 2) {
             const int c0 = vl * p.AL;
             int c = 0;
             for (; c + 16 <= p.AL; c += 16) {
                 float r[16];
                 tmem_ld16(lane_addr + (uint32_t)(c0 + c), r);
 #pragma unroll
-                for (int q = 0; q < 16; ++q) tr[lane * p.ALs + c + q] = r[q];
+                for (int k = 0; k < 16; ++k) trq[lane * p.ALt + c0 + c + k] = r[k];
             }
-            for (; c < p.AL; ++c) tr[lane * p.ALs + c] = tmem_ld1(lane_addr + (uint32_t)(c0 + c));
-            __syncwarp();
-            if (i < p.YL) {
-                const float* row = tr + lane * p.ALs;
-                float* o = p.out + (size_t)v * p.ZL * p.YL + i;
-#pragma unroll 8
-                for (int k = 0; k < p.ZL; ++k) {
-                    const BkEntry e = p.bk[(size_t)k * p.YL + i];
-                    o[(size_t)k * p.YL] = fmaf(e.gb, row[e.b], e.ge * row[e.e]);
-                }
-            }
-            __syncwarp();
+            for (; c < p.AL; ++c) trq[lane * p.ALt + c0 + c] = tmem_ld1(lane_addr + (uint32_t)(c0 + c));
+        }
+    }
+    __syncthreads();
+    if (have && i < p.YL) {
+        const float* row = trq + lane * p.ALt;
+        float* o = p.out + (size_t)vg0 * p.ZL * p.YL + i;
+        const size_t vstride = (size_t)p.ZL * p.YL;
+        for (int k = h; k < p.ZL; k += 2) {
+            const BkEntry e = p.bk[(size_t)k * p.YL + i];
+            float* ok = o + (size_t)k * p.YL;
+            for (int vl = 0; vl < nv; ++vl)
+                ok[vl * vstride] = fmaf(e.gb, row[vl * p.AL + e.b], e.ge * row[vl * p.AL + e.e]);
         }
     }
     tc_fence_before();
@@ -380,13 +385,13 @@ Status launch_hilbert_tc(ctrecon_ctx* ctx, cudaStream_t s, FilterPlan& plan, con
     TcParams p;
     p.AL = AL; p.YL = YL; p.ZL = ZL; p.nviews = nviews; p.vpt = vpt; p.ntile = ntile;
     p.nk = YLp / (int)kin;
-    p.ALs = AL | 1;
+    p.ALt = (vpt * AL) | 1;
     p.bk = plan.bk.as<BkEntry>();
     p.out = d_fproj_chunk;
     p.err = ctx->ws_flag.as<int>();
     const int PL = bf ? 2 : 1, S = bf ? 2 : 4;
     const size_t stage = (size_t)PL * (kM * 128 + (size_t)ntile * 128);
-    const size_t epi = (size_t)4 * 32 * p.ALs * sizeof(float);
+    const size_t epi = (size_t)4 * 32 * p.ALt * sizeof(float);
     const size_t smem = std::max(S * stage, epi) + 1024 + 256;
     if ((size_t)S * stage < epi)
         return make_status(CTRECON_ERR_INTERNAL, "epilogue buffer exceeds the stage memory");
@@ -394,11 +399,11 @@ Status launch_hilbert_tc(ctrecon_ctx* ctx, cudaStream_t s, FilterPlan& plan, con
     if (bf) {
         CTR_CUDA(cudaFuncSetAttribute(k_hilbert_tc<CTRECON_HILBERT_BF16X3>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_hilbert_tc<CTRECON_HILBERT_BF16X3><<<grid, 128, smem, s>>>(tA0, tA1, tB0, tB1, p);
+        k_hilbert_tc<CTRECON_HILBERT_BF16X3><<<grid, 256, smem, s>>>(tA0, tA1, tB0, tB1, p);
     } else {
         CTR_CUDA(cudaFuncSetAttribute(k_hilbert_tc<CTRECON_HILBERT_TF32>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_hilbert_tc<CTRECON_HILBERT_TF32><<<grid, 128, smem, s>>>(tA0, tA1, tB0, tB1, p);
+        k_hilbert_tc<CTRECON_HILBERT_TF32><<<grid, 256, smem, s>>>(tA0, tA1, tB0, tB1, p);
     }
     CTR_CUDA(cudaGetLastError());
     return Status::Ok();
