@@ -38,6 +38,18 @@ class FilterParams(ctypes.Structure):
                 ("proj_number", ctypes.c_int)]
 
 
+class ProjFileHeader(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in (
+        "source_to_center", "source_to_detector", "det_reso_u", "det_reso_v", "det_pixel_u",
+        "det_pixel_v", "det_center_u", "det_center_v", "is_arc", "start_angle_deg", "start_z",
+        "pitch", "total_views", "views_per_turn")] + [("storage_order", ctypes.c_double * 3)]
+
+
+class ImgFileHeader(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double * 3) for n in ("reso", "pixel", "ctr_idx", "center",
+                                                    "storage_order")]
+
+
 BP_AUTO = -1
 TUNE_MAX = 16
 
@@ -107,6 +119,12 @@ SIGNATURES = [
     ("ctrecon_geometry_sizing", None, [ctypes.c_double] * 4 + [ctypes.c_int] * 2 + [_dp] * 3),
     ("ctrecon_phantom_project_dev", _st, [_vp, _vp, ctypes.POINTER(BPGeom), _dp, ctypes.c_int,
                                           ctypes.c_double, ctypes.c_uint64, _vp]),
+    ("ctrecon_projfile_read", _st, [ctypes.c_char_p, ctypes.POINTER(ProjFileHeader), _dp,
+                                    ctypes.c_size_t]),
+    ("ctrecon_projfile_write", _st, [ctypes.c_char_p, ctypes.POINTER(ProjFileHeader), _dp]),
+    ("ctrecon_imgfile_read", _st, [ctypes.c_char_p, ctypes.POINTER(ImgFileHeader), _dp,
+                                   ctypes.c_size_t]),
+    ("ctrecon_imgfile_write", _st, [ctypes.c_char_p, ctypes.POINTER(ImgFileHeader), _dp]),
 ]
 
 _lib = None

@@ -299,6 +299,38 @@ ctrecon_status ctrecon_phantom_project_dev(ctrecon_ctx* ctx, void* stream,
                                            int n_ell, double photons, uint64_t seed,
                                            float* d_proj);
 
+/* ---- the reference's data files (host only, no GPU) ---------------------------------------
+ * ProjectionData.m:113-176 and ReconImage.m:60-117 store little-endian doubles: a header of
+ * scalars, the data array, then a 3-entry storage order ([1 2 3] = U V P for projections,
+ * X Y Z for images; the data's MATLAB dimensions are those axes in that order). The readers
+ * validate the file size against the header; `data` may be NULL to read the header alone. */
+typedef struct ctrecon_projfile_header {
+    double source_to_center, source_to_detector;  /* SourceToCenterDistance, ...DetectorDistance */
+    double det_reso_u, det_reso_v;                /* DetResoU, DetResoV (cells) */
+    double det_pixel_u, det_pixel_v;              /* DetPixelSizeU, DetPixelSizeV */
+    double det_center_u, det_center_v;            /* DetCntIdxU, DetCntIdxV (0-based) */
+    double is_arc;                                /* IsArcDetector (1 arc, 0 flat) */
+    double start_angle_deg, start_z, pitch;       /* StartSourceAngle, StartSourceZPos, Pitch */
+    double total_views, views_per_turn;           /* TotalProjectionNumber, ...PerTurn */
+    double storage_order[3];                      /* StorageOrder */
+} ctrecon_projfile_header;
+ctrecon_status ctrecon_projfile_read(const char* path, ctrecon_projfile_header* h, double* data,
+                                     size_t capacity);
+ctrecon_status ctrecon_projfile_write(const char* path, const ctrecon_projfile_header* h,
+                                      const double* data);
+
+typedef struct ctrecon_imgfile_header {
+    double reso[3];          /* resoX, resoY, resoZ */
+    double pixel[3];         /* pixelSizeX, ... */
+    double ctr_idx[3];       /* ctrIdxX, ... */
+    double center[3];        /* imgCenterX, ... */
+    double storage_order[3]; /* storageOrder */
+} ctrecon_imgfile_header;
+ctrecon_status ctrecon_imgfile_read(const char* path, ctrecon_imgfile_header* h, double* data,
+                                    size_t capacity);
+ctrecon_status ctrecon_imgfile_write(const char* path, const ctrecon_imgfile_header* h,
+                                     const double* data);
+
 #ifdef __cplusplus
 }
 #endif
