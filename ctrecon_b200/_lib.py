@@ -87,6 +87,7 @@ SIGNATURES = [
     ("ctrecon_pi_table_bytes", _st, [ctypes.POINTER(BPGeom), ctypes.POINTER(ctypes.c_size_t)]),
     ("ctrecon_pi_dev", _st, [_vp, _vp, ctypes.POINTER(BPGeom), _vp, _vp]),
     ("ctrecon_bkproj_dev_f32", _st, [_vp, _vp, ctypes.POINTER(BPGeom), _vp, _vp, _vp]),
+    ("ctrecon_filter_mode1_dev_f32", _st, [_vp, _vp, ctypes.POINTER(FilterParams), _vp, _vp]),
     ("ctrecon_filter_noalloc_dev_f32", _st, [_vp, ctypes.POINTER(FilterParams), _vp, _vp]),
     ("ctrecon_sync", _st, [_vp, _vp]),
     ("ctrecon_pi_dev_stats", _st, [_vp, _vp, ctypes.POINTER(BPGeom), _vp, _vp, _vp]),
@@ -119,6 +120,12 @@ SIGNATURES = [
     ("ctrecon_geometry_sizing", None, [ctypes.c_double] * 4 + [ctypes.c_int] * 2 + [_dp] * 3),
     ("ctrecon_phantom_project_dev", _st, [_vp, _vp, ctypes.POINTER(BPGeom), _dp, ctypes.c_int,
                                           ctypes.c_double, ctypes.c_uint64, _vp]),
+    ("ctrecon_rebin_to_panel_dev_f32", _st, [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int,
+                                             ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                             ctypes.c_double, _vp, _dp]),
+    ("ctrecon_rebin_to_panel_dev_f64", _st, [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int,
+                                             ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                             ctypes.c_double, _vp, _dp]),
     ("ctrecon_projfile_read", _st, [ctypes.c_char_p, ctypes.POINTER(ProjFileHeader), _dp,
                                     ctypes.c_size_t]),
     ("ctrecon_projfile_write", _st, [ctypes.c_char_p, ctypes.POINTER(ProjFileHeader), _dp]),

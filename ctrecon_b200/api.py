@@ -203,6 +203,13 @@ class Context:
                                            _tptr(d_proj, "float32", "d_proj"),
                                            _tptr(d_fproj, "float32", "d_fproj")), self._h)
 
+    def filter_mode1_dev(self, p: FilterParams, d_proj, d_fproj, stream=None):
+        """FilteringMode 1 (FunctionKat_v6.m:86-90): mean of the filters with FilterCoeFF and
+        1 - FilterCoeFF."""
+        check(lib().ctrecon_filter_mode1_dev_f32(self._h, _stream_handle(stream), ctypes.byref(p),
+                                                 _tptr(d_proj, "float32", "d_proj"),
+                                                 _tptr(d_fproj, "float32", "d_fproj")), self._h)
+
     @staticmethod
     def pi_table_bytes(geom) -> int:
         g = bp_geom(geom)
@@ -222,6 +229,21 @@ class Context:
                                            _tptr(d_fproj, "float32", "d_fproj"),
                                            _tptr(d_pitab, "", "d_pitab"),
                                            _tptr(d_image, "float32", "d_image")), self._h)
+
+    # -- arc detector to flat panel (rebinToPanel.m) ------------------------------------------
+    def rebin_to_panel_dev(self, d_proj, det_center_idx: float, det_cell_width: float,
+                           sour_to_det: float, d_out, stream=None) -> float:
+        """d_proj, d_out: device tensors (prj_num, det_hei, det_num), float32 or float64 (the
+        latter reproduces the reference's arithmetic exactly). Returns the panel width."""
+        P, H, N = d_proj.shape
+        dt = str(d_proj.dtype).replace("torch.", "")
+        fn = {"float32": lib().ctrecon_rebin_to_panel_dev_f32,
+              "float64": lib().ctrecon_rebin_to_panel_dev_f64}[dt]
+        width = ctypes.c_double()
+        check(fn(self._h, _stream_handle(stream), _tptr(d_proj, dt, "d_proj"), N, H, P,
+                 float(det_center_idx), float(det_cell_width), float(sour_to_det),
+                 _tptr(d_out, dt, "d_out"), ctypes.byref(width)), self._h)
+        return width.value
 
     # -- autotuner -----------------------------------------------------------------------------
     def tune_bkproj(self, geom, d_fproj, d_image, d_pitab=None, stream=None) -> dict:

@@ -418,6 +418,37 @@ ctrecon_status ctrecon_filter_dev_f32(ctrecon_ctx* ctx, void* stream,
     API_END(ctx)
 }
 
+ctrecon_status ctrecon_filter_mode1_dev_f32(ctrecon_ctx* ctx, void* stream,
+                                            const ctrecon_filter_params* p, const float* d_proj,
+                                            float* d_fproj) {
+    if (!ctx) return CTRECON_ERR_INVALID_ARGUMENT;
+    API_BEGIN
+    if (!p || !d_proj || !d_fproj)
+        return finish(ctx, make_status(CTRECON_ERR_INVALID_ARGUMENT, "NULL argument"));
+    if ((const void*)d_proj == (const void*)d_fproj)
+        return finish(ctx, make_status(CTRECON_ERR_INVALID_ARGUMENT,
+                                       "device filter needs distinct input and output"));
+    cudaStream_t st = (cudaStream_t)stream;
+    ctrecon_filter_params p1 = *p;
+    p1.filter_coeff = 1.0 - p->filter_coeff;  // the second pass of FunctionKat_v6.m:88
+    Status s = use_device(ctx);
+    FilterPlan* plan0 = nullptr;
+    FilterPlan* plan1 = nullptr;
+    if (s.ok()) s = get_filter_plan(ctx, *p, &plan0);
+    if (s.ok()) s = get_filter_plan(ctx, p1, &plan1);
+    const size_t n = (size_t)p->proj_number * p->yl * p->zl;
+    if (s.ok()) s = ctx->ws_dual.ensure(n * sizeof(float), "FilteringMode 1 second result");
+    if (s.ok()) s = reset_device_flag(ctx, st);
+    if (s.ok())
+        s = launch_filter(ctx, st, *plan0, d_proj, 0, p->proj_number, d_fproj, 0, 0, p->proj_number);
+    if (s.ok())
+        s = launch_filter(ctx, st, *plan1, d_proj, 0, p->proj_number, ctx->ws_dual.as<float>(), 0,
+                          0, p->proj_number);
+    if (s.ok()) s = launch_average_into(st, d_fproj, ctx->ws_dual.as<float>(), n);
+    return finish(ctx, s);
+    API_END(ctx)
+}
+
 ctrecon_status ctrecon_pi_dev(ctrecon_ctx* ctx, void* stream, const ctrecon_bp_geom* g,
                               void* d_pitab, unsigned long long* d_updates) {
     if (!ctx) return CTRECON_ERR_INVALID_ARGUMENT;

@@ -206,6 +206,19 @@ Status launch_convert_f32_to_f64(cudaStream_t s, const float* in, double* out, s
     return Status::Ok();
 }
 
+// FilteringMode 1 (FunctionKat_v6.m:86-90): FProj = (FProj + FProj1) / 2, in place in `a`
+__global__ void k_average_into(float* __restrict__ a, const float* __restrict__ b, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x)
+        a[i] = (a[i] + b[i]) / 2.f;
+}
+Status launch_average_into(cudaStream_t s, float* a, const float* b, size_t n) {
+    if (n == 0) return Status::Ok();
+    k_average_into<<<grid_for(n), 256, 0, s>>>(a, b, n);
+    CTR_CUDA(cudaGetLastError());
+    return Status::Ok();
+}
+
 // implemented in hilbert_tc.cu
 Status launch_hilbert_tc(ctrecon_ctx* ctx, cudaStream_t s, FilterPlan& plan, const void* X,
                          int nviews, float* d_fproj_chunk, int mode);

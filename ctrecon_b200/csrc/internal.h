@@ -181,6 +181,8 @@ struct ctrecon_ctx {
     ctr::DevBuf ws_count;    // update counter
     ctr::DevBuf ws_a, ws_b, ws_c, ws_d;  // host-call staging (f64 in, f32, f32 out, f64 out)
     ctr::DevBuf ws_e;        // FP64 image of the host backprojection
+    ctr::DevBuf ws_panel;    // arc-to-flat rebin table
+    ctr::DevBuf ws_dual;     // second filter result of FilteringMode 1
     ctr::DevBuf ws_ell;      // phantom ellipsoids
     ctr::DevBuf ws_flag;     // device error word
     ctr::PinetState pinet;   // learned PI-line initialiser
@@ -210,6 +212,7 @@ Status launch_bkproj_f64out(ctrecon_ctx* ctx, cudaStream_t s, BPPlan& plan,
                             const float* d_fproj, const PiRecord* d_pitab, double* d_image);
 Status launch_convert_f64_to_f32(cudaStream_t s, const double* in, float* out, size_t n);
 Status launch_convert_f32_to_f64(cudaStream_t s, const float* in, double* out, size_t n);
+Status launch_average_into(cudaStream_t s, float* a, const float* b, size_t n);
 Status launch_phantom(cudaStream_t s, const BPGeom& g, const double* d_ell, int n_ell,
                       double photons, uint64_t seed, float* d_proj, float* d_max);
 }  // namespace ctr

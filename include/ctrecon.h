@@ -144,6 +144,13 @@ ctrecon_status ctrecon_filter_dev_f32(ctrecon_ctx* ctx, void* stream,
                                       const ctrecon_filter_params* p, const float* d_proj,
                                       float* d_fproj);
 
+/* FilteringMode 1 of the reference's driver (FunctionKat_v6.m:86-90): the average of the
+ * filters with FilterCoeFF and 1 - FilterCoeFF, (FProj + FProj1) / 2, into d_fproj. Holds a
+ * second filtered copy in the context (4 bytes per projection sample) while it runs. */
+ctrecon_status ctrecon_filter_mode1_dev_f32(ctrecon_ctx* ctx, void* stream,
+                                            const ctrecon_filter_params* p, const float* d_proj,
+                                            float* d_fproj);
+
 /* Bytes of the per-voxel PI-interval table written by ctrecon_pi_dev. */
 ctrecon_status ctrecon_pi_table_bytes(const ctrecon_bp_geom* g, size_t* bytes);
 
@@ -298,6 +305,25 @@ ctrecon_status ctrecon_phantom_project_dev(ctrecon_ctx* ctx, void* stream,
                                            const ctrecon_bp_geom* g, const double* ell,
                                            int n_ell, double photons, uint64_t seed,
                                            float* d_proj);
+
+/* ---- arc detector to flat panel (rebinToPanel.m:1-36) -------------------------------------
+ * Resamples projections from an arc detector (det_num columns of arc length det_cell_width at
+ * distance sour_to_det, centre index det_center_idx 0-based) onto a flat panel with the same
+ * column count and width 2 D tan(largest half fan) (returned in *det_width, may be NULL).
+ * d_proj / d_out: [prj_num][det_hei][det_num] (MATLAB det_num x det_hei x prj_num), distinct.
+ * The reference's edge rules are kept: columns it skips are 0, and a panel column whose fan
+ * angle falls exactly on an arc-cell centre is 0 as well (its weights use clamped indices).
+ * The FP64 variant reproduces the reference's arithmetic exactly; stream-ordered. */
+ctrecon_status ctrecon_rebin_to_panel_dev_f32(ctrecon_ctx* ctx, void* stream, const float* d_proj,
+                                              int det_num, int det_hei, int prj_num,
+                                              double det_center_idx, double det_cell_width,
+                                              double sour_to_det, float* d_out,
+                                              double* det_width);
+ctrecon_status ctrecon_rebin_to_panel_dev_f64(ctrecon_ctx* ctx, void* stream, const double* d_proj,
+                                              int det_num, int det_hei, int prj_num,
+                                              double det_center_idx, double det_cell_width,
+                                              double sour_to_det, double* d_out,
+                                              double* det_width);
 
 /* ---- the reference's data files (host only, no GPU) ---------------------------------------
  * ProjectionData.m:113-176 and ReconImage.m:60-117 store little-endian doubles: a header of

@@ -763,3 +763,36 @@ int orc_project_ellipsoids(const orc_bp_geom* g, const double* ell, int n_ell,
     free(rot);
     return 0;
 }
+
+/* rebinToPanel.m:1-36, line for line: the panel column ii (1-based) sits at fan angle
+ * atan((ii - (N+1)/2) * newW / D) (:14), i.e. at fractional arc index idx (:15); the two arc
+ * cells floor/ceil(idx) (:16-17) are clamped as at :18-29 (a column whose ceil is below 1 or
+ * whose floor is beyond N stays zero) and blended with the weights of :33, which use the
+ * clamped indices -- so an idx that is exactly a cell centre gives weight 0 to both cells. */
+double orc_rebin_to_panel(const double* proj, int det_num, int det_hei, int prj_num,
+                          double c, double w, double D, double* out) {
+    const double oneFanAngle = atan(w / 2 / D) * 2.0;                                /* :6 */
+    const double a1 = (c + 0.5) * oneFanAngle, a2 = (det_num - 1 - c + 0.5) * oneFanAngle;
+    const double largerAngle = a1 > a2 ? a1 : a2;                                   /* :7 */
+    const double detWidth = tan(largerAngle) * D * 2;                               /* :9 */
+    const double newW = detWidth / det_num;                                         /* :10 */
+    const size_t rows = (size_t)det_hei * prj_num;
+    for (size_t r = 0; r < rows; ++r)
+        for (int i = 0; i < det_num; ++i) out[r * det_num + i] = 0.0;               /* :11 */
+    for (int ii = 1; ii <= det_num; ++ii) {
+        const double fanAngle = atan((ii - (det_num + 1) / 2.0) * newW / D);         /* :15 */
+        const double idx = fanAngle / oneFanAngle + c + 1;                          /* :16 */
+        double lowIdx = floor(idx), higIdx = ceil(idx);
+        if (lowIdx < 1) lowIdx = 1;
+        if (higIdx < 1) continue;
+        if (lowIdx > det_num) continue;
+        if (higIdx > det_num) higIdx = det_num;
+        const double wl = higIdx - idx, wh = idx - lowIdx;
+        const int lo = (int)lowIdx - 1, hi = (int)higIdx - 1;
+        for (size_t r = 0; r < rows; ++r) {                                         /* :30-33 */
+            const double* src = proj + r * det_num;
+            out[r * det_num + ii - 1] = src[lo] * wl + src[hi] * wh;
+        }
+    }
+    return detWidth;
+}

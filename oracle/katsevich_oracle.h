@@ -110,6 +110,13 @@ int orc_pi_table(const orc_bp_geom* g, double* B, double* T, int* loop_begin,
 int orc_project_ellipsoids(const orc_bp_geom* g, const double* ell, int n_ell,
                            double* proj, int p_begin, int p_end, int nthreads);
 
+/* rebinToPanel.m:1-36: arc detector (det_num columns, centre index c 0-based, cell width w at
+ * source distance D) to a flat panel of the same column count; proj is [views][rows][det_num]
+ * (MATLAB det_num x det_hei x prj_num). Columns the reference skips stay 0. Returns the panel
+ * width detWidth. */
+double orc_rebin_to_panel(const double* proj, int det_num, int det_hei, int prj_num,
+                          double c, double w, double D, double* out);
+
 #ifdef __cplusplus
 }
 #endif

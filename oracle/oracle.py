@@ -231,3 +231,16 @@ def ref_bkproj(geom: dict, fproj: np.ndarray, image: np.ndarray):
     m.set_print(False)
     m.call([geom, fproj, image], nlhs=0)
     return image
+
+
+def rebin_to_panel(proj, c, w, D):
+    """rebinToPanel.m:1-36 on numpy (prj_num, det_hei, det_num); returns (out, detWidth)."""
+    proj = np.ascontiguousarray(proj, dtype=np.float64)
+    P, H, N = proj.shape
+    out = np.empty_like(proj)
+    L = lib()
+    L.orc_rebin_to_panel.restype = ctypes.c_double
+    L.orc_rebin_to_panel.argtypes = [_dp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                     ctypes.c_double, ctypes.c_double, ctypes.c_double, _dp]
+    width = L.orc_rebin_to_panel(_ptr(proj), N, H, P, c, w, D, _ptr(out))
+    return out, width
