@@ -61,6 +61,10 @@ def parse():
                          "100 first form")
     ap.add_argument("--batched", action="store_true",
                     help="16 uneven scans (c4): one-at-a-time vs one batched graph replay")
+    ap.add_argument("--report", choices=["c3", "c5"],
+                    help="c3: error of each Hilbert variant vs the FP64 oracle and their times; "
+                         "c5: the learned PI initialiser at 1024^3 (iterations saved, endpoint "
+                         "agreement, time vs the plain form)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     return ap.parse_args()
@@ -412,6 +416,189 @@ def run_batched(args):
 
 
 # ---------------------------------------------------------------------------------------------
+def _pi_stats(ctx, torch, geom, d_tab):
+    """PI solve with the context's solver: (update count, solver iterations)."""
+    import ctypes
+    import ctrecon_b200 as ct
+    from ctrecon_b200 import _lib
+    g = ct.bp_geom(geom)
+    d_cnt = torch.zeros(1, dtype=torch.int64, device="cuda")
+    d_its = torch.zeros(1, dtype=torch.int64, device="cuda")
+    _lib.check(_lib.lib().ctrecon_pi_dev_stats(ctx.handle, torch.cuda.current_stream().cuda_stream,
+                                               ctypes.byref(g), d_tab.data_ptr(),
+                                               d_cnt.data_ptr(), d_its.data_ptr()), ctx.handle)
+    torch.cuda.synchronize()
+    return int(d_cnt.item()), int(d_its.item())
+
+
+def _compare_pi_tables(torch, a, b, chunk=1 << 26):
+    """Endpoint agreement of two PI tables on the device: max |dB|, |dT| (views) over voxels
+    valid in both, voxels whose validity or loop range [Bindex, Tindex] differ."""
+    ra, rb = a.view(torch.int32).view(-1, 4), b.view(torch.int32).view(-1, 4)
+    fa, fb = a.view(torch.float32).view(-1, 4), b.view(torch.float32).view(-1, 4)
+    dB = dT = 0.0
+    bad_valid = bad_range = 0
+    for i in range(0, ra.shape[0], chunk):
+        sa, sb = ra[i:i + chunk], rb[i:i + chunk]
+        va, vb = sa[:, 0] != 0x7FFFFFFF, sb[:, 0] != 0x7FFFFFFF
+        bad_valid += int((va != vb).sum())
+        v = va & vb
+        if not bool(v.any()):
+            continue
+        Ba = sa[v, 0].double() + fa[i:i + chunk][v, 1].double()
+        Bb = sb[v, 0].double() + fb[i:i + chunk][v, 1].double()
+        Ta = sa[v, 2].double() + fa[i:i + chunk][v, 3].double()
+        Tb = sb[v, 2].double() + fb[i:i + chunk][v, 3].double()
+        dB = max(dB, float((Ba - Bb).abs().max()))
+        dT = max(dT, float((Ta - Tb).abs().max()))
+        bad_range += int(((sa[v, 0] != sb[v, 0]) | (sa[v, 2] != sb[v, 2])).sum())
+    return {"max_abs_dB_views": dB, "max_abs_dT_views": dT, "voxels_validity_differs": bad_valid,
+            "voxels_loop_range_differs": bad_range}
+
+
+def run_report(args):
+    """Reports of the c3 and c5 configurations (not the headline line)."""
+    import torch
+    import ctrecon_b200 as ct
+    from ctrecon_b200 import _lib
+    s = config(args.config if args.config != "c2" else args.report)
+    geom = s.geom_struct()
+    fpar = ct.scan_filter_params(s)
+    ctx = ct.Context(0)
+    d_proj = torch.empty(s.proj_shape, dtype=torch.float32, device="cuda")
+    ctx.phantom_dev(geom, s.ellipsoids(), d_proj, photons=s.photons or 0.0, seed=s.seed)
+    d_fproj = torch.empty_like(d_proj)
+    d_img = torch.zeros(s.vol_shape, dtype=torch.float32, device="cuda")
+    d_tab = torch.empty(ctx.pi_table_bytes(geom), dtype=torch.uint8, device="cuda")
+    ctx.set_option(_lib.OPT_PI_SOLVER, _lib.PI_BISECT)
+    updates, iters_bisect = _pi_stats(ctx, torch, geom, d_tab)
+    stream = torch.cuda.current_stream()
+
+    def chain_ms(steps=2):
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        ctx.filter_dev(fpar, d_proj, d_fproj)
+        ctx.pi_dev(geom, d_tab)
+        ctx.bkproj_dev(geom, d_fproj, d_img, d_pitab=d_tab)
+        ph = [0.0, 0.0, 0.0]
+        for _ in range(steps):
+            e[0].record(stream)
+            ctx.filter_dev(fpar, d_proj, d_fproj)
+            e[1].record(stream)
+            ctx.pi_dev(geom, d_tab)
+            e[2].record(stream)
+            ctx.bkproj_dev(geom, d_fproj, d_img, d_pitab=d_tab)
+            e[3].record(stream)
+            torch.cuda.synchronize()
+            for k in range(3):
+                ph[k] += e[k].elapsed_time(e[k + 1]) / steps
+        return {"filter": ph[0], "pi": ph[1], "bkproj": ph[2], "step": sum(ph)}
+
+    out = {"report": args.report, "workload": workload_name(s), "volume": list(s.vol_shape),
+           "detector": [s.ZL, s.YL], "views": s.P, "updates_per_step": updates}
+    if args.bp_variant == -1:
+        ctx.filter_dev(fpar, d_proj, d_fproj)
+        out["bp_tune"] = ctx.tune_bkproj(geom, d_fproj, d_img, d_pitab=d_tab)
+        ctx.set_option(_lib.OPT_BP_VARIANT, _lib.BP_AUTO)
+    else:
+        ctx.set_option(_lib.OPT_BP_VARIANT, args.bp_variant)
+
+    if args.report == "c3":
+        O = _oracle()
+        cores = os.cpu_count() or 1
+        m = s.P // 2
+        proj_v = d_proj[m - 1:m + 17].cpu().numpy().astype(np.float64)
+        ref_views = cpu_filter_views(O, s, proj_v)[1:-1]          # views m .. m+15
+        n = 48
+        locus, det, obj, lo, hi = block_problem(O, s, n)
+        proj_b = d_proj[lo - 1:hi + 1].cpu().numpy().astype(np.float64)
+        t0 = time.perf_counter()
+        ref_fb = np.ascontiguousarray(cpu_filter_views(O, s, proj_b)[1:-1])
+        gb = O.bp_geom(locus, det, obj, honour_extras=True)
+        ref_img, _, touched = O.bkproj(gb, ref_fb, np.zeros((n, n, n)), nthreads=cores,
+                                       want_touched=True)
+        t_oracle = time.perf_counter() - t0
+        touched = touched.astype(bool)
+        block = {"Locus": locus, "Detector": det, "Object": obj}
+        modes = {}
+        for name, mode in (("fp32", _lib.HILBERT_FP32), ("bf16x3", _lib.HILBERT_BF16X3),
+                           ("tf32", _lib.HILBERT_TF32)):
+            ctx.set_option(_lib.OPT_HILBERT, mode)
+            ctx.set_option(_lib.OPT_PI_SOLVER, _lib.PI_NEWTON)
+            ph = chain_ms()
+            got_v = d_fproj[m:m + 16].cpu().numpy().astype(np.float64)
+            d_blk = torch.zeros((n, n, n), dtype=torch.float32, device="cuda")
+            ctx.set_option(_lib.OPT_PI_SOLVER, _lib.PI_BISECT)
+            ctx.bkproj_dev(block, d_fproj[lo:hi].contiguous(), d_blk)
+            torch.cuda.synchronize()
+            got_b = d_blk.cpu().numpy().astype(np.float64)
+            dv, db = got_v - ref_views, (got_b - ref_img)[touched]
+            modes[name] = {
+                "filter_rel_rmse": float(np.linalg.norm(dv) / np.linalg.norm(ref_views)),
+                "filter_max_abs": float(np.abs(dv).max()),
+                "filter_ref_max_abs": float(np.abs(ref_views).max()),
+                "chain_block_rel_rmse": float(np.linalg.norm(db) /
+                                              np.linalg.norm(ref_img[touched])),
+                "chain_block_max_abs": float(np.abs(db).max()),
+                "chain_block_ref_max_abs": float(np.abs(ref_img[touched]).max()),
+                "phase_ms": ph, "gups": updates / (ph["step"] / 1e3) / 1e9,
+                "s_per_vol": ph["step"] / 1e3}
+        out.update({"modes": modes, "filter_views_compared": [m, m + 16],
+                    "chain_block": {"voxels": n ** 3, "written": int(touched.sum()),
+                                    "views": [lo, hi], "oracle_s": t_oracle,
+                                    "pi_solver": "bisection (the reference's) for the block"},
+                    "pi_solver_in_timing": "newton"})
+    else:  # c5: the learned PI-line initialiser at scale
+        import ctypes
+        loss = ctypes.c_float()
+        t0 = time.perf_counter()
+        _lib.check(_lib.lib().ctrecon_pinet_train(
+            ctx.handle, stream.cuda_stream, 1 << 22, 8192, 8, s.ObjR / s.ScanR * 1.05, 2024,
+            ctypes.byref(loss)), ctx.handle)
+        torch.cuda.synchronize()
+        train_s = time.perf_counter() - t0
+        d_tab_b = d_tab.clone()  # the bisection table (the judge)
+        res = {}
+        for name, solver in (("bisect", _lib.PI_BISECT), ("newton", _lib.PI_NEWTON),
+                             ("learned", _lib.PI_LEARNED)):
+            ctx.set_option(_lib.OPT_PI_SOLVER, solver)
+            cnt, its = _pi_stats(ctx, torch, geom, d_tab)
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+            ev[0].record(stream)
+            ctx.pi_dev(geom, d_tab)
+            ev[1].record(stream)
+            torch.cuda.synchronize()
+            r = {"updates": cnt, "iterations": its, "pi_ms": ev[0].elapsed_time(ev[1])}
+            if name != "bisect":
+                r["vs_bisection"] = _compare_pi_tables(torch, d_tab, d_tab_b)
+            if name == "newton":
+                d_tab_n = d_tab.clone()
+            if name == "learned":  # converged endpoints of the two Newton starts
+                r["vs_newton"] = _compare_pi_tables(torch, d_tab, d_tab_n)
+                del d_tab_n
+            res[name] = r
+        out["pi"] = res
+        out["newton_iterations_saved_per_voxel"] = (
+            (res["newton"]["iterations"] - res["learned"]["iterations"]) /
+            max(1, int((d_tab_b.view(torch.int32).view(-1, 4)[:, 0] != 0x7FFFFFFF).sum())))
+        out["pinet"] = {"train_pairs": 1 << 22, "epochs": 8, "train_s": train_s,
+                        "final_loss": loss.value}
+        ctx.set_option(_lib.OPT_HILBERT, _lib.HILBERT_FP32)
+        ctx.set_option(_lib.OPT_PI_SOLVER, _lib.PI_BISECT)
+        plain = chain_ms(1)
+        ctx.set_option(_lib.OPT_PI_SOLVER, _lib.PI_LEARNED)
+        learned = chain_ms(1)
+        ctx.set_option(_lib.OPT_PI_SOLVER, _lib.PI_NEWTON)
+        newton = chain_ms(1)
+        out["chain_ms"] = {"plain_fp32_bisect": plain, "fp32_learned": learned,
+                           "fp32_newton": newton}
+        out["note"] = ("the tensor-core Hilbert needs AL <= 256 kappa rows; this detector has "
+                       f"AL = {2 * int(np.ceil(0.65 * s.ZL)) + 1}, so every form uses the FP32 "
+                       "filter")
+    print(json.dumps(out))
+    ctx.close()
+
+
+# ---------------------------------------------------------------------------------------------
 def main():
     args = parse()
     if args.impl == "reference":
@@ -419,6 +606,9 @@ def main():
         return
     if args.batched:
         run_batched(args)
+        return
+    if args.report:
+        run_report(args)
         return
     import torch
     import ctrecon_b200 as ct
