@@ -582,18 +582,18 @@ def run_report(args):
             max(1, int((d_tab_b.view(torch.int32).view(-1, 4)[:, 0] != 0x7FFFFFFF).sum())))
         out["pinet"] = {"train_pairs": 1 << 22, "epochs": 8, "train_s": train_s,
                         "final_loss": loss.value}
-        ctx.set_option(_lib.OPT_HILBERT, _lib.HILBERT_FP32)
-        ctx.set_option(_lib.OPT_PI_SOLVER, _lib.PI_BISECT)
-        plain = chain_ms(1)
-        ctx.set_option(_lib.OPT_PI_SOLVER, _lib.PI_LEARNED)
-        learned = chain_ms(1)
-        ctx.set_option(_lib.OPT_PI_SOLVER, _lib.PI_NEWTON)
-        newton = chain_ms(1)
-        out["chain_ms"] = {"plain_fp32_bisect": plain, "fp32_learned": learned,
-                           "fp32_newton": newton}
-        out["note"] = ("the tensor-core Hilbert needs AL <= 256 kappa rows; this detector has "
-                       f"AL = {2 * int(np.ceil(0.65 * s.ZL)) + 1}, so every form uses the FP32 "
-                       "filter")
+        forms = {"plain_fp32_bisect": (_lib.HILBERT_FP32, _lib.PI_BISECT),
+                 "fp32_newton": (_lib.HILBERT_FP32, _lib.PI_NEWTON),
+                 "fp32_learned": (_lib.HILBERT_FP32, _lib.PI_LEARNED),
+                 "bf16x3_newton": (_lib.HILBERT_BF16X3, _lib.PI_NEWTON),
+                 "bf16x3_learned": (_lib.HILBERT_BF16X3, _lib.PI_LEARNED)}
+        out["chain_ms"] = {}
+        for name, (hil, pis) in forms.items():
+            ctx.set_option(_lib.OPT_HILBERT, hil)
+            ctx.set_option(_lib.OPT_PI_SOLVER, pis)
+            ph = chain_ms(1)
+            ph["gups"] = updates / (ph["step"] / 1e3) / 1e9
+            out["chain_ms"][name] = ph
     print(json.dumps(out))
     ctx.close()
 

@@ -38,6 +38,8 @@ constexpr int kM = 128;
 
 struct TcParams {
     int AL, YL, ZL, nviews, vpt, ntile, nk, ALt;  // ALt: odd row stride >= vpt * AL
+    int nh;       // N halves: 1, or 2 when one view's kappa rows exceed 256 (vpt = 1)
+    int bar_off;  // byte offset of the mbarriers (past the stages and the epilogue buffer)
     const BkEntry* bk;
     float* out;
     int* err;
@@ -153,7 +155,7 @@ k_hilbert_tc(const __grid_constant__ CUtensorMap tA0, const __grid_constant__ CU
     const int abytes = kM * 128;
     const int bbytes = p.ntile * 128;
     const int stage_bytes = PL * (abytes + bbytes);
-    uint64_t* full = (uint64_t*)(smem + S * stage_bytes);
+    uint64_t* full = (uint64_t*)(smem + p.bar_off);
     uint64_t* empty = full + S;
     uint64_t* done = empty + S;
     uint32_t* tslot = (uint32_t*)(done + 1);
@@ -161,7 +163,9 @@ k_hilbert_tc(const __grid_constant__ CUtensorMap tA0, const __grid_constant__ CU
     const int i0 = blockIdx.x * kM;
     const int vg0 = blockIdx.y * p.vpt;
     const int n0 = vg0 * p.AL;
-    const uint32_t ncols = tmem_cols_for(p.ntile);
+    // with two halves, half h accumulates in TMEM columns [256 h, 256 h + ntile)
+    const uint32_t ncols = p.nh == 2 ? 512u : tmem_cols_for(p.ntile);
+    const int nit = p.nk * p.nh;  // pipeline steps: (K block, half)
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < S; ++s) {
@@ -185,16 +189,17 @@ k_hilbert_tc(const __grid_constant__ CUtensorMap tA0, const __grid_constant__ CU
 
     if (warp == 0 && lane == 0) {
         // TMA producer
-        for (int kb = 0; kb < p.nk; ++kb) {
-            const int s = kb % S;
-            if (kb >= S && !mbar_wait(&empty[s], ((kb / S) - 1) & 1, p.err, 1)) break;
+        for (int it = 0; it < nit; ++it) {
+            const int s = it % S, kb = it / p.nh, hf = it % p.nh;
+            if (it >= S && !mbar_wait(&empty[s], ((it / S) - 1) & 1, p.err, 1)) break;
             uint8_t* st = smem + s * stage_bytes;
             mbar_expect_tx(&full[s], (uint32_t)stage_bytes);
             const int x = kb * (MODE == CTRECON_HILBERT_BF16X3 ? 64 : 32);
+            const int nb = n0 + hf * p.ntile;
             tma_load_2d(st, &tA0, &full[s], x, i0);
             if (PL == 2) tma_load_2d(st + abytes, &tA1, &full[s], x, i0);
-            tma_load_2d(st + PL * abytes, &tB0, &full[s], x, n0);
-            if (PL == 2) tma_load_2d(st + PL * abytes + bbytes, &tB1, &full[s], x, n0);
+            tma_load_2d(st + PL * abytes, &tB0, &full[s], x, nb);
+            if (PL == 2) tma_load_2d(st + PL * abytes + bbytes, &tB1, &full[s], x, nb);
         }
     } else if (warp == 1 && lane == 0) {
         // MMA issuer: c = F32; a, b = BF16 (1) or TF32 (2); both K-major; N, M
@@ -202,9 +207,10 @@ k_hilbert_tc(const __grid_constant__ CUtensorMap tA0, const __grid_constant__ CU
         const uint32_t idesc = (1u << 4) | (fmt << 7) | (fmt << 10) |
                                ((uint32_t)(p.ntile >> 3) << 17) | ((uint32_t)(kM >> 4) << 24);
         bool ok = true;
-        for (int kb = 0; kb < p.nk; ++kb) {
-            const int s = kb % S;
-            if (!mbar_wait(&full[s], (kb / S) & 1, p.err, 2)) { ok = false; break; }
+        for (int it = 0; it < nit; ++it) {
+            const int s = it % S, kb = it / p.nh, hf = it % p.nh;
+            const uint32_t td = tmem + (uint32_t)(hf * 256);
+            if (!mbar_wait(&full[s], (it / S) & 1, p.err, 2)) { ok = false; break; }
             tc_fence_after();
             const uint32_t a0 = smem_u32(smem + s * stage_bytes);
             const uint32_t a1 = a0 + abytes;
@@ -214,10 +220,10 @@ k_hilbert_tc(const __grid_constant__ CUtensorMap tA0, const __grid_constant__ CU
             for (int ks = 0; ks < 4; ++ks) {  // four MMAs of 32 bytes of K per 128-byte block
                 const uint32_t off = 32u * ks;
                 const uint32_t acc = (kb > 0 || ks > 0) ? 1u : 0u;
-                mma<MODE>(tmem, sw128_desc(a0 + off), sw128_desc(b0 + off), idesc, acc);
+                mma<MODE>(td, sw128_desc(a0 + off), sw128_desc(b0 + off), idesc, acc);
                 if (MODE == CTRECON_HILBERT_BF16X3) {
-                    mma<MODE>(tmem, sw128_desc(a0 + off), sw128_desc(b1 + off), idesc, 1u);
-                    mma<MODE>(tmem, sw128_desc(a1 + off), sw128_desc(b0 + off), idesc, 1u);
+                    mma<MODE>(td, sw128_desc(a0 + off), sw128_desc(b1 + off), idesc, 1u);
+                    mma<MODE>(td, sw128_desc(a1 + off), sw128_desc(b0 + off), idesc, 1u);
                 }
             }
             mma_commit(&empty[s]);
@@ -238,16 +244,21 @@ k_hilbert_tc(const __grid_constant__ CUtensorMap tA0, const __grid_constant__ CU
     const int i = i0 + q * 32 + lane;
     if (have) {
         const uint32_t lane_addr = tmem + ((uint32_t)(q * 32) << 16);
-        for (int vl = h; vl < nv; vl += 2) {
-            const int c0 = vl * p.AL;
-            int c = 0;
-            for (; c + 16 <= p.AL; c += 16) {
+        // (view, column range) pieces this warp moves: per view when the tile holds several
+        // views, per TMEM half when one view spans both halves
+        const int npiece = p.nh == 2 ? 2 : nv;
+        for (int pc = h; pc < npiece; pc += 2) {
+            const int c0 = p.nh == 2 ? pc * p.ntile : pc * p.AL;             // logical column
+            const int c1 = p.nh == 2 ? min(p.AL, c0 + p.ntile) : c0 + p.AL;
+            const int t0 = p.nh == 2 ? pc * 256 : c0;                        // TMEM column
+            int c = c0;
+            for (; c + 16 <= c1; c += 16) {
                 float r[16];
-                tmem_ld16(lane_addr + (uint32_t)(c0 + c), r);
+                tmem_ld16(lane_addr + (uint32_t)(t0 + c - c0), r);
 #pragma unroll
-                for (int k = 0; k < 16; ++k) trq[lane * p.ALt + c0 + c + k] = r[k];
+                for (int k = 0; k < 16; ++k) trq[lane * p.ALt + c + k] = r[k];
             }
-            for (; c < p.AL; ++c) trq[lane * p.ALt + c0 + c] = tmem_ld1(lane_addr + (uint32_t)(c0 + c));
+            for (; c < c1; ++c) trq[lane * p.ALt + c] = tmem_ld1(lane_addr + (uint32_t)(t0 + c - c0));
         }
     }
     __syncthreads();
@@ -361,19 +372,22 @@ static Status ensure_toeplitz(FilterPlan& plan, int mode, DevBuf& T0, DevBuf& T1
     return Status::Ok();
 }
 
-int hilbert_tc_views_per_tile(int AL) { return std::max(1, 256 / AL); }
+// Views per CTA tile: as many whole views' kappa rows as fit in N = 256; one view (in two
+// N-halves) when a view has more than 256 kappa rows.
+int hilbert_tc_views_per_tile(int AL) { return AL > 256 ? 1 : std::max(1, 256 / AL); }
 
 Status launch_hilbert_tc(ctrecon_ctx* ctx, cudaStream_t s, FilterPlan& plan, const void* X,
                          int nviews, float* d_fproj_chunk, int mode) {
     const int AL = plan.t.AL, YL = plan.t.YL, ZL = plan.t.ZL, YLp = plan.YLp;
-    if (AL > 256)
+    if (AL > 512)
         return make_status(CTRECON_ERR_UNSUPPORTED,
-                           "tensor-core Hilbert needs AL <= 256 kappa lines (ZL <= 196)");
+                           "tensor-core Hilbert needs AL <= 512 kappa lines (ZL <= 392)");
     CTR_TRY(ensure_toeplitz(plan, mode, plan.tcT0, plan.tcT1, plan.tc_mode));
     if (!ctx->ws_flag.ptr) return make_status(CTRECON_ERR_INTERNAL, "device error word not set up");
     const bool bf = (mode == CTRECON_HILBERT_BF16X3);
     const int vpt = hilbert_tc_views_per_tile(AL);
-    const int ntile = (vpt * AL + 15) / 16 * 16;
+    const int nh = AL > 256 ? 2 : 1;
+    const int ntile = nh == 2 ? ((AL + 1) / 2 + 15) / 16 * 16 : (vpt * AL + 15) / 16 * 16;
     const uint64_t rows = (uint64_t)nviews * AL;
     const uint32_t kin = bf ? 64 : 32;
     CUtensorMap tA0, tA1, tB0, tB1;
@@ -386,15 +400,18 @@ Status launch_hilbert_tc(ctrecon_ctx* ctx, cudaStream_t s, FilterPlan& plan, con
     p.AL = AL; p.YL = YL; p.ZL = ZL; p.nviews = nviews; p.vpt = vpt; p.ntile = ntile;
     p.nk = YLp / (int)kin;
     p.ALt = (vpt * AL) | 1;
+    p.nh = nh;
     p.bk = plan.bk.as<BkEntry>();
     p.out = d_fproj_chunk;
     p.err = ctx->ws_flag.as<int>();
     const int PL = bf ? 2 : 1, S = bf ? 2 : 4;
     const size_t stage = (size_t)PL * (kM * 128 + (size_t)ntile * 128);
     const size_t epi = (size_t)4 * 32 * p.ALt * sizeof(float);
-    const size_t smem = std::max(S * stage, epi) + 1024 + 256;
-    if ((size_t)S * stage < epi)
-        return make_status(CTRECON_ERR_INTERNAL, "epilogue buffer exceeds the stage memory");
+    // stages and the epilogue's transpose buffer share [0, bar_off); the mbarriers follow
+    p.bar_off = (int)((std::max(S * stage, epi) + 7) / 8 * 8);
+    const size_t smem = (size_t)p.bar_off + 256 + 1024;
+    if (smem > 227 * 1024)
+        return make_status(CTRECON_ERR_UNSUPPORTED, "tensor-core Hilbert tile exceeds shared memory");
     dim3 grid((YL + kM - 1) / kM, (nviews + vpt - 1) / vpt);
     if (bf) {
         CTR_CUDA(cudaFuncSetAttribute(k_hilbert_tc<CTRECON_HILBERT_BF16X3>,

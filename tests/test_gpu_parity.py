@@ -97,6 +97,27 @@ def test_filter_tensor_core_matches_oracle(torch_mod, tiny_case, c1_case, case, 
     assert err < bound
 
 
+@pytest.mark.parametrize("mode,bound", [("bf16x3", 5e-5), ("tf32", 5e-3)])
+@pytest.mark.parametrize("zl,yl", [(200, 96), (260, 64)])
+def test_filter_tensor_core_two_halves(torch_mod, oracle_mod, zl, yl, mode, bound):
+    """Detectors with more than 256 kappa rows per view (AL = 261, 339): the tensor-core
+    Hilbert splits a view's rows into two N-halves accumulated in TMEM columns [0, 256) and
+    [256, 512); must agree with the FP64 oracle like the one-half form."""
+    import ctrecon_b200 as ct
+    from ctrecon_b200.geometry import small_config
+    s = small_config(name="tall", YL=yl, ZL=zl, views_per_turn=120, turns=2.2, NX=24, NY=24,
+                     NZ=8)
+    O = oracle_mod
+    proj = O.project_ellipsoids(oracle_geom(O, s), s.ellipsoids())
+    ref = O.katsevich_filter(oracle_filter_params(O, s), proj)
+    m = ct.HILBERT_BF16X3 if mode == "bf16x3" else ct.HILBERT_TF32
+    with ct.Context(0, hilbert=m) as cx:
+        out = cx.filter_host(ct.scan_filter_params(s), proj)
+    err = rel_rmse(out, ref)
+    print(f"filter {zl}x{yl} (AL {2 * int(np.ceil(0.65 * zl)) + 1}) {mode}: rel RMSE {err:.3e}")
+    assert err < bound
+
+
 def test_chain_c1_bf16x3_matches_oracle(torch_mod, c1_case):
     import ctrecon_b200 as ct
     s = c1_case["s"]
