@@ -311,6 +311,11 @@ ctrecon_status ctrecon_set_option(ctrecon_ctx* ctx, ctrecon_option opt, int valu
         ctx->opt_bp_variant = value;
         break;
     case CTRECON_OPT_VERBOSE: ctx->opt_verbose = value; break;
+    case CTRECON_OPT_DERIVATIVE:
+        if (value != CTRECON_DERIV_DIRECT && value != CTRECON_DERIV_CHAIN)
+            return finish(ctx, make_status(CTRECON_ERR_INVALID_ARGUMENT, "bad derivative mode"));
+        ctx->opt_deriv = value;
+        break;
     default: return finish(ctx, make_status(CTRECON_ERR_INVALID_ARGUMENT, "unknown option"));
     }
     return finish(ctx, Status::Ok());
@@ -324,6 +329,7 @@ ctrecon_status ctrecon_get_option(const ctrecon_ctx* ctx, ctrecon_option opt, in
     case CTRECON_OPT_FILTER_CHUNK: *value = ctx->opt_filter_chunk; break;
     case CTRECON_OPT_BP_VARIANT: *value = ctx->opt_bp_variant; break;
     case CTRECON_OPT_VERBOSE: *value = ctx->opt_verbose; break;
+    case CTRECON_OPT_DERIVATIVE: *value = ctx->opt_deriv; break;
     default: return CTRECON_ERR_INVALID_ARGUMENT;
     }
     return CTRECON_OK;

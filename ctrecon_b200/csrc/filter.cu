@@ -19,6 +19,7 @@
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <vector>
 
 namespace ctr {
 
@@ -47,10 +48,13 @@ __device__ __forceinline__ void store_kappa(void* X, size_t idx, size_t plane, f
 // Block (T columns) x (RG row groups): thread (tx, ry) owns column j = blockIdx.x * T + tx and
 // computes the derivative rows k = ry, ry + RG, ... then the kappa rows a = ry, ry + RG, ...;
 // the RG groups keep RG independent row walks in flight per column.
+// dres != NULL selects the direct half-view derivative of KatsevichFiltering_T.m:50-101
+// (entries [sample][side], side 0 applied to the next view, side 1 to this one; dl = DeltaL).
 __global__ void k_deriv_rebin(const float* __restrict__ proj, int proj_view0, int P, int YL,
                               int ZL, int AL, int YLp, int vbeg,
                               const FwEntry* __restrict__ fw, const float2* __restrict__ cuy,
                               const float* __restrict__ zcv, float inv2dl,
+                              const DresEntry* __restrict__ dres, float dl,
                               void* __restrict__ X, size_t plane, int mode) {
     extern __shared__ float gf[];  // ZL x blockDim.x: the derivative of the block's columns
     const int T = blockDim.x, tx = threadIdx.x, ry = threadIdx.y, RG = blockDim.y;
@@ -58,7 +62,24 @@ __global__ void k_deriv_rebin(const float* __restrict__ proj, int proj_view0, in
     const int p = vbeg + blockIdx.y;
     const size_t xv = (size_t)blockIdx.y * AL * YLp;
     const bool real = j < YL;
-    if (real) {
+    if (real && dres) {
+        const size_t S = (size_t)YL * ZL;
+        const int pc = p > P - 2 ? P - 2 : p;  // the last view repeats its neighbour (:101)
+        const float* Pn = proj + (size_t)(pc + 1 - proj_view0) * S;
+        const float* Pc = proj + (size_t)(pc - proj_view0) * S;
+        for (int k = ry; k < ZL; k += RG) {
+            const DresEntry e1 = dres[((size_t)k * YL + j) * 2];
+            const DresEntry e2 = dres[((size_t)k * YL + j) * 2 + 1];
+            float g1 = e1.w[0] * Pn[e1.o[0]];
+            float g2 = e2.w[0] * Pc[e2.o[0]];
+#pragma unroll
+            for (int q = 1; q < 4; ++q) {
+                g1 = fmaf(e1.w[q], Pn[e1.o[q]], g1);
+                g2 = fmaf(e2.w[q], Pc[e2.o[q]], g2);
+            }
+            gf[k * T + tx] = (g1 - g2) / dl;
+        }
+    } else if (real) {
         const size_t S = (size_t)YL * ZL;
         // view derivative: views 0 and P-1 reuse the derivative of views 1 and P-2 (:58-59)
         const int pc = p < 1 ? 1 : (p > P - 2 ? P - 2 : p);
@@ -239,6 +260,23 @@ Status launch_filter(ctrecon_ctx* ctx, cudaStream_t s, FilterPlan& plan, const f
     // 4 bytes per kappa sample in every format (FP32, TF32, or BF16 hi + lo planes)
     CTR_TRY(ctx->ws_kappa.ensure((size_t)chunk * AL * YLp * sizeof(float), "filter kappa rows"));
     void* X = ctx->ws_kappa.ptr;
+    const DresEntry* dres = nullptr;  // DerMode 0 resampling entries
+    if (ctx->opt_deriv == CTRECON_DERIV_DIRECT) {
+        if (!plan.dres_ready) {
+            const size_t ns = (size_t)ZL * YL;
+            std::vector<DresEntry> h(ns * 2);
+            for (size_t e = 0; e < ns; ++e)
+                for (int side = 0; side < 2; ++side)
+                    for (int q = 0; q < 4; ++q) {
+                        h[e * 2 + side].o[q] = t.dres_off[side][e * 4 + q];
+                        h[e * 2 + side].w[q] = (float)t.dres_w[side][e * 4 + q];
+                    }
+            CTR_TRY(plan.dres.ensure(h.size() * sizeof(DresEntry), "DerMode 0 resampling table"));
+            CTR_TRY(upload_now(plan.dres.ptr, h.data(), h.size() * sizeof(DresEntry)));
+            plan.dres_ready = true;
+        }
+        dres = plan.dres.as<DresEntry>();
+    }
 
     // K1 launch shape: one thread per column, ZL floats of shared memory per thread
     int tj = 128;
@@ -267,7 +305,8 @@ Status launch_filter(ctrecon_ctx* ctx, cudaStream_t s, FilterPlan& plan, const f
         const size_t plane = (size_t)n * AL * YLp;
         k_deriv_rebin<<<g1, b1, smem1, s>>>(d_proj, proj_view0, P, YL, ZL, AL, YLp, c0,
                                             plan.fw.as<FwEntry>(), plan.cuy.as<float2>(),
-                                            plan.zcv.as<float>(), plan.inv2dl, X, plane, mode);
+                                            plan.zcv.as<float>(), plan.inv2dl, dres,
+                                            (float)t.DeltaL, X, plane, mode);
         CTR_CUDA(cudaGetLastError());
         float* out = d_fproj + (size_t)(c0 - out_view0) * YL * ZL;
         if (mode == CTRECON_HILBERT_FP32) {
@@ -313,7 +352,8 @@ Status launch_filter_fp32_preplaced(cudaStream_t s, const FilterTables& t, int Y
         const int n = std::min(chunk, P - c0);
         dim3 g1((YLp + tj - 1) / tj, n);
         k_deriv_rebin<<<g1, b1, smem1, s>>>(d_proj, 0, P, YL, ZL, AL, YLp, c0, fw, cuy, zcv,
-                                            inv2dl, kappa, 0, CTRECON_HILBERT_FP32);
+                                            inv2dl, nullptr, 0.f, kappa, 0,
+                                            CTRECON_HILBERT_FP32);
         CTR_CUDA(cudaGetLastError());
         dim3 g2((YL + kTileI - 1) / kTileI, n);
         k_hilbert_simt<<<g2, nthreads2, smem2, s>>>(kappa, AL, ALpad, YL, YLp, ZL, hpad, HOFF, bk,

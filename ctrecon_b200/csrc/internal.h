@@ -75,9 +75,17 @@ struct FilterTables {
     std::vector<double> cu;                 // u-derivative coefficient per column
     double cv = 0;                          // v-derivative coefficient 1/(2 dV D)
     std::vector<double> h;                  // Hilbert taps h[m + YL - 1]
+    // DerMode 0 derivative (KatsevichFiltering_T.m:50-94): per (row z, column y) the four
+    // clamped 0-based sample offsets z*YL + y and bilinear weights of the projection resampled
+    // for the source rotated by -dL/2 (index 0, applied to the next view) and +dL/2 (index 1)
+    std::vector<int> dres_off[2];           // [ZL*YL*4]
+    std::vector<double> dres_w[2];          // [ZL*YL*4]
 };
 // Builds the tables of KatsevichFiltering.m:40-153 and :191-287 on the host in FP64.
 Status build_filter_tables(const ctrecon_filter_params& p, FilterTables& t);
+
+// DerMode 0 sample of the direct derivative: four element offsets in one view and weights
+struct DresEntry { int o[4]; float w[4]; };
 
 // Device form of the tables for one parameter set.
 struct FilterPlan {
@@ -89,6 +97,9 @@ struct FilterPlan {
     // tensor-core Hilbert operands (Toeplitz hi/lo in BF16, or TF32), built on first use
     DevBuf tcT0, tcT1;
     int tc_mode = -1;
+    // DerMode 0 resampling entries (DresEntry per sample, two per (z, y)), built on first use
+    DevBuf dres;
+    bool dres_ready = false;
 };
 
 // ---- backprojection geometry ----------------------------------------------------------------
@@ -168,6 +179,7 @@ struct ctrecon_ctx {
     int opt_filter_chunk = 512;
     int opt_bp_variant = 2;  // second form, 8 slices x 8 views
     int opt_verbose = 0;
+    int opt_deriv = CTRECON_DERIV_CHAIN;
     cudaStream_t host_stream = nullptr;  // stream for the synchronous host calls
     cudaStream_t up_stream = nullptr;    // host -> device copies of the host calls
     cudaStream_t down_stream = nullptr;  // device -> host copies of the host calls

@@ -90,6 +90,15 @@ enum {
     CTRECON_PI_LEARNED = 2  /* Newton seeded by the trained PI-line network */
 };
 
+/* Derivative of the filter (CTRECON_OPT_DERIVATIVE). */
+enum {
+    CTRECON_DERIV_DIRECT = 0,  /* DerMode 0: KatsevichFiltering_T.m:50-101, the projections
+                                  resampled for the source rotated by -/+ dL/2 and differenced:
+                                  the derivative sits half a view later (its backprojection takes
+                                  ProjCtr - 0.5, FunctionKat_v6.m:102) */
+    CTRECON_DERIV_CHAIN = 1    /* DerMode 1: KatsevichFiltering.m:52-95, chain rule (default) */
+};
+
 typedef enum ctrecon_option {
     CTRECON_OPT_HILBERT = 1,          /* CTRECON_HILBERT_*; default FP32 */
     CTRECON_OPT_PI_SOLVER = 2,        /* CTRECON_PI_*; default BISECT */
@@ -101,7 +110,8 @@ typedef enum ctrecon_option {
                                          ring slots x producer warps) 4x2x1, 2x4x1, 4x2x2;
                                          8, 9 = the same with 4x2x3, 4x3x4; 100 = first
                                          form; CTRECON_BP_AUTO = the tuning table's choice */
-    CTRECON_OPT_VERBOSE = 5
+    CTRECON_OPT_VERBOSE = 5,
+    CTRECON_OPT_DERIVATIVE = 6        /* CTRECON_DERIV_*; default CHAIN (the MEX filter's) */
 } ctrecon_option;
 
 /* ---- context ---------------------------------------------------------------------- */

@@ -330,6 +330,48 @@ static void view_derivative(const orc_filter_params* fp, const orc_tables* t,
     }
 }
 
+/* The direct derivative of KatsevichFiltering_T.m:50-94 (DerMode 0 of FunctionKat_v6.m:95-102):
+ * the projections bilinearly resampled onto the detector coordinates of the source rotated by
+ * -dL/2 (GF1, :51-71) and +dL/2 (GF2, :73-93), then GF(p) = (GF1(p+1) - GF2(p)) / dL (:95-99),
+ * the last view repeating its neighbour (:101). Sample positions use one-based coordinates; the
+ * fractions come from the unclamped indices, the indices are clamped to the detector
+ * (CheckData.m). */
+static double resample_half(const orc_filter_params* fp, const orc_tables* t, const double* Pv,
+                            int j, int k, int sign) {
+    const int YL = t->YL, ZL = t->ZL;
+    const double D = fp->StdDis, h = t->DeltaL / 2;
+    const double Dzc = sign < 0 ? D / (D * cos(h) - t->y[j] * sin(h))
+                                : D / (D * cos(h) + t->y[j] * sin(h));
+    const double Uy = sign < 0 ? (t->y[j] * cos(h) + D * sin(h)) * Dzc
+                               : (t->y[j] * cos(h) - D * sin(h)) * Dzc;
+    const double ycor = Uy / t->DeltaU + t->HalfY1;
+    const double zcor = (Dzc * t->z[k]) / t->DeltaV + t->HalfZ1;
+    int YD = (int)floor(ycor), ZD = (int)floor(zcor);
+    int YU = YD + 1, ZU = ZD + 1;
+    const double alfa = ycor - YD, beta = zcor - ZD;
+    YD = YD < 1 ? 1 : (YD > YL ? YL : YD);
+    YU = YU < 1 ? 1 : (YU > YL ? YL : YU);
+    ZD = ZD < 1 ? 1 : (ZD > ZL ? ZL : ZD);
+    ZU = ZU < 1 ? 1 : (ZU > ZL ? ZL : ZU);
+#define P1(yy, zz) Pv[(size_t)((zz) - 1) * YL + ((yy) - 1)]
+    return P1(YD, ZD) * (1 - alfa) * (1 - beta) + P1(YD, ZU) * (1 - alfa) * beta +
+           P1(YU, ZD) * alfa * (1 - beta) + P1(YU, ZU) * alfa * beta;
+#undef P1
+}
+
+static void view_derivative_direct(const orc_filter_params* fp, const orc_tables* t,
+                                   const double* Proj, int p, double* GF) {
+    const int YL = t->YL, ZL = t->ZL, P = t->P;
+    const size_t S = (size_t)YL * ZL;
+    const int pc = p == P - 1 ? P - 2 : p;
+    const double* Pn = Proj + (size_t)(pc + 1) * S;
+    const double* Pc = Proj + (size_t)pc * S;
+    for (int k = 0; k < ZL; ++k)
+        for (int j = 0; j < YL; ++j)
+            GF[(size_t)k * YL + j] = (resample_half(fp, t, Pn, j, k, -1) -
+                                      resample_half(fp, t, Pc, j, k, +1)) / t->DeltaL;
+}
+
 /* Step 2, forward height rebin + pre-weight (:131-153) into X[AL*YL]. */
 static void view_rebin(const orc_tables* t, const double* GF, double* X) {
     const int YL = t->YL;
@@ -397,6 +439,43 @@ int orc_filter(const orc_filter_params* fp, const double* Proj, double* FProj, i
         }
         free(GF); free(X); free(C);
     }
+    free_tables(&t);
+    return 0;
+}
+
+int orc_filter_direct(const orc_filter_params* fp, const double* Proj, double* FProj,
+                      int p_begin, int p_end, int nthreads) {
+    orc_tables t;
+    int rc = build_tables(fp, &t);
+    if (rc) return rc;
+    if (p_begin < 0) p_begin = 0;
+    if (p_end <= 0 || p_end > t.P) p_end = t.P;
+    set_threads(nthreads);
+    const size_t S = (size_t)t.YL * t.ZL, A = (size_t)t.AL * t.YL;
+#pragma omp parallel
+    {
+        double* GF = malloc(sizeof(double) * S);
+        double* X = malloc(sizeof(double) * A);
+        double* C = malloc(sizeof(double) * A);
+#pragma omp for schedule(dynamic, 1)
+        for (int p = p_begin; p < p_end; ++p) {
+            view_derivative_direct(fp, &t, Proj, p, GF);
+            view_rebin(&t, GF, X);
+            view_hilbert(&t, X, C);
+            view_backrebin(&t, C, FProj + (size_t)p * S);
+        }
+        free(GF); free(X); free(C);
+    }
+    free_tables(&t);
+    return 0;
+}
+
+int orc_derivative_direct(const orc_filter_params* fp, const double* Proj, int p, double* GF) {
+    orc_tables t;
+    int rc = build_tables(fp, &t);
+    if (rc) return rc;
+    if (p < 0 || p >= t.P || t.P < 2) { free_tables(&t); return -2; }
+    view_derivative_direct(fp, &t, Proj, p, GF);
     free_tables(&t);
     return 0;
 }

@@ -71,6 +71,11 @@ int orc_hilbert_taps(int YL, double* h);
  * derivative needs view neighbours). FProj gets the same views. nthreads <= 0: all. */
 int orc_filter(const orc_filter_params* fp, const double* Proj, double* FProj, int p_begin,
                int p_end, int nthreads);
+/* KatsevichFiltering_T.m (DerMode 0): the same filter with the direct half-view derivative. */
+int orc_filter_direct(const orc_filter_params* fp, const double* Proj, double* FProj,
+                      int p_begin, int p_end, int nthreads);
+/* Its derivative stage alone (KatsevichFiltering_T.m:50-101) for view p into GF[ZL*YL]. */
+int orc_derivative_direct(const orc_filter_params* fp, const double* Proj, int p, double* GF);
 
 /* Stage outputs for one view (for stage-level tests): GF (ZL*YL) after step 1,
  * ConvRes before the Hilbert (AL*YL, pre-weighted, index a*YL + y), and after the

@@ -54,6 +54,8 @@ def lib():
         L.orc_hilbert_taps.argtypes = [ctypes.c_int, _dp]
         L.orc_filter.argtypes = [ctypes.POINTER(FilterParams), _dp, _dp, ctypes.c_int,
                                  ctypes.c_int, ctypes.c_int]
+        L.orc_filter_direct.argtypes = [ctypes.POINTER(FilterParams), _dp, _dp, ctypes.c_int,
+                                        ctypes.c_int, ctypes.c_int]
         L.orc_filter_view_stages.argtypes = [ctypes.POINTER(FilterParams), _dp, ctypes.c_int,
                                              _dp, _dp, _dp]
         L.orc_pisegment.argtypes = [ctypes.c_double] * 3 + [_dp, _dp]
@@ -122,6 +124,28 @@ def hilbert_taps(YL) -> np.ndarray:
     h = np.zeros(2 * YL - 1)
     _check(lib().orc_hilbert_taps(YL, _ptr(h)), "orc_hilbert_taps")
     return h
+
+
+def katsevich_filter_direct(fp: FilterParams, proj: np.ndarray, p_begin=0, p_end=0,
+                            nthreads=0):
+    """KatsevichFiltering_T.m (DerMode 0: direct half-view derivative) -> FProj."""
+    proj = np.ascontiguousarray(proj, dtype=np.float64)
+    assert proj.shape == (fp.ProjNumber, fp.ZL, fp.YL)
+    out = np.zeros_like(proj)
+    _check(lib().orc_filter_direct(ctypes.byref(fp), _ptr(proj), _ptr(out), p_begin, p_end,
+                                   nthreads), "orc_filter_direct")
+    return out
+
+
+def derivative_direct(fp: FilterParams, proj: np.ndarray, p: int):
+    """KatsevichFiltering_T.m:50-101 for view p -> GF (ZL, YL)."""
+    proj = np.ascontiguousarray(proj, dtype=np.float64)
+    gf = np.zeros((fp.ZL, fp.YL))
+    L = lib()
+    L.orc_derivative_direct.argtypes = [ctypes.POINTER(FilterParams), _dp, ctypes.c_int, _dp]
+    _check(L.orc_derivative_direct(ctypes.byref(fp), _ptr(proj), p, _ptr(gf)),
+           "orc_derivative_direct")
+    return gf
 
 
 def katsevich_filter(fp: FilterParams, proj: np.ndarray, p_begin=0, p_end=0, nthreads=0):
