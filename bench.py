@@ -61,10 +61,11 @@ def parse():
                          "100 first form")
     ap.add_argument("--batched", action="store_true",
                     help="16 uneven scans (c4): one-at-a-time vs one batched graph replay")
-    ap.add_argument("--report", choices=["c3", "c5"],
+    ap.add_argument("--report", choices=["c3", "c5", "extras"],
                     help="c3: error of each Hilbert variant vs the FP64 oracle and their times; "
                          "c5: the learned PI initialiser at 1024^3 (iterations saved, endpoint "
-                         "agreement, time vs the plain form)")
+                         "agreement, time vs the plain form); extras: the panel rebin, "
+                         "DerMode 0, FilteringMode 1 and the file formats on the c2 scan")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     return ap.parse_args()
@@ -456,12 +457,92 @@ def _compare_pi_tables(torch, a, b, chunk=1 << 26):
             "voxels_loop_range_differs": bad_range}
 
 
-def run_report(args):
-    """Reports of the c3 and c5 configurations (not the headline line)."""
+def run_report_extras(args):
+    """The rows next to the path on the c2 scan: arc-to-flat panel rebin (HBM roofline),
+    DerMode 0 and FilteringMode 1 filters against the chain-rule filter, file read/write."""
     import torch
     import ctrecon_b200 as ct
     from ctrecon_b200 import _lib
-    s = config(args.config if args.config != "c2" else args.report)
+    from ctrecon_b200.formats import ProjectionData
+    s = config(args.config)
+    geom = s.geom_struct()
+    fpar = ct.scan_filter_params(s)
+    ctx = ct.Context(0)
+    d_proj = torch.empty(s.proj_shape, dtype=torch.float32, device="cuda")
+    ctx.phantom_dev(geom, s.ellipsoids(), d_proj, photons=s.photons or 0.0, seed=s.seed)
+    d_out = torch.empty_like(d_proj)
+    peak, peak_kind = load_peaks()
+    stream = torch.cuda.current_stream()
+
+    def timed(fn, reps=5):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    out = {"report": "extras", "workload": workload_name(s)}
+    n = d_proj.numel()
+    # panel rebin: arc detector of the same size (pitch = arc length 0.8 mm at D)
+    c_idx = (s.YL - 1) / 2 + 0.25
+    rb = {}
+    for name, t in (("f32", d_proj), ("f64", d_proj.double())):
+        o = torch.empty_like(t)
+        ms = timed(lambda: ctx.rebin_to_panel_dev(t, c_idx, 0.8, s.StdDis, o))
+        b = 2 * n * t.element_size()  # one read and one write of each sample
+        rb[name] = {"ms": ms, "bytes": b, "achieved_gbs": b / ms / 1e6,
+                    "frac_of_hbm": b / ms / 1e6 / peak}
+        del o
+    out["panel_rebin"] = dict(rb, peak_gbs=peak, peak_source=peak_kind,
+                              model="one read + one write per sample")
+    # filters
+    flt = {}
+    for name, hil in (("fp32", _lib.HILBERT_FP32), ("bf16x3", _lib.HILBERT_BF16X3)):
+        ctx.set_option(_lib.OPT_HILBERT, hil)
+        ctx.set_option(_lib.OPT_DERIVATIVE, _lib.DERIV_CHAIN)
+        chain = timed(lambda: ctx.filter_dev(fpar, d_proj, d_out), 3)
+        mode1 = timed(lambda: ctx.filter_mode1_dev(fpar, d_proj, d_out), 3)
+        ctx.set_option(_lib.OPT_DERIVATIVE, _lib.DERIV_DIRECT)
+        direct = timed(lambda: ctx.filter_dev(fpar, d_proj, d_out), 3)
+        ctx.set_option(_lib.OPT_DERIVATIVE, _lib.DERIV_CHAIN)
+        flt[name] = {"chain_rule_ms": chain, "dermode0_ms": direct, "filtering_mode1_ms": mode1}
+    out["filter"] = flt
+    # files (host): one c2 projection file, 3.5 GB of doubles
+    h = ProjectionData(source_to_center=s.ScanR, source_to_detector=s.StdDis, det_reso_u=s.YL,
+                       det_reso_v=s.ZL, det_pixel_u=0.8, det_pixel_v=0.8,
+                       det_center_u=(s.YL - 1) / 2, det_center_v=(s.ZL - 1) / 2, is_arc=False,
+                       total_views=s.P, views_per_turn=s.views_per_turn,
+                       projection=d_proj.cpu().numpy().astype(np.float64))
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "c2.prj")
+        t0 = time.perf_counter()
+        h.write(path)
+        tw = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        q = ProjectionData.read(path)
+        tr = time.perf_counter() - t0
+        size = os.path.getsize(path)
+        ok = bool(np.array_equal(q.projection, h.projection))
+    out["projection_file"] = {"bytes": size, "write_gbs": size / tw / 1e9,
+                              "read_gbs": size / tr / 1e9, "round_trip_equal": ok,
+                              "note": "page-cache bound (tmpfs or disk of the host)"}
+    print(json.dumps(out))
+    ctx.close()
+
+
+def run_report(args):
+    """Reports of the c3 and c5 configurations (not the headline line)."""
+    if args.report == "extras":
+        run_report_extras(args)
+        return
+    import torch
+    import ctrecon_b200 as ct
+    from ctrecon_b200 import _lib
+    s = config(args.config if args.config != "c2" else args.report)  # c3 / c5 by default
     geom = s.geom_struct()
     fpar = ct.scan_filter_params(s)
     ctx = ct.Context(0)

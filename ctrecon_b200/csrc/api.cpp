@@ -667,6 +667,73 @@ ctrecon_status ctrecon_filter_host_f64(ctrecon_ctx* ctx, const ctrecon_filter_pa
     API_END(ctx)
 }
 
+// KatsevichBkProj with FProj from host memory, with the transfer overlapping the work: the
+// image goes up first, the PI solve runs meanwhile, the valid voxels are zeroed, then the views
+// go up in windows of about 2048 and each window is backprojected (accumulating) as soon as it
+// is resident; the image comes down at the end. Summing per window reorders the FP32 sums of a
+// voxel (the windows' partial sums are added in FP64).
+static Status host_bkproj_windowed(ctrecon_ctx* ctx, BPPlan& plan, const double* fproj,
+                                   double* image) {
+    cudaStream_t up = ctx->up_stream, comp = ctx->host_stream, side = ctx->down_stream;
+    const int P = plan.g.ProjNum;
+    const size_t S = (size_t)plan.g.YL * plan.g.ZL, n = S * P;
+    const size_t nvox = (size_t)plan.kp.NX * plan.kp.NY * plan.kp.NZ;
+    CTR_TRY(ctx->ws_a.ensure(n * sizeof(double), "FP64 staging"));
+    CTR_TRY(ctx->ws_c.ensure(n * sizeof(float), "filtered projections"));
+    CTR_TRY(ctx->ws_pitab.ensure(nvox * sizeof(PiRecord), "PI table"));
+    CTR_TRY(ctx->ws_e.ensure(nvox * sizeof(double), "FP64 image"));
+    cudaEvent_t pi_done = nullptr, img_up = nullptr;
+    CTR_TRY(event_at(ctx, 0, &pi_done));
+    CTR_TRY(event_at(ctx, 1, &img_up));
+    CTR_TRY(launch_pi(ctx, side, plan, ctx->ws_pitab.as<PiRecord>(), nullptr));
+    CTR_CUDA(cudaEventRecord(pi_done, side));
+    CTR_CUDA(cudaMemcpyAsync(ctx->ws_e.ptr, image, nvox * sizeof(double), cudaMemcpyHostToDevice, up));
+    CTR_CUDA(cudaEventRecord(img_up, up));
+    CTR_CUDA(cudaStreamWaitEvent(comp, pi_done, 0));
+    CTR_CUDA(cudaStreamWaitEvent(comp, img_up, 0));
+    CTR_TRY(launch_zero_valid_f64(comp, ctx->ws_pitab.as<PiRecord>(), ctx->ws_e.as<double>(), nvox));
+    // windows: whole upload chunks, about 2048 views each
+    const int per_win = std::max(kHostChunkViews, (2048 / kHostChunkViews) * kHostChunkViews);
+    const BPParams saved = plan.kp;
+    Status st;
+    int w = 0;
+    for (int v0 = 0; st.ok() && v0 < P; v0 += per_win, ++w) {
+        const int v1 = std::min(P, v0 + per_win);
+        for (int c0 = v0; st.ok() && c0 < v1; c0 += kHostChunkViews) {
+            const size_t m = (size_t)(std::min(v1, c0 + kHostChunkViews) - c0) * S;
+            cudaError_t e = cudaMemcpyAsync(ctx->ws_a.as<double>() + (size_t)c0 * S,
+                                            fproj + (size_t)c0 * S, m * sizeof(double),
+                                            cudaMemcpyHostToDevice, up);
+            if (e != cudaSuccess) st = cuda_status(e, "FProj upload");
+            if (st.ok())
+                st = launch_convert_f64_to_f32(up, ctx->ws_a.as<double>() + (size_t)c0 * S,
+                                               ctx->ws_c.as<float>() + (size_t)c0 * S, m);
+        }
+        cudaEvent_t ev = nullptr;
+        if (st.ok()) st = event_at(ctx, 2 + (size_t)w, &ev);
+        if (st.ok()) {
+            cudaError_t e = cudaEventRecord(ev, up);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(comp, ev, 0);
+            if (e != cudaSuccess) st = cuda_status(e, "window event");
+        }
+        if (st.ok()) {
+            plan.kp.win0 = v0;
+            plan.kp.win1 = v1 - 1;
+            plan.kp.accum = 1;
+            st = launch_bkproj_f64out(ctx, comp, plan, ctx->ws_c.as<float>(),
+                                      ctx->ws_pitab.as<PiRecord>(), ctx->ws_e.as<double>());
+            plan.kp = saved;
+        }
+    }
+    plan.kp = saved;
+    CTR_TRY(st);
+    CTR_CUDA(cudaMemcpyAsync(image, ctx->ws_e.ptr, nvox * sizeof(double), cudaMemcpyDeviceToHost, comp));
+    CTR_CUDA(cudaStreamSynchronize(comp));
+    CTR_CUDA(cudaStreamSynchronize(side));
+    CTR_CUDA(cudaStreamSynchronize(up));
+    return check_device_flag(ctx);
+}
+
 ctrecon_status ctrecon_bkproj_host_f64(ctrecon_ctx* ctx, const ctrecon_bp_geom* g,
                                        const double* fproj, double* image) {
     if (!ctx) return CTRECON_ERR_INVALID_ARGUMENT;
@@ -677,28 +744,7 @@ ctrecon_status ctrecon_bkproj_host_f64(ctrecon_ctx* ctx, const ctrecon_bp_geom* 
     BPPlan* plan = nullptr;
     if (s.ok()) s = get_bp_plan(ctx, *g, &plan);
     if (s.ok()) s = host_reset(ctx);
-    if (s.ok()) {
-        const size_t S = (size_t)plan->g.YL * plan->g.ZL, n = S * plan->g.ProjNum;
-        cudaStream_t up = ctx->up_stream;
-        s = ctx->ws_a.ensure(n * sizeof(double), "FP64 staging");
-        if (s.ok()) s = ctx->ws_c.ensure(n * sizeof(float), "filtered projections");
-        for (size_t v0 = 0; s.ok() && v0 < (size_t)plan->g.ProjNum; v0 += kHostChunkViews) {
-            const size_t m = std::min<size_t>(kHostChunkViews, plan->g.ProjNum - v0) * S;
-            cudaError_t e = cudaMemcpyAsync(ctx->ws_a.as<double>() + v0 * S, fproj + v0 * S,
-                                            m * sizeof(double), cudaMemcpyHostToDevice, up);
-            if (e != cudaSuccess) s = cuda_status(e, "FProj upload");
-            if (s.ok())
-                s = launch_convert_f64_to_f32(up, ctx->ws_a.as<double>() + v0 * S,
-                                              ctx->ws_c.as<float>() + v0 * S, m);
-        }
-        cudaEvent_t ready = nullptr;
-        if (s.ok()) s = event_at(ctx, 2, &ready);
-        if (s.ok()) {
-            cudaError_t e = cudaEventRecord(ready, up);
-            if (e != cudaSuccess) s = cuda_status(e, "cudaEventRecord");
-        }
-        if (s.ok()) s = host_bkproj_pipeline(ctx, *plan, ctx->ws_c.as<float>(), ready, image);
-    }
+    if (s.ok()) s = host_bkproj_windowed(ctx, *plan, fproj, image);
     return finish(ctx, s);
     API_END(ctx)
 }

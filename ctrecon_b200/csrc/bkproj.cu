@@ -70,8 +70,8 @@ k_bkproj(BPParams kp, const float* __restrict__ fproj, const PiRecord* __restric
         zv[k] = (z < NZ) ? zc[z] : 0.f;
         acc[k] = 0.f;
         if (r.bi != kPiInvalid) {
-            tmin = min(tmin, max(1, r.bi));
-            tmax = max(tmax, min(r.ti + 1, P - 2));
+            tmin = min(tmin, max(max(1, r.bi), kp.win0));
+            tmax = max(tmax, min(min(r.ti + 1, P - 2), kp.win1));
         }
     }
     // warp and CTA view ranges
@@ -209,7 +209,11 @@ k_bkproj(BPParams kp, const float* __restrict__ fproj, const PiRecord* __restric
 #pragma unroll
     for (int k = 0; k < kTZ; ++k) {
         const int z = zb + k;
-        if (z < NZ && bi[k] != kPiInvalid) image[colbase + z] = (OutT)(-acc[k] * kp.invPs);
+        if (z < NZ && bi[k] != kPiInvalid) {
+            OutT* o = image + colbase + z;
+            const OutT v = (OutT)(-acc[k] * kp.invPs);
+            *o = kp.accum ? *o + v : v;
+        }
     }
 }
 
@@ -223,6 +227,22 @@ static Status launch_bk(cudaStream_t s, BPPlan& plan, const float* d_fproj,
                                   (int)smem));
     k_bkproj<OutT><<<grid, 256, smem, s>>>(kp, d_fproj, d_pitab, plan.views.as<float4>(),
                                            plan.xyz.as<float>(), d_image);
+    CTR_CUDA(cudaGetLastError());
+    return Status::Ok();
+}
+
+// Valid voxels (those with a PI interval) set to 0 before view-window accumulation.
+__global__ void k_zero_valid(const PiRecord* __restrict__ pit, double* __restrict__ image,
+                             size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x)
+        if (pit[i].bi != kPiInvalid) image[i] = 0.0;
+}
+
+Status launch_zero_valid_f64(cudaStream_t s, const PiRecord* d_pitab, double* d_image, size_t n) {
+    if (n == 0) return Status::Ok();
+    const unsigned grid = (unsigned)std::min<size_t>((n + 255) / 256, 148 * 32);
+    k_zero_valid<<<grid, 256, 0, s>>>(d_pitab, d_image, n);
     CTR_CUDA(cudaGetLastError());
     return Status::Ok();
 }

@@ -84,8 +84,8 @@ __device__ __forceinline__ void bp_tile(const BPParams& kp, const float* __restr
         bi[k] = r.bi; bf[k] = r.bf; ti[k] = r.ti; tf[k] = r.tf;
         acc[k] = 0.f;
         if (r.bi != kPiInvalid) {
-            tmin = min(tmin, max(1, r.bi));
-            tmax = max(tmax, min(r.ti + 1, P - 2));
+            tmin = min(tmin, max(max(1, r.bi), kp.win0));
+            tmax = max(tmax, min(min(r.ti + 1, P - 2), kp.win1));
             flo = max(flo, r.bi + 2);  // views past both B-side ramp views
             fhi = min(fhi, r.ti - 1);  // views before both T-side ramp views
         } else {
@@ -260,7 +260,11 @@ __device__ __forceinline__ void bp_tile(const BPParams& kp, const float* __restr
 #pragma unroll
     for (int k = 0; k < TZ; ++k) {
         const int z = zb + k;
-        if (z < NZ && bi[k] != kPiInvalid) image[colbase + z] = (OutT)(-acc[k] * kp.invPs);
+        if (z < NZ && bi[k] != kPiInvalid) {
+            OutT* o = image + colbase + z;
+            const OutT v = (OutT)(-acc[k] * kp.invPs);
+            *o = kp.accum ? *o + v : v;
+        }
     }
 }
 

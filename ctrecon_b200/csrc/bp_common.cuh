@@ -60,10 +60,11 @@ struct VoxelRanges {
     bool all_valid;  // every voxel has a PI interval (and the column is in the volume)
 };
 
+// loop ranges clamped to the view window [win0, win1] (BPParams)
 template <int TZ>
 __device__ __forceinline__ void load_ranges(const PiRecord* __restrict__ pit, size_t colbase,
-                                            int zb, int NZ, int P, bool col_ok,
-                                            VoxelRanges<TZ>& r) {
+                                            int zb, int NZ, int P, bool col_ok, int win0,
+                                            int win1, VoxelRanges<TZ>& r) {
     r.tmin = INT_MAX; r.tmax = INT_MIN; r.flo = INT_MIN; r.fhi = INT_MAX;
     r.all_valid = col_ok;
 #pragma unroll
@@ -74,8 +75,8 @@ __device__ __forceinline__ void load_ranges(const PiRecord* __restrict__ pit, si
         r.bi[k] = q.bi; r.bf[k] = q.bf; r.ti[k] = q.ti; r.tf[k] = q.tf;
         if (q.bi != kPiInvalid) {
             // loop range of KatsevichBkProj.cpp:180-181: [max(1,Bindex), min(Tindex,P-2)]
-            r.tmin = min(r.tmin, max(1, q.bi));
-            r.tmax = max(r.tmax, min(q.ti + 1, P - 2));
+            r.tmin = min(r.tmin, max(max(1, q.bi), win0));
+            r.tmax = max(r.tmax, min(min(q.ti + 1, P - 2), win1));
             r.flo = max(r.flo, q.bi + 2);  // views past both B-side ramp views
             r.fhi = min(r.fhi, q.ti - 1);  // views before both T-side ramp views
         } else {
@@ -94,6 +95,12 @@ __device__ __forceinline__ float voxel_weight(const VoxelRanges<TZ>& r, int k, i
     if (d1 <= 1) return ramp(r.tf[k] + (float)(d1 - 1));
     if (d0 <= 1) return ramp((float)d0 - r.bf[k]);
     return 1.f;
+}
+
+// the voxel's result: assigned, or added in view-window accumulation
+template <typename OutT>
+__device__ __forceinline__ void store_voxel(OutT* o, float v, int accum) {
+    *o = accum ? *o + (OutT)v : (OutT)v;
 }
 
 }  // namespace bp

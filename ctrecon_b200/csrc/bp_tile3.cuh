@@ -79,7 +79,7 @@ __device__ __forceinline__ void tile3(const BPParams& kp, const float* __restric
     if (tid == 0) { sh.s_pmin = INT_MAX; sh.s_pmax = INT_MIN; }
     VoxelRanges<TZ> vr;
     const size_t colbase = ((size_t)x * NY + y) * NZ;
-    load_ranges<TZ>(pit, colbase, zb, NZ, P, col_ok, vr);
+    load_ranges<TZ>(pit, colbase, zb, NZ, P, col_ok, kp.win0, kp.win1, vr);
     float acc[TZ];
 #pragma unroll
     for (int k = 0; k < TZ; ++k) acc[k] = 0.f;
@@ -289,7 +289,7 @@ __device__ __forceinline__ void tile3(const BPParams& kp, const float* __restric
 #pragma unroll
     for (int k = 0; k < TZ; ++k) {
         const int z = zb + k;
-        if (z < NZ && vr.bi[k] != kPiInvalid) image[colbase + z] = (OutT)(-acc[k] * kp.invPs);
+        if (z < NZ && vr.bi[k] != kPiInvalid) store_voxel(image + colbase + z, -acc[k] * kp.invPs, kp.accum);
     }
 }
 

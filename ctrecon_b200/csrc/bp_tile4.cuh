@@ -98,7 +98,7 @@ __device__ __forceinline__ uint32_t tile4(const BPParams& kp, const float* __res
     const bool col_ok = consumer && (x < NX) && (y < NY);
     const size_t colbase = ((size_t)x * NY + y) * NZ;
     VoxelRanges<TZ> vr;
-    load_ranges<TZ>(pit, colbase, zb, NZ, P, col_ok, vr);
+    load_ranges<TZ>(pit, colbase, zb, NZ, P, col_ok, kp.win0, kp.win1, vr);
     int wmin = vr.tmin, wmax = vr.tmax;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -343,7 +343,7 @@ __device__ __forceinline__ uint32_t tile4(const BPParams& kp, const float* __res
 #pragma unroll
         for (int k = 0; k < TZ; ++k) {
             const int z = zb + k;
-            if (z < NZ && vr.bi[k] != kPiInvalid) image[colbase + z] = (OutT)(-acc[k] * kp.invPs);
+            if (z < NZ && vr.bi[k] != kPiInvalid) store_voxel(image + colbase + z, -acc[k] * kp.invPs, kp.accum);
         }
     }
     __syncthreads();  // the caller may reuse the shared state for the next tile

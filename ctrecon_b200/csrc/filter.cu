@@ -49,12 +49,14 @@ __device__ __forceinline__ void store_kappa(void* X, size_t idx, size_t plane, f
 // computes the derivative rows k = ry, ry + RG, ... then the kappa rows a = ry, ry + RG, ...;
 // the RG groups keep RG independent row walks in flight per column.
 // dres != NULL selects the direct half-view derivative of KatsevichFiltering_T.m:50-101
-// (entries [sample][side], side 0 applied to the next view, side 1 to this one; dl = DeltaL).
+// (entries [column][side], side 0 applied to the next view, side 1 to this one; dl = DeltaL):
+// the resampled row position (k + 1 - HalfZ) * Dzc + HalfZ is formed here in FP32, the column
+// position comes from the FP64 host table; indices clamped as CheckData.m.
 __global__ void k_deriv_rebin(const float* __restrict__ proj, int proj_view0, int P, int YL,
                               int ZL, int AL, int YLp, int vbeg,
                               const FwEntry* __restrict__ fw, const float2* __restrict__ cuy,
                               const float* __restrict__ zcv, float inv2dl,
-                              const DresEntry* __restrict__ dres, float dl,
+                              const DresCol* __restrict__ dres, float dl,
                               void* __restrict__ X, size_t plane, int mode) {
     extern __shared__ float gf[];  // ZL x blockDim.x: the derivative of the block's columns
     const int T = blockDim.x, tx = threadIdx.x, ry = threadIdx.y, RG = blockDim.y;
@@ -67,18 +69,21 @@ __global__ void k_deriv_rebin(const float* __restrict__ proj, int proj_view0, in
         const int pc = p > P - 2 ? P - 2 : p;  // the last view repeats its neighbour (:101)
         const float* Pn = proj + (size_t)(pc + 1 - proj_view0) * S;
         const float* Pc = proj + (size_t)(pc - proj_view0) * S;
-        for (int k = ry; k < ZL; k += RG) {
-            const DresEntry e1 = dres[((size_t)k * YL + j) * 2];
-            const DresEntry e2 = dres[((size_t)k * YL + j) * 2 + 1];
-            float g1 = e1.w[0] * Pn[e1.o[0]];
-            float g2 = e2.w[0] * Pc[e2.o[0]];
-#pragma unroll
-            for (int q = 1; q < 4; ++q) {
-                g1 = fmaf(e1.w[q], Pn[e1.o[q]], g1);
-                g2 = fmaf(e2.w[q], Pc[e2.o[q]], g2);
-            }
-            gf[k * T + tx] = (g1 - g2) / dl;
-        }
+        const DresCol c1 = dres[(size_t)j * 2], c2 = dres[(size_t)j * 2 + 1];
+        const float hz = 0.5f * (float)(ZL + 1);
+        auto sample = [&](const float* Pv, const DresCol& c, int k) {
+            const float zc = fmaf(c.dzc, (float)(k + 1) - hz, hz);
+            const float fz = floorf(zc);
+            const float b = zc - fz, a = c.alfa;
+            const int iz = (int)fz;
+            const int ZD = min(max(iz, 1), ZL) - 1, ZU = min(max(iz + 1, 1), ZL) - 1;
+            const float* rd = Pv + (size_t)ZD * YL;
+            const float* ru = Pv + (size_t)ZU * YL;
+            return rd[c.yd] * (1.f - a) * (1.f - b) + ru[c.yd] * (1.f - a) * b +
+                   rd[c.yu] * a * (1.f - b) + ru[c.yu] * a * b;
+        };
+        for (int k = ry; k < ZL; k += RG)
+            gf[k * T + tx] = (sample(Pn, c1, k) - sample(Pc, c2, k)) / dl;
     } else if (real) {
         const size_t S = (size_t)YL * ZL;
         // view derivative: views 0 and P-1 reuse the derivative of views 1 and P-2 (:58-59)
@@ -260,22 +265,20 @@ Status launch_filter(ctrecon_ctx* ctx, cudaStream_t s, FilterPlan& plan, const f
     // 4 bytes per kappa sample in every format (FP32, TF32, or BF16 hi + lo planes)
     CTR_TRY(ctx->ws_kappa.ensure((size_t)chunk * AL * YLp * sizeof(float), "filter kappa rows"));
     void* X = ctx->ws_kappa.ptr;
-    const DresEntry* dres = nullptr;  // DerMode 0 resampling entries
+    const DresCol* dres = nullptr;  // DerMode 0 resampling columns
     if (ctx->opt_deriv == CTRECON_DERIV_DIRECT) {
         if (!plan.dres_ready) {
-            const size_t ns = (size_t)ZL * YL;
-            std::vector<DresEntry> h(ns * 2);
-            for (size_t e = 0; e < ns; ++e)
+            std::vector<DresCol> h((size_t)YL * 2);
+            for (int j = 0; j < YL; ++j)
                 for (int side = 0; side < 2; ++side)
-                    for (int q = 0; q < 4; ++q) {
-                        h[e * 2 + side].o[q] = t.dres_off[side][e * 4 + q];
-                        h[e * 2 + side].w[q] = (float)t.dres_w[side][e * 4 + q];
-                    }
-            CTR_TRY(plan.dres.ensure(h.size() * sizeof(DresEntry), "DerMode 0 resampling table"));
-            CTR_TRY(upload_now(plan.dres.ptr, h.data(), h.size() * sizeof(DresEntry)));
+                    h[(size_t)j * 2 + side] =
+                        DresCol{t.dres_yd[side][j], t.dres_yu[side][j],
+                                (float)t.dres_alfa[side][j], (float)t.dres_dzc[side][j]};
+            CTR_TRY(plan.dres.ensure(h.size() * sizeof(DresCol), "DerMode 0 resampling table"));
+            CTR_TRY(upload_now(plan.dres.ptr, h.data(), h.size() * sizeof(DresCol)));
             plan.dres_ready = true;
         }
-        dres = plan.dres.as<DresEntry>();
+        dres = plan.dres.as<DresCol>();
     }
 
     // K1 launch shape: one thread per column, ZL floats of shared memory per thread

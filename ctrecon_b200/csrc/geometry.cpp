@@ -184,33 +184,24 @@ Status build_filter_tables(const ctrecon_filter_params& p, FilterTables& t) {
     // detector coordinates; fractions from the unclamped indices, indices clamped (CheckData.m)
     {
         const double h2 = t.DeltaL / 2, D = p.std_dis;
+        auto clampi = [](double v, int hi) { return (int)(v < 1 ? 1 : (v > hi ? hi : v)) - 1; };
         for (int side = 0; side < 2; ++side) {
-            t.dres_off[side].assign((size_t)ZL * YL * 4, 0);
-            t.dres_w[side].assign((size_t)ZL * YL * 4, 0.0);
+            t.dres_yd[side].assign(YL, 0);
+            t.dres_yu[side].assign(YL, 0);
+            t.dres_alfa[side].assign(YL, 0.0);
+            t.dres_dzc[side].assign(YL, 0.0);
             for (int j = 0; j < YL; ++j) {
                 const double y = t.y[j];
                 const double Dzc = side == 0 ? D / (D * std::cos(h2) - y * std::sin(h2))
                                              : D / (D * std::cos(h2) + y * std::sin(h2));
                 const double Uy = side == 0 ? (y * std::cos(h2) + D * std::sin(h2)) * Dzc
                                             : (y * std::cos(h2) - D * std::sin(h2)) * Dzc;
-                for (int k = 0; k < ZL; ++k) {
-                    const double ycor = Uy / t.DeltaU + (YL + 1) / 2.0;
-                    const double zcor = (Dzc * t.z[k]) / t.DeltaV + (ZL + 1) / 2.0;
-                    const double fy = std::floor(ycor), fz = std::floor(zcor);
-                    const double a = ycor - fy, b = zcor - fz;
-                    auto clampi = [](double v, int hi) {
-                        return (int)(v < 1 ? 1 : (v > hi ? hi : v)) - 1;
-                    };
-                    const int YD = clampi(fy, YL), YU = clampi(fy + 1, YL);
-                    const int ZD = clampi(fz, ZL), ZU = clampi(fz + 1, ZL);
-                    const size_t e = ((size_t)k * YL + j) * 4;
-                    int* o = &t.dres_off[side][e];
-                    double* w = &t.dres_w[side][e];
-                    o[0] = ZD * YL + YD; w[0] = (1 - a) * (1 - b);
-                    o[1] = ZU * YL + YD; w[1] = (1 - a) * b;
-                    o[2] = ZD * YL + YU; w[2] = a * (1 - b);
-                    o[3] = ZU * YL + YU; w[3] = a * b;
-                }
+                const double ycor = Uy / t.DeltaU + (YL + 1) / 2.0;
+                const double fy = std::floor(ycor);
+                t.dres_yd[side][j] = clampi(fy, YL);
+                t.dres_yu[side][j] = clampi(fy + 1, YL);
+                t.dres_alfa[side][j] = ycor - fy;
+                t.dres_dzc[side][j] = Dzc;  // (Dzc * z) / DeltaV = Dzc * (k + 1 - HalfZ)
             }
         }
     }
@@ -298,6 +289,9 @@ BPParams make_bp_params(const BPGeom& g) {
     k.HalfZ = (float)g.HalfZ;
     k.invPs = (float)(1.0 / g.ProjScale);
     k.dzf = (float)g.dz;
+    k.win0 = 0;
+    k.win1 = g.ProjNum - 1;
+    k.accum = 0;
     return k;
 }
 

@@ -75,17 +75,18 @@ struct FilterTables {
     std::vector<double> cu;                 // u-derivative coefficient per column
     double cv = 0;                          // v-derivative coefficient 1/(2 dV D)
     std::vector<double> h;                  // Hilbert taps h[m + YL - 1]
-    // DerMode 0 derivative (KatsevichFiltering_T.m:50-94): per (row z, column y) the four
-    // clamped 0-based sample offsets z*YL + y and bilinear weights of the projection resampled
-    // for the source rotated by -dL/2 (index 0, applied to the next view) and +dL/2 (index 1)
-    std::vector<int> dres_off[2];           // [ZL*YL*4]
-    std::vector<double> dres_w[2];          // [ZL*YL*4]
+    // DerMode 0 derivative (KatsevichFiltering_T.m:50-94), for the source rotated by -dL/2
+    // (index 0, applied to the next view) and +dL/2 (index 1): per column the clamped 0-based
+    // columns YD, YU and fraction alfa of the resampled position, and its row scale Dzc (the
+    // row position is (k + 1 - HalfZ) * Dzc + HalfZ, one-based)
+    std::vector<int> dres_yd[2], dres_yu[2];  // [YL]
+    std::vector<double> dres_alfa[2], dres_dzc[2];
 };
 // Builds the tables of KatsevichFiltering.m:40-153 and :191-287 on the host in FP64.
 Status build_filter_tables(const ctrecon_filter_params& p, FilterTables& t);
 
-// DerMode 0 sample of the direct derivative: four element offsets in one view and weights
-struct DresEntry { int o[4]; float w[4]; };
+// DerMode 0 resampling of one column (one side): columns, fraction, row scale
+struct DresCol { int yd, yu; float alfa, dzc; };
 
 // Device form of the tables for one parameter set.
 struct FilterPlan {
@@ -97,7 +98,7 @@ struct FilterPlan {
     // tensor-core Hilbert operands (Toeplitz hi/lo in BF16, or TF32), built on first use
     DevBuf tcT0, tcT1;
     int tc_mode = -1;
-    // DerMode 0 resampling entries (DresEntry per sample, two per (z, y)), built on first use
+    // DerMode 0 resampling (DresCol per column and side, [column][side]), built on first use
     DevBuf dres;
     bool dres_ready = false;
 };
@@ -122,6 +123,10 @@ struct BPParams {
     double ScanR, HelicP, DeltaL, CtrMinusBeg, ObjR2;
     double XC, YC, ZC, dx, dy, dz;
     float Rf, DdU, DdV, HalfY, HalfZ, invPs, dzf;
+    // view window of the backprojection: only loop views in [win0, win1] are summed; accum = 1
+    // adds the window's sum to the image instead of assigning it (the full scan, assign, is the
+    // default from make_bp_params)
+    int win0, win1, accum;
 };
 BPParams make_bp_params(const BPGeom& g);
 
@@ -223,6 +228,7 @@ Status launch_bkproj_f32(ctrecon_ctx* ctx, cudaStream_t s, BPPlan& plan, const f
 Status launch_bkproj_f64out(ctrecon_ctx* ctx, cudaStream_t s, BPPlan& plan,
                             const float* d_fproj, const PiRecord* d_pitab, double* d_image);
 Status launch_convert_f64_to_f32(cudaStream_t s, const double* in, float* out, size_t n);
+Status launch_zero_valid_f64(cudaStream_t s, const PiRecord* d_pitab, double* d_image, size_t n);
 Status launch_convert_f32_to_f64(cudaStream_t s, const float* in, double* out, size_t n);
 Status launch_average_into(cudaStream_t s, float* a, const float* b, size_t n);
 Status launch_phantom(cudaStream_t s, const BPGeom& g, const double* d_ell, int n_ell,

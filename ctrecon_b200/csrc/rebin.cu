@@ -3,9 +3,10 @@
 // The host builds, in FP64, one entry per flat-panel column: the two arc columns around its
 // fan angle and their weights, with the reference's clamps (a column it skips gets no entry
 // and stays zero; a fan position exactly on a cell centre gets weight 0 on both cells, as the
-// reference's weights use the clamped indices). One thread per output element then blends two
-// input elements of its row: HBM-bound, 8 (FP32) or 16 (FP64) bytes read and 4 or 8 written per
-// element. The FP64 kernel multiplies and adds without contraction, in the reference's order.
+// reference's weights use the clamped indices). Blocks keep the table in shared memory and walk
+// detector rows, one thread per output column blending two input elements of its row:
+// HBM-bound, one read and one write per sample. The FP64 kernel multiplies and adds without
+// contraction, in the reference's order.
 #include "internal.h"
 
 #include <cmath>
@@ -41,22 +42,43 @@ double panel_table(int N, double c, double w, double D, std::vector<PanelEntry>&
     return detWidth;
 }
 
+// One block per group of rows: the column table goes to shared memory once, then the block
+// walks its rows (row r = all N columns of one detector row of one view), thread per column.
 template <typename T>
 __global__ void k_rebin_panel(const T* __restrict__ in, T* __restrict__ out,
-                              const PanelEntry* __restrict__ tab, int N, size_t total) {
-    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
-         e += (size_t)gridDim.x * blockDim.x) {
-        const int i = (int)(e % (size_t)N);
-        const PanelEntry t = tab[i];
-        const T* row = in + (e - i);
-        T v = T(0);
-        if (t.lo >= 0) {
-            if constexpr (sizeof(T) == 8)
-                v = __dadd_rn(__dmul_rn(row[t.lo], t.wl), __dmul_rn(row[t.hi], t.wh));
-            else
-                v = fmaf(row[t.lo], (float)t.wl, row[t.hi] * (float)t.wh);
+                              const PanelEntry* __restrict__ tab, int N, size_t rows) {
+    extern __shared__ PanelEntry st[];
+    for (int i = threadIdx.x; i < N; i += blockDim.x) st[i] = tab[i];
+    __syncthreads();
+    constexpr int RB = sizeof(T) == 8 ? 2 : 4;  // rows per step: independent loads in flight
+    for (size_t r0 = (size_t)blockIdx.x * RB; r0 < rows; r0 += (size_t)gridDim.x * RB) {
+        const int nr = (int)(rows - r0 < (size_t)RB ? rows - r0 : (size_t)RB);
+        for (int i = threadIdx.x; i < N; i += blockDim.x) {
+            const PanelEntry t = st[i];
+            T a[RB], b[RB];
+#pragma unroll
+            for (int q = 0; q < RB; ++q) {
+                a[q] = T(0);
+                b[q] = T(0);
+                if (q < nr && t.lo >= 0) {
+                    const T* row = in + (r0 + q) * (size_t)N;
+                    a[q] = row[t.lo];
+                    b[q] = row[t.hi];
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < RB; ++q) {
+                if (q >= nr) break;
+                T v = T(0);
+                if (t.lo >= 0) {
+                    if constexpr (sizeof(T) == 8)
+                        v = __dadd_rn(__dmul_rn(a[q], t.wl), __dmul_rn(b[q], t.wh));
+                    else
+                        v = fmaf(a[q], (float)t.wl, b[q] * (float)t.wh);
+                }
+                out[(r0 + q) * (size_t)N + i] = v;
+            }
         }
-        out[e] = v;
     }
 }
 
@@ -84,12 +106,21 @@ ctrecon_status rebin_dev(ctrecon_ctx* ctx, cudaStream_t s, const T* d_in, int N,
         Status st = ctx->ws_panel.ensure(tab.size() * sizeof(PanelEntry), "panel-rebin table");
         if (st.ok()) st = upload_now(ctx->ws_panel.ptr, tab.data(), tab.size() * sizeof(PanelEntry));
         if (!st.ok()) return fin(st);
-        const size_t total = (size_t)N * H * P;
+        const size_t rows = (size_t)H * P;
+        const size_t smem = (size_t)N * sizeof(PanelEntry);
+        if (smem > 200 * 1024)
+            return fin(make_status(CTRECON_ERR_UNSUPPORTED, "panel rebin: more than 8533 columns"));
+        if (smem > 48 * 1024) {
+            e = cudaFuncSetAttribute(k_rebin_panel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem);
+            if (e != cudaSuccess) return fin(cuda_status(e, "cudaFuncSetAttribute"));
+        }
         int sms = 148;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
-        const size_t want = (total + 255) / 256;
-        const unsigned grid = (unsigned)std::min<size_t>(want, (size_t)sms * 16);
-        k_rebin_panel<T><<<grid, 256, 0, s>>>(d_in, d_out, ctx->ws_panel.as<PanelEntry>(), N, total);
+        const int threads = N >= 512 ? 256 : 128;
+        const unsigned grid = (unsigned)std::min<size_t>((rows + 3) / 4, (size_t)sms * 8);
+        k_rebin_panel<T><<<grid, threads, smem, s>>>(d_in, d_out, ctx->ws_panel.as<PanelEntry>(), N,
+                                                     rows);
         e = cudaGetLastError();
         if (e != cudaSuccess) return fin(cuda_status(e, "k_rebin_panel"));
         return fin(Status::Ok());

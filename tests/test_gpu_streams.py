@@ -5,7 +5,8 @@
   contexts give: a geometry change must never touch tables that queued kernels still read.
 * The host (MEX-equivalent) calls pipeline their copies on three streams; with pinned host
   buffers the copies overlap the kernels, with pageable ones they do not. Both must give the
-  same bits.
+  same bits. The host backprojection accumulates view windows as they arrive: equal to the
+  one-pass backprojection up to the order of the FP32 sums.
 """
 import numpy as np
 import pytest
@@ -99,5 +100,11 @@ def test_host_calls_pinned_equal_pageable(torch_mod):
         assert np.array_equal(f_pin.numpy(), f_pg)
         assert np.array_equal(img_pin.numpy(), img_pg)
         assert np.array_equal(rec_pin.numpy(), rec_pg)
-        # the chain through the host equals filter then backprojection through the host
-        assert np.array_equal(rec_pg, img_pg)
+        # the chain through the host equals filter then backprojection through the host; the
+        # host backprojection sums its views in windows (as their upload completes), which only
+        # reorders the FP32 sums of a voxel
+        written = img_pg != 7.25
+        assert np.array_equal(written, rec_pg != 7.25)
+        rel = np.linalg.norm(rec_pg[written] - img_pg[written]) / np.linalg.norm(img_pg[written])
+        print(f"windowed vs one-pass host backprojection: rel diff {rel:.2e}")
+        assert rel < 1e-6
