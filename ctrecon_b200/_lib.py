@@ -97,6 +97,8 @@ SIGNATURES = [
                                    ctypes.POINTER(BPGeom), ctypes.POINTER(_vp)]),
     ("ctrecon_batch_destroy", None, [_vp]),
     ("ctrecon_batch_set_variant", _st, [_vp, ctypes.c_int]),
+    ("ctrecon_batch_get_variants", _st, [_vp, _ip, ctypes.c_int]),
+    ("ctrecon_batch_set_variants", _st, [_vp, _ip, ctypes.c_int]),
     ("ctrecon_batch_run_dev", _st, [_vp, _vp, ctypes.POINTER(_vp), ctypes.POINTER(_vp),
                                     ctypes.POINTER(_vp), ctypes.c_int]),
     ("ctrecon_batch_updates", _st, [_vp, ctypes.POINTER(ctypes.c_ulonglong)]),

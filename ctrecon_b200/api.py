@@ -324,7 +324,20 @@ class Batch:
                                        arr(d_fprojs, "d_fproj", "float32"),
                                        arr(d_images, "d_image", "float32"), ctypes.byref(r)),
               self.ctx.handle)
-        return _tune_dict(r)
+        d = _tune_dict(r)
+        d["per_scan"] = self.variants()
+        return d
+
+    def set_variants(self, variants):
+        """One backprojector form per scan (scans sharing a form share a launch)."""
+        arr = (ctypes.c_int * self.n)(*[int(v) for v in variants])
+        check(lib().ctrecon_batch_set_variants(self._h, arr, self.n), self.ctx.handle)
+
+    def variants(self):
+        """The backprojector form of each scan."""
+        out = (ctypes.c_int * self.n)()
+        check(lib().ctrecon_batch_get_variants(self._h, out, self.n), self.ctx.handle)
+        return [int(v) for v in out]
 
 
 def _tune_dict(r) -> dict:

@@ -28,17 +28,28 @@ void set_noctx_error(const std::string& m);
 
 using namespace ctr;
 
+// Scans that share a backprojector form: one persistent launch over their tiles.
+struct BatchGroup {
+    int variant = 0;
+    int nscans = 0;
+    long long tiles = 0;
+    int cells = 0, raw = 0;  // fourth-form staging capacities (largest over the group)
+    DevBuf table, counter;
+};
+
 struct ctrecon_batch {
     ctrecon_ctx* ctx = nullptr;
     int n = 0;
-    int variant = 0;
+    std::vector<int> svar;            // backprojector form of each scan
     std::vector<ctrecon_filter_params> fp;
     std::vector<std::unique_ptr<FilterPlan>> fplans;
     std::vector<std::unique_ptr<BPPlan>> bplans;
     std::vector<int> order;           // scans by decreasing backprojection work
     std::vector<size_t> pit_off;      // PiRecord offset of each scan in `pitab`
-    DevBuf pitab, scans_dev, counter, updates;
-    long long total_tiles = 0;
+    DevBuf pitab, updates;
+    // groups of scans by form (rebuilt by upload_scans; the buffers are reused)
+    std::vector<std::unique_ptr<BatchGroup>> groups;
+    int ngroups = 0;
     // what the graph was captured with: the buffer pointers, the context options, the
     // learned-initialiser version and the work-buffer allocation epoch
     std::vector<unsigned long long> key;
@@ -59,17 +70,16 @@ static ctrecon_status bfinish(ctrecon_ctx* ctx, const Status& s) {
     return s.code;
 }
 
-// the persistent backprojection launch over all scans (the scan table must be uploaded)
+// one persistent backprojection launch per group of scans sharing a form (the scan tables
+// must be uploaded)
 static Status batch_backproject(ctrecon_batch* b, cudaStream_t s) {
-    int cells = 0, raw = 0;  // fourth-form capacities: the largest over the scans
-    for (int i = 0; i < b->n; ++i) {
-        bp4_caps(*b->bplans[i]);
-        cells = std::max(cells, b->bplans[i]->caps_cells);
-        raw = std::max(raw, b->bplans[i]->caps_raw);
+    for (int g = 0; g < b->ngroups; ++g) {
+        BatchGroup& G = *b->groups[g];
+        CTR_TRY(launch_bkproj_batch(G.variant, s, G.table.as<BatchScanDev>(), G.nscans, G.tiles,
+                                    G.counter.as<unsigned long long>(), G.cells, G.raw,
+                                    b->ctx->ws_flag.as<int>()));
     }
-    return launch_bkproj_batch(b->variant, s, b->scans_dev.as<BatchScanDev>(), b->n,
-                               b->total_tiles, b->counter.as<unsigned long long>(), cells, raw,
-                               b->ctx->ws_flag.as<int>());
+    return Status::Ok();
 }
 
 static Status enqueue(ctrecon_batch* b, cudaStream_t s, const float* const* d_proj,
@@ -88,27 +98,51 @@ static Status enqueue(ctrecon_batch* b, cudaStream_t s, const float* const* d_pr
     return batch_backproject(b, s);
 }
 
+// Groups the scans by form (largest work first within a group) and uploads each group's scan
+// table; the group buffers are reused, so a stable configuration allocates nothing.
 static Status upload_scans(ctrecon_batch* b, cudaStream_t s, float* const* d_fproj,
                            float* const* d_image) {
-    std::vector<BatchScanDev> h(b->n);
-    long long first = 0;
+    std::vector<int> forms;
     for (int k = 0; k < b->n; ++k) {
-        const int i = b->order[k];
-        BPPlan& bp = *b->bplans[i];
-        h[k].kp = bp.kp;
-        h[k].fproj = d_fproj[i];
-        h[k].pit = b->pitab.as<PiRecord>() + b->pit_off[i];
-        h[k].views = bp.views.as<float4>();
-        h[k].xyz = bp.xyz.as<float>();
-        h[k].image = d_image[i];
-        h[k].first_tile = first;
-        first += bkproj_batch_tiles(bp.kp, b->variant);
+        const int v = b->svar[b->order[k]];
+        if (std::find(forms.begin(), forms.end(), v) == forms.end()) forms.push_back(v);
     }
-    b->total_tiles = first;
-    CTR_TRY(b->scans_dev.ensure(h.size() * sizeof(BatchScanDev), "batch scan table"));
-    CTR_CUDA(cudaMemcpyAsync(b->scans_dev.ptr, h.data(), h.size() * sizeof(BatchScanDev),
-                             cudaMemcpyHostToDevice, s));
-    CTR_CUDA(cudaStreamSynchronize(s));  // `h` is pageable and local
+    while (b->groups.size() < forms.size()) b->groups.emplace_back(new BatchGroup());
+    b->ngroups = (int)forms.size();
+    for (int g = 0; g < b->ngroups; ++g) {
+        BatchGroup& G = *b->groups[g];
+        G.variant = forms[g];
+        std::vector<BatchScanDev> h;
+        long long first = 0;
+        int cells = 0, raw = 0;
+        for (int k = 0; k < b->n; ++k) {
+            const int i = b->order[k];
+            if (b->svar[i] != G.variant) continue;
+            BPPlan& bp = *b->bplans[i];
+            BatchScanDev d;
+            d.kp = bp.kp;
+            d.fproj = d_fproj[i];
+            d.pit = b->pitab.as<PiRecord>() + b->pit_off[i];
+            d.views = bp.views.as<float4>();
+            d.xyz = bp.xyz.as<float>();
+            d.image = d_image[i];
+            d.first_tile = first;
+            first += bkproj_batch_tiles(bp.kp, G.variant);
+            h.push_back(d);
+            bp4_caps(bp);
+            cells = std::max(cells, bp.caps_cells);
+            raw = std::max(raw, bp.caps_raw);
+        }
+        G.nscans = (int)h.size();
+        G.tiles = first;
+        G.cells = cells;
+        G.raw = raw;
+        CTR_TRY(G.table.ensure(h.size() * sizeof(BatchScanDev), "batch scan table"));
+        CTR_TRY(G.counter.ensure(64, "batch work counter"));
+        CTR_CUDA(cudaMemcpyAsync(G.table.ptr, h.data(), h.size() * sizeof(BatchScanDev),
+                                 cudaMemcpyHostToDevice, s));
+        CTR_CUDA(cudaStreamSynchronize(s));  // `h` is pageable and local
+    }
     return Status::Ok();
 }
 
@@ -124,8 +158,9 @@ ctrecon_status ctrecon_batch_create(ctrecon_ctx* ctx, int n_scans,
         auto b = std::make_unique<ctrecon_batch>();
         b->ctx = ctx;
         b->n = n_scans;
-        b->variant = (ctx->opt_bp_variant >= 0 && ctx->opt_bp_variant <= 9) ? ctx->opt_bp_variant
-                                                                             : kDefaultBPVariant;
+        b->svar.assign(n_scans, (ctx->opt_bp_variant >= 0 && ctx->opt_bp_variant <= 9)
+                                    ? ctx->opt_bp_variant
+                                    : kDefaultBPVariant);
         b->fp.assign(fp, fp + n_scans);
         size_t nvox = 0;
         std::vector<double> work(n_scans);
@@ -150,7 +185,6 @@ ctrecon_status ctrecon_batch_create(ctrecon_ctx* ctx, int n_scans,
         std::stable_sort(b->order.begin(), b->order.end(),
                          [&](int a, int c) { return work[a] > work[c]; });
         Status s = b->pitab.ensure(nvox * sizeof(PiRecord), "batch PI tables");
-        if (s.ok()) s = b->counter.ensure(64, "batch work counter");
         if (s.ok()) s = b->updates.ensure(sizeof(unsigned long long) * n_scans, "batch counts");
         if (!s.ok()) return bfinish(ctx, s);
         *out = b.release();
@@ -168,10 +202,23 @@ void ctrecon_batch_destroy(ctrecon_batch* b) {
 
 ctrecon_status ctrecon_batch_set_variant(ctrecon_batch* b, int variant) {
     if (!b || variant < 0 || variant > 9) return CTRECON_ERR_INVALID_ARGUMENT;
-    if (variant != b->variant) {
-        b->variant = variant;
-        b->key.clear();  // tile counts change: rebuild the scan table and the graph
-    }
+    for (int& v : b->svar) v = variant;
+    b->key.clear();  // tile counts change: rebuild the scan tables and the graph
+    return CTRECON_OK;
+}
+
+ctrecon_status ctrecon_batch_set_variants(ctrecon_batch* b, const int* variants, int n) {
+    if (!b || !variants || n != b->n) return CTRECON_ERR_INVALID_ARGUMENT;
+    for (int i = 0; i < n; ++i)
+        if (variants[i] < 0 || variants[i] > 9) return CTRECON_ERR_INVALID_ARGUMENT;
+    b->svar.assign(variants, variants + n);
+    b->key.clear();
+    return CTRECON_OK;
+}
+
+ctrecon_status ctrecon_batch_get_variants(const ctrecon_batch* b, int* variants, int n) {
+    if (!b || !variants || n < b->n) return CTRECON_ERR_INVALID_ARGUMENT;
+    for (int i = 0; i < b->n; ++i) variants[i] = b->svar[i];
     return CTRECON_OK;
 }
 
@@ -241,19 +288,48 @@ ctrecon_status ctrecon_batch_tune(ctrecon_batch* b, void* stream, const float* c
     try {
         cudaSetDevice(ctx->device);
         cudaStream_t s = (cudaStream_t)stream;
-        // one eager run: filters, PI solves and a backprojection with the current form
+        // one eager run: filters, PI solves and a backprojection with the current forms
         ctrecon_status rc = ctrecon_batch_run_dev(b, stream, d_proj, d_fproj, d_image, 0);
         if (rc != CTRECON_OK) return rc;
-        const int saved = b->variant;
-        Status st = tune_candidates(
-            out, s,
-            [&](int v) {
-                b->variant = v;
-                return upload_scans(b, s, d_fproj, d_image);  // tile counts depend on the form
-            },
-            [&](int) { return batch_backproject(b, s); });
-        b->variant = st.ok() ? out->best_variant : saved;
-        if (st.ok()) {  // leave the winner's backprojection in the images
+        // each scan's form: every candidate timed on that scan alone (single-scan launches)
+        std::memset(out, 0, sizeof *out);
+        const int saved_opt = ctx->opt_bp_variant;
+        Status st;
+        std::vector<int> best(b->n, kDefaultBPVariant);
+        double best_sum = 0;
+        std::vector<double> cand_sum;
+        for (int i = 0; st.ok() && i < b->n; ++i) {
+            ctrecon_tune_result r;
+            st = tune_candidates(&r, s, nullptr, [&](int v) {
+                ctx->opt_bp_variant = v;
+                return launch_bkproj_f32(ctx, s, *b->bplans[i],
+                                         d_fproj[i], b->pitab.as<PiRecord>() + b->pit_off[i],
+                                         d_image[i]);
+            });
+            if (!st.ok()) break;
+            best[i] = r.best_variant;
+            best_sum += r.best_ms;
+            if (cand_sum.empty()) {
+                out->n = r.n;
+                cand_sum.assign(r.n, 0.0);
+                for (int c = 0; c < r.n; ++c) out->variants[c] = r.variants[c];
+            }
+            for (int c = 0; c < r.n; ++c)
+                cand_sum[c] = (cand_sum[c] < 0 || r.ms[c] < 0) ? -1.0 : cand_sum[c] + r.ms[c];
+        }
+        ctx->opt_bp_variant = saved_opt;
+        if (st.ok()) {
+            b->svar = best;
+            for (int c = 0; c < out->n; ++c) out->ms[c] = (float)cand_sum[c];
+            out->best_ms = (float)best_sum;  // sum of the scans' best single-scan times
+            // the form that covers most scans
+            int most = best[0], cnt = 0;
+            for (int v : best) {
+                const int k = (int)std::count(best.begin(), best.end(), v);
+                if (k > cnt) { cnt = k; most = v; }
+            }
+            out->best_variant = most;
+            // leave the winners' backprojections in the images
             st = upload_scans(b, s, d_fproj, d_image);
             if (st.ok()) st = batch_backproject(b, s);
             if (st.ok()) {

@@ -216,8 +216,13 @@ ctrecon_status ctrecon_batch_create(ctrecon_ctx* ctx, int n_scans,
                                     const ctrecon_filter_params* params,
                                     const ctrecon_bp_geom* geoms, ctrecon_batch** out);
 void ctrecon_batch_destroy(ctrecon_batch* batch);
-/* backprojector form of the batch: 0 .. 9 as CTRECON_OPT_BP_VARIANT (default: the context's) */
+/* backprojector form of every scan of the batch: 0 .. 9 as CTRECON_OPT_BP_VARIANT (default:
+ * the context's); scans that share a form share one persistent launch */
 ctrecon_status ctrecon_batch_set_variant(ctrecon_batch* batch, int variant);
+/* per-scan forms (n = the batch's scan count) */
+ctrecon_status ctrecon_batch_set_variants(ctrecon_batch* batch, const int* variants, int n);
+/* the form of each scan (n >= the batch's scan count) */
+ctrecon_status ctrecon_batch_get_variants(const ctrecon_batch* batch, int* variants, int n);
 /* d_proj[i] (input), d_fproj[i] (work), d_image[i] (output, in place) for scan i */
 ctrecon_status ctrecon_batch_run_dev(ctrecon_batch* batch, void* stream,
                                      const float* const* d_proj, float* const* d_fproj,
@@ -246,8 +251,10 @@ typedef struct ctrecon_tune_result {
 ctrecon_status ctrecon_tune_bkproj(ctrecon_ctx* ctx, void* stream, const ctrecon_bp_geom* g,
                                    const float* d_fproj, const void* d_pitab, float* d_image,
                                    ctrecon_tune_result* out);
-/* Batch: runs the batch once (filters and PI solves included), then times its persistent
- * backprojection launch for each candidate form and keeps the fastest for this batch. */
+/* Batch: runs the batch once (filters and PI solves included), then times every candidate form
+ * on each scan and keeps each scan's fastest (ctrecon_batch_get_variants); scans are grouped by
+ * form, one persistent launch per group. `out` gives, per candidate, the summed time over the
+ * scans, best_ms the sum of the scans' best times and best_variant the most chosen form. */
 ctrecon_status ctrecon_batch_tune(ctrecon_batch* batch, void* stream, const float* const* d_proj,
                                   float* const* d_fproj, float* const* d_image,
                                   ctrecon_tune_result* out);

@@ -85,14 +85,15 @@ def test_batch_tune_keeps_results(torch_mod):
         b = ct.Batch(cx, scans)
         res = b.tune(projs, fprojs, imgs, stream=stream)
         print("batch tuning:", res)
-        best = res["best_variant"]
-        assert best in res["ms"] and res["best_ms"] > 0
-        # a graph-replayed run with the tuned form equals single scans with that form
+        per_scan = res["per_scan"]
+        assert len(per_scan) == len(scans) and all(v in res["ms"] for v in per_scan)
+        assert res["best_ms"] > 0 and res["best_variant"] in per_scan
+        # a graph-replayed run with the tuned forms equals single scans with each scan's form
         for _ in range(3):
             b.run(projs, fprojs, imgs, stream=stream, use_graph=True)
-        cx.set_option(_lib.OPT_BP_VARIANT, best)
         singles = []
-        for s, d in zip(scans, projs):
+        for s, d, v in zip(scans, projs, per_scan):
+            cx.set_option(_lib.OPT_BP_VARIANT, v)
             f = torch.empty_like(d)
             cx.filter_dev(ct.scan_filter_params(s), d, f)
             img = torch.full(s.vol_shape, 7.25, dtype=torch.float32, device="cuda")
