@@ -44,6 +44,10 @@ struct Shared4 {
     uint64_t full[S], empty[S];
     Foot3 foot[S][NB];
     float4 vg[S][NB];
+    // per staged view: {byte address of the cell records less (kMagicBits + u0) * 16 +
+    // (kMagicBits + v0) * W16, W16 = row stride in bytes}, so that a consumer's cell base is
+    // bits(u + kMagic) * 16 + kb
+    int2 kw[S][NB];
     Foot3 pfoot[2][NB];  // producer side: footprints of the blocks being staged
     float4 pvg[2][NB];
     int s_pmin, s_pmax, s_abort;
@@ -151,7 +155,7 @@ __device__ __forceinline__ uint32_t tile4(const BPParams& kp, const float* __res
                         const float cx = (c & 1) ? bx1 : bx0, cy = (c & 2) ? by1 : by0;
                         const float fen = R - (cx * g.x + cy * g.y);
                         ok = ok && (fen > 1e-3f * R);
-                        const float inv = 1.f / fen;
+                        const float inv = rcp_approx(fen);  // within the +-1 cell margin
                         const float u = (cy * g.x - cx * g.y) * DdU * inv + HalfY;
                         const float va = (bz0 - g.z) * DdV * inv + HalfZ;
                         const float vb = (bz1 - g.z) * DdV * inv + HalfZ;
@@ -213,6 +217,11 @@ __device__ __forceinline__ uint32_t tile4(const BPParams& kp, const float* __res
                 if (lane == 0) {
                     sh.foot[slot][j] = f;
                     sh.vg[slot][j] = sh.pvg[ib & 1][j];
+                    const uint32_t W16 = (uint32_t)(f.W - 1) * 16u;
+                    const uint32_t kb = cell_s + (uint32_t)((slot * NB + j) * ccap) * 16u -
+                                        (uint32_t)(kMagicBits + f.u0) * 16u -
+                                        (uint32_t)(kMagicBits + f.v0) * W16;
+                    sh.kw[slot][j] = make_int2((int)kb, (int)W16);
                 }
                 if (f.W <= 0) continue;
                 const float* src = raw + ((ib & 1) * NB + j) * rcap;
@@ -252,12 +261,41 @@ __device__ __forceinline__ uint32_t tile4(const BPParams& kp, const float* __res
             const bool fast = __all_sync(0xffffffffu, vr.all_valid && pb >= vr.flo &&
                                                        pb + NB - 1 <= vr.fhi &&
                                                        pb + NB - 1 <= pmax && cells);
-            if (col_ok && wmin <= wmax && !(pb + NB - 1 < wmin || pb > wmax)) {
+            if (fast) {
+                // every view of the block has cell records and weight 1 for all voxels of the
+                // warp: no per-view tests
+#pragma unroll
+                for (int j = 0; j < NB; ++j) {
+                    const float4 gv = sh.vg[slot][j];
+                    const int2 kw = sh.kw[slot][j];
+                    const float fen = R - (X * gv.x + Y * gv.y);
+                    const float YY = Y * gv.x - X * gv.y;
+                    const float inv = rcp_approx(fen);
+                    const float kv = DdV * inv;
+                    const float r2 = fen * fen + YY * YY;
+                    const float dz0 = z0 - gv.z;
+                    const float u = fmaf(YY * DdU, inv, HalfYm);  // u - 1/2
+                    const float tu = u + kMagic;
+                    const float a = u - (tu - kMagic);           // alpha - 1/2
+                    const uint32_t W16 = (uint32_t)kw.y;
+                    const uint32_t cbase = (uint32_t)__float_as_int(tu) * 16u + (uint32_t)kw.x;
+#pragma unroll
+                    for (int k = 0; k < TZ; ++k) {
+                        const float dz = fmaf((float)k, dzf, dz0);
+                        const float v = fmaf(dz, kv, HalfZm);  // v - 1/2
+                        const float rinv = rsqrt_approx(fmaf(dz, dz, r2));
+                        const float tv = v + kMagic;
+                        const float b = v - (tv - kMagic);
+                        const float4 q = lds128((uint32_t)__float_as_int(tv) * W16 + cbase);
+                        acc[k] = fmaf(fmaf(b, fmaf(a, q.w, q.z), fmaf(a, q.y, q.x)), rinv, acc[k]);
+                    }
+                }
+            } else if (col_ok && wmin <= wmax && !(pb + NB - 1 < wmin || pb > wmax)) {
 #pragma unroll 1
                 for (int j = 0; j < NB; ++j) {
                     const int p = pb + j;
                     if (p > pmax) break;
-                    if (!fast && (p < vr.tmin || p > vr.tmax)) continue;
+                    if (p < vr.tmin || p > vr.tmax) continue;
                     const Foot3 f = sh.foot[slot][j];
                     const float4 gv = sh.vg[slot][j];
                     const float fen = R - (X * gv.x + Y * gv.y);
@@ -270,24 +308,11 @@ __device__ __forceinline__ uint32_t tile4(const BPParams& kp, const float* __res
                         const float u = fmaf(YY * DdU, inv, HalfYm);  // u - 1/2
                         const float tu = u + kMagic;
                         const float a = u - (tu - kMagic);           // alpha - 1/2
-                        const uint32_t W16 = (uint32_t)(f.W - 1) * 16u;
+                        const int2 kw = sh.kw[slot][j];
+                        const uint32_t W16 = (uint32_t)kw.y;
                         const uint32_t cbase =
-                            cell_s + (uint32_t)((slot * NB + j) * ccap) * 16u +
-                            ((uint32_t)__float_as_int(tu) - (uint32_t)(kMagicBits + f.u0)) * 16u -
-                            (uint32_t)(kMagicBits + f.v0) * W16;
-                        if (fast) {
-#pragma unroll
-                            for (int k = 0; k < TZ; ++k) {
-                                const float dz = fmaf((float)k, dzf, dz0);
-                                const float v = fmaf(dz, kv, HalfZm);  // v - 1/2
-                                const float rinv = rsqrt_approx(fmaf(dz, dz, r2));
-                                const float tv = v + kMagic;
-                                const float b = v - (tv - kMagic);
-                                const float4 q = lds128((uint32_t)__float_as_int(tv) * W16 + cbase);
-                                acc[k] = fmaf(fmaf(b, fmaf(a, q.w, q.z), fmaf(a, q.y, q.x)), rinv,
-                                              acc[k]);
-                            }
-                        } else {
+                            (uint32_t)__float_as_int(tu) * 16u + (uint32_t)kw.x;
+                        {
 #pragma unroll
                             for (int k = 0; k < TZ; ++k) {
                                 const int d0 = p - vr.bi[k];
