@@ -305,9 +305,9 @@ ctrecon_status ctrecon_set_option(ctrecon_ctx* ctx, ctrecon_option opt, int valu
         ctx->opt_filter_chunk = value;
         break;
     case CTRECON_OPT_BP_VARIANT:
-        if (!(value == CTRECON_BP_AUTO || (value >= 0 && value <= 9) || value == 100))
+        if (!(value == CTRECON_BP_AUTO || (value >= 0 && value <= kMaxBPVariant) || value == 100))
             return finish(ctx, make_status(CTRECON_ERR_INVALID_ARGUMENT,
-                                           "backprojector variant must be -1, 0..9 or 100"));
+                                           "backprojector variant must be -1, 0..12 or 100"));
         ctx->opt_bp_variant = value;
         break;
     case CTRECON_OPT_VERBOSE: ctx->opt_verbose = value; break;
@@ -315,6 +315,11 @@ ctrecon_status ctrecon_set_option(ctrecon_ctx* ctx, ctrecon_option opt, int valu
         if (value != CTRECON_DERIV_DIRECT && value != CTRECON_DERIV_CHAIN)
             return finish(ctx, make_status(CTRECON_ERR_INVALID_ARGUMENT, "bad derivative mode"));
         ctx->opt_deriv = value;
+        break;
+    case CTRECON_OPT_BP_WINDOW:
+        if (value < 0)
+            return finish(ctx, make_status(CTRECON_ERR_INVALID_ARGUMENT, "window must be >= 0"));
+        ctx->opt_bp_window = value;
         break;
     default: return finish(ctx, make_status(CTRECON_ERR_INVALID_ARGUMENT, "unknown option"));
     }
@@ -330,6 +335,7 @@ ctrecon_status ctrecon_get_option(const ctrecon_ctx* ctx, ctrecon_option opt, in
     case CTRECON_OPT_BP_VARIANT: *value = ctx->opt_bp_variant; break;
     case CTRECON_OPT_VERBOSE: *value = ctx->opt_verbose; break;
     case CTRECON_OPT_DERIVATIVE: *value = ctx->opt_deriv; break;
+    case CTRECON_OPT_BP_WINDOW: *value = ctx->opt_bp_window; break;
     default: return CTRECON_ERR_INVALID_ARGUMENT;
     }
     return CTRECON_OK;

@@ -13,8 +13,9 @@
 namespace ctr {
 
 // candidate forms: second form (tile shapes 8x8, 4x8, 8x4 slices x views), third form
-// (blocks of 4 views), fourth form (producer-warp staging: 2, 3, 4 producer warps)
-const int kTuneCandidates[] = {2, 3, 4, 0, 7, 8, 9};
+// (blocks of 4 views), fourth form (producer-warp staging: 2, 3, 4 producer warps), fifth form
+// (cell records copied from global memory: three rings)
+const int kTuneCandidates[] = {2, 3, 4, 0, 7, 8, 9, 10, 11, 12};
 const int kNumTuneCandidates = (int)(sizeof(kTuneCandidates) / sizeof(kTuneCandidates[0]));
 
 std::string tune_key(const BPGeom& g) {
@@ -89,12 +90,13 @@ bool launch_does_not_fit(const Status& st) {
 
 Status tune_candidates(ctrecon_tune_result* res, cudaStream_t s,
                        const std::function<Status(int)>& prepare,
-                       const std::function<Status(int)>& run_one) {
+                       const std::function<Status(int)>& run_one, int max_variant) {
     std::memset(res, 0, sizeof *res);
     res->best_variant = -1;
     res->best_ms = -1.f;
     for (int c = 0; c < kNumTuneCandidates && res->n < CTRECON_TUNE_MAX; ++c) {
         const int v = kTuneCandidates[c];
+        if (v > max_variant) continue;
         float ms = -1.f;
         Status st = prepare ? prepare(v) : Status::Ok();
         if (st.ok()) st = time_launches(s, 2, [&] { return run_one(v); }, &ms);
@@ -186,7 +188,7 @@ ctrecon_status ctrecon_tune_load(ctrecon_ctx* ctx, const char* path) {
         std::string key;
         int v = 0;
         float ms = 0.f;
-        if (!(is >> key >> v >> ms) || !((v >= 0 && v <= 9) || v == 100))
+        if (!(is >> key >> v >> ms) || !((v >= 0 && v <= kMaxBPVariant) || v == 100))
             return tfinish(ctx, make_status(CTRECON_ERR_INVALID_ARGUMENT, "bad tuning table line"));
         ctx->tune[key] = {v, ms};
     }

@@ -305,7 +305,7 @@ ctrecon_status ctrecon_batch_tune(ctrecon_batch* b, void* stream, const float* c
                 return launch_bkproj_f32(ctx, s, *b->bplans[i],
                                          d_fproj[i], b->pitab.as<PiRecord>() + b->pit_off[i],
                                          d_image[i]);
-            });
+            }, 9);  // the forms the persistent batched kernel has
             if (!st.ok()) break;
             best[i] = r.best_variant;
             best_sum += r.best_ms;

@@ -251,14 +251,17 @@ template <typename OutT>
 Status launch_bkproj_v2(int variant, cudaStream_t s, BPPlan& plan, const float* d_fproj,
                         const PiRecord* d_pitab, OutT* d_image, int* err);
 
-// CTRECON_OPT_BP_VARIANT: 0..9 select the tiled forms (bkproj2.cu), 100 the first form above,
-// CTRECON_BP_AUTO the tuning table's choice. The fourth form (5..9) reports a bounded wait
-// that gave up in the context's device word.
+// CTRECON_OPT_BP_VARIANT: 0..12 select the tiled forms (bkproj2.cu), 100 the first form above,
+// CTRECON_BP_AUTO the tuning table's choice. The fourth and fifth forms (5..12) report a
+// bounded wait that gave up in the context's device word.
 Status launch_bkproj_f32(ctrecon_ctx* ctx, cudaStream_t s, BPPlan& plan, const float* d_fproj,
                          const PiRecord* d_pitab, float* d_image) {
     const int variant = bp_variant_for(ctx, plan.g);
     if (variant >= 100) return launch_bk<float>(s, plan, d_fproj, d_pitab, d_image);
     if (!ctx->ws_flag.ptr) return make_status(CTRECON_ERR_INTERNAL, "device error word not set up");
+    if (variant >= 10)
+        return launch_bkproj_v5<float>(variant, s, plan, d_fproj, d_pitab, d_image,
+                                       ctx->ws_flag.as<int>(), ctx->ws_rec, ctx->opt_bp_window);
     return launch_bkproj_v2<float>(variant, s, plan, d_fproj, d_pitab, d_image,
                                    ctx->ws_flag.as<int>());
 }
@@ -268,6 +271,9 @@ Status launch_bkproj_f64out(ctrecon_ctx* ctx, cudaStream_t s, BPPlan& plan,
     const int variant = bp_variant_for(ctx, plan.g);
     if (variant >= 100) return launch_bk<double>(s, plan, d_fproj, d_pitab, d_image);
     if (!ctx->ws_flag.ptr) return make_status(CTRECON_ERR_INTERNAL, "device error word not set up");
+    if (variant >= 10)
+        return launch_bkproj_v5<double>(variant, s, plan, d_fproj, d_pitab, d_image,
+                                        ctx->ws_flag.as<int>(), ctx->ws_rec, ctx->opt_bp_window);
     return launch_bkproj_v2<double>(variant, s, plan, d_fproj, d_pitab, d_image,
                                     ctx->ws_flag.as<int>());
 }

@@ -298,8 +298,46 @@ k_bkproj4(BPParams kp, const float* __restrict__ fproj, const PiRecord* __restri
     extern __shared__ __align__(16) unsigned char dyn4[];
     __shared__ Shared4<NB, S, PW> sh;
     tile4_init(sh);
-    tile4<NB, S, PW, OutT>(kp, fproj, pit, views, xyz, image, blockIdx.x, blockIdx.y, blockIdx.z,
-                           sh, dyn4, caps, err, 0u);
+    tile4<NB, S, PW, false, OutT>(kp, fproj, pit, views, xyz, image, blockIdx.x, blockIdx.y,
+                                  blockIdx.z, sh, dyn4, caps, err, 0u);
+}
+
+// Fifth form: the fourth form's consumers fed from the global cell records (k_cell_records) by
+// one producer warp with bulk copies. Three CTAs per SM.
+template <int NB, int S, int MINB, typename OutT>
+__global__ void __launch_bounds__(32 * 9, MINB)
+k_bkproj5(BPParams kp, const float* __restrict__ fproj, const PiRecord* __restrict__ pit,
+          const float4* __restrict__ views, const float* __restrict__ xyz,
+          OutT* __restrict__ image, Caps4 caps, int* err, const float4* __restrict__ rec,
+          int rec_p0) {
+    extern __shared__ __align__(128) unsigned char dyn5[];
+    __shared__ Shared4<NB, S, 1> sh;
+    tile4_init(sh);
+    tile4<NB, S, 1, true, OutT>(kp, fproj, pit, views, xyz, image, blockIdx.x, blockIdx.y,
+                                blockIdx.z, sh, dyn5, caps, err, 0u, rec, rec_p0);
+}
+
+// The cell records of views [p0, p0 + nviews): rec[v][r][c] = cell_record of the samples
+// (r, c) .. (r + 1, c + 1) of view p0 + v, (ZL - 1) x (YL - 1) cells per view.
+__global__ void k_cell_records(const float* __restrict__ fproj, float4* __restrict__ rec, int p0,
+                               int nviews, int YL, int ZL) {
+    const int RW = YL - 1, RH = ZL - 1;
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int r = blockIdx.y;
+    if (c >= RW) return;
+    for (int v = blockIdx.z; v < nviews; v += gridDim.z) {
+        const float* t = fproj + ((size_t)(p0 + v) * ZL + r) * YL + c;
+        rec[((size_t)v * RH + r) * RW + c] =
+            cell_record(__ldg(t), __ldg(t + 1), __ldg(t + YL), __ldg(t + YL + 1));
+    }
+}
+
+template <typename OutT>
+__global__ void k_zero_valid_any(const PiRecord* __restrict__ pit, OutT* __restrict__ image,
+                                 size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x)
+        if (pit[i].bi != kPiInvalid) image[i] = (OutT)0;
 }
 
 // Variants: 0, 1 = third form with blocks of 4 / 8 views; 2, 3, 4 = second form with
@@ -335,8 +373,8 @@ k_bkproj4_batch(const BatchScanDev* __restrict__ scans, int n_scans, long long t
         const int bx = (int)(local % nxt);
         const int by = (int)((local / nxt) % nyt);
         const int bz = (int)(local / ((long long)nxt * nyt));
-        iter = tile4<NB, S, PW, float>(sc.kp, sc.fproj, sc.pit, sc.views, sc.xyz, sc.image, bx,
-                                       by, bz, sh, dynb4, caps, err, iter);
+        iter = tile4<NB, S, PW, false, float>(sc.kp, sc.fproj, sc.pit, sc.views, sc.xyz,
+                                              sc.image, bx, by, bz, sh, dynb4, caps, err, iter);
         if (sh.s_abort) break;  // uniform: read after the tile's closing barrier
     }
 }
@@ -583,6 +621,81 @@ Status launch_bkproj_v2(int variant, cudaStream_t s, BPPlan& plan, const float* 
     default: return launch_v3<4, OutT>(s, plan, d_fproj, d_pitab, d_image);
     }
 }
+
+// ---- fifth form ------------------------------------------------------------------------
+// Shared memory per fifth-form CTA: three CTAs per SM (MINB 3) or two.
+constexpr size_t smem5_budget(int minb) { return minb >= 3 ? 72 * 1024 : 108 * 1024; }
+
+template <int NB, int S, int MINB, typename OutT>
+static Status launch_v5(cudaStream_t s, BPPlan& plan, const BPParams& kp, const float* d_fproj,
+                        const PiRecord* d_pitab, OutT* d_image, int* err, const float4* rec,
+                        int rec_p0) {
+    bp4_caps(plan);
+    int cells = plan.caps_cells;
+    const size_t budget = smem5_budget(MINB);
+    if ((size_t)S * NB * cells * 16 > budget)
+        cells = std::max(64, (int)(budget / ((size_t)S * NB * 16)) / 4 * 4);
+    const Caps4 caps{cells, 0};
+    dim3 grid((kp.NX + kTXY2 - 1) / kTXY2, (kp.NY + kTXY2 - 1) / kTXY2, (kp.NZ + 7) / 8);
+    const size_t smem = tile4_smem_bytes<NB, S, 1>(caps);
+    CTR_CUDA(cudaFuncSetAttribute(k_bkproj5<NB, S, MINB, OutT>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_bkproj5<NB, S, MINB, OutT><<<grid, 32 * 9, smem, s>>>(
+        kp, d_fproj, d_pitab, plan.views.as<float4>(), plan.xyz.as<float>(), d_image, caps, err,
+        rec, rec_p0);
+    CTR_CUDA(cudaGetLastError());
+    return Status::Ok();
+}
+
+// Variants 10, 11, 12: (NB, S, CTAs per SM) = (4, 3, 3), (4, 4, 2), (8, 2, 2). The loop views
+// [win0, win1] of the plan are backprojected in windows whose cell records fit kRecBudget (and
+// of at most max_views views when that is > 0);
+// with more than one window the valid voxels are zeroed first (or kept, when the plan
+// accumulates) and every window adds its sum.
+template <typename OutT>
+Status launch_bkproj_v5(int variant, cudaStream_t s, BPPlan& plan, const float* d_fproj,
+                        const PiRecord* d_pitab, OutT* d_image, int* err, DevBuf& recbuf,
+                        int max_views) {
+    const BPParams& kp0 = plan.kp;
+    const int RW = kp0.YL - 1, RH = kp0.ZL - 1;
+    const size_t plane = (size_t)RW * RH * sizeof(float4);
+    const int w0 = std::max(0, kp0.win0), w1 = std::min(kp0.P - 1, kp0.win1);
+    if (w1 < w0) return Status::Ok();
+    const int nv_all = w1 - w0 + 1;
+    int per = (int)std::max<size_t>(1, std::min<size_t>(nv_all, kRecBudget / plane));
+    if (max_views > 0) per = std::min(per, max_views);
+    const int nwin = (nv_all + per - 1) / per;
+    CTR_TRY(recbuf.ensure((size_t)std::min(per, nv_all) * plane, "cell records"));
+    BPParams kp = kp0;
+    if (nwin > 1 && !kp0.accum) {
+        const size_t n = (size_t)kp0.NX * kp0.NY * kp0.NZ;
+        const unsigned g = (unsigned)std::min<size_t>((n + 255) / 256, 148 * 32);
+        k_zero_valid_any<OutT><<<g, 256, 0, s>>>(d_pitab, d_image, n);
+        CTR_CUDA(cudaGetLastError());
+        kp.accum = 1;
+    }
+    float4* rec = recbuf.as<float4>();
+    for (int w = 0; w < nwin; ++w) {
+        const int a = w0 + w * per, b = std::min(w1, a + per - 1);
+        const int nv = b - a + 1;
+        dim3 g((RW + 127) / 128, RH, (unsigned)std::min(nv, 65535));
+        k_cell_records<<<g, 128, 0, s>>>(d_fproj, rec, a, nv, kp0.YL, kp0.ZL);
+        CTR_CUDA(cudaGetLastError());
+        kp.win0 = a;
+        kp.win1 = b;
+        Status st;
+        switch (variant) {
+        case 11: st = launch_v5<4, 4, 2, OutT>(s, plan, kp, d_fproj, d_pitab, d_image, err, rec, a); break;
+        case 12: st = launch_v5<8, 2, 2, OutT>(s, plan, kp, d_fproj, d_pitab, d_image, err, rec, a); break;
+        default: st = launch_v5<4, 3, 3, OutT>(s, plan, kp, d_fproj, d_pitab, d_image, err, rec, a); break;
+        }
+        CTR_TRY(st);
+    }
+    return Status::Ok();
+}
+
+template Status launch_bkproj_v5<float>(int, cudaStream_t, BPPlan&, const float*, const PiRecord*, float*, int*, DevBuf&, int);
+template Status launch_bkproj_v5<double>(int, cudaStream_t, BPPlan&, const float*, const PiRecord*, double*, int*, DevBuf&, int);
 
 template Status launch_bkproj_v2<float>(int, cudaStream_t, BPPlan&, const float*, const PiRecord*, float*, int*);
 template Status launch_bkproj_v2<double>(int, cudaStream_t, BPPlan&, const float*, const PiRecord*, double*, int*);

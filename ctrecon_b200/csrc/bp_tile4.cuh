@@ -15,6 +15,10 @@
 //  * Capacities (cell records and raw floats per staged view) are launch parameters sized on
 //    the host from the geometry; a view whose footprint does not fit, or reaches the detector
 //    border, is read directly from FProj with the first form's clamped indices.
+//  * REC = true (the fifth form): the cell records of every view were written to global memory
+//    beforehand (k_cell_records); a single producer warp computes the footprints and brings
+//    each footprint row into the ring with one cp.async.bulk (complete_tx on `full`), so no
+//    thread builds records and no raw rows are staged.
 #pragma once
 
 #include "bp_tile3.cuh"
@@ -32,6 +36,27 @@ __device__ __forceinline__ void mbar_arrive4(uint64_t* bar) {
 // bounded wait (suspend-hinted try_wait, time limit): tc_util.cuh
 __device__ __forceinline__ bool mbar_wait4(uint64_t* bar, uint32_t parity, int* err, int code) {
     return tcu::mbar_wait(bar, parity, err, code);
+}
+__device__ __forceinline__ void mbar_expect_tx4(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.expect_tx.relaxed.cta.shared::cta.b64 [%0], %1;"
+                 ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+// global -> shared bulk copy (16-byte aligned addresses, size a multiple of 16) completing
+// `bytes` of the barrier's transaction count
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes,
+                                         uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+        ::"r"(dst), "l"(src), "r"(bytes), "r"(smem_addr(bar)) : "memory");
+}
+
+// The bilinear record of the cell between detector samples (r, c) .. (r + 1, c + 1), for
+// offsets alpha - 1/2, beta - 1/2 from the cell centre: value = A + a B + b (C + a D).
+__device__ __forceinline__ float4 cell_record(float t00, float t01, float t10, float t11) {
+    const float h0 = t01 - t00, h1 = t11 - t10;
+    const float g0 = t10 - t00, g1 = t11 - t01;
+    return make_float4(0.25f * ((t00 + t01) + (t10 + t11)), 0.5f * (h0 + h1), 0.5f * (g0 + g1),
+                       h1 - h0);
 }
 
 struct Caps4 {
@@ -75,14 +100,15 @@ __device__ __forceinline__ void tile4_init(Shared4<NB, S, PW>& sh) {
 // Called by all 32 * (8 + PW) threads with the same `iter` (blocks of views this CTA has
 // processed before); returns the new count. Returns with no copies in flight. Sets
 // sh.s_abort (and leaves the tile unwritten) when a wait gave up.
-template <int NB, int S, int PW, typename OutT>
+template <int NB, int S, int PW, bool REC, typename OutT>
 __device__ __forceinline__ uint32_t tile4(const BPParams& kp, const float* __restrict__ fproj,
                                           const PiRecord* __restrict__ pit,
                                           const float4* __restrict__ views,
                                           const float* __restrict__ xyz, OutT* __restrict__ image,
                                           int bx, int by, int bz, Shared4<NB, S, PW>& sh,
                                           unsigned char* dyn, Caps4 caps, int* err,
-                                          uint32_t iter) {
+                                          uint32_t iter, const float4* __restrict__ rec = nullptr,
+                                          int rec_p0 = 0) {
     constexpr int TZ = 8;
     const int ccap = caps.cells, rcap = caps.raw;
     float4* cellbuf = reinterpret_cast<float4*>(dyn);                          // S * NB * ccap
@@ -124,6 +150,7 @@ __device__ __forceinline__ uint32_t tile4(const BPParams& kp, const float* __res
     float acc[TZ];
 #pragma unroll
     for (int k = 0; k < TZ; ++k) acc[k] = 0.f;
+    int issued = 0;  // fifth form: blocks whose copies this producer thread has started
 
     if (!consumer) {
         // ------------------------------------------------------------------ producers
@@ -168,8 +195,8 @@ __device__ __forceinline__ uint32_t tile4(const BPParams& kp, const float* __res
                         const int u0 = (int)floorf(umin) - 1, u1 = (int)floorf(umax) + 2;
                         const int v0 = (int)floorf(vmin) - 1, v1 = (int)floorf(vmax) + 2;
                         const int W = u1 - u0 + 1, H = v1 - v0 + 1;
-                        if (u0 >= 0 && u1 <= YL - 1 && v0 >= 0 && v1 <= ZL - 1 && W <= 64 &&
-                            W * H <= rcap && (W - 1) * (H - 1) <= ccap)
+                        if (u0 >= 0 && u1 <= YL - 1 && v0 >= 0 && v1 <= ZL - 1 &&
+                            (REC || (W <= 64 && W * H <= rcap)) && (W - 1) * (H - 1) <= ccap)
                             f = Foot3{u0, v0, W, H};
                     }
                 }
@@ -193,6 +220,50 @@ __device__ __forceinline__ uint32_t tile4(const BPParams& kp, const float* __res
             }
             cp_async_commit();
         };
+        // the block's records: per-view constants, then the footprint (or nothing) in slot
+        auto publish = [&](int ib, uint32_t slot, int j, const Foot3& f) {
+            if (lane == 0) {
+                sh.foot[slot][j] = f;
+                sh.vg[slot][j] = sh.pvg[ib & 1][j];
+                const uint32_t W16 = (uint32_t)(f.W - 1) * 16u;
+                const uint32_t kb = cell_s + (uint32_t)((slot * NB + j) * ccap) * 16u -
+                                    (uint32_t)(kMagicBits + f.u0) * 16u -
+                                    (uint32_t)(kMagicBits + f.v0) * W16;
+                sh.kw[slot][j] = make_int2((int)kb, (int)W16);
+            }
+        };
+        if constexpr (REC) {
+            // fifth form: footprint rows copied from the global cell records
+            const int RW = YL - 1;
+            const size_t plane = (size_t)(ZL - 1) * RW;
+            float4 gnext = view_of(0);
+            for (int ib = 0; ib < nblk; ++ib) {
+                const float4 gv = gnext;
+                gnext = view_of(ib + 1);
+                footprint(ib, gv);
+                const uint32_t g = iter + ib, slot = g % S, use = g / S;
+                if (use >= 1 && !mbar_wait4(&sh.empty[slot], (use - 1) & 1, err, 11)) {
+                    sh.s_abort = 1;
+                    break;
+                }
+                for (int j = pw; j < NB; j += PW) {
+                    const Foot3 f = sh.pfoot[ib & 1][j];
+                    publish(ib, slot, j, f);
+                    if (f.W <= 0) continue;
+                    const uint32_t rowb = (uint32_t)(f.W - 1) * 16u;
+                    const float4* src = rec + (size_t)(pmin + ib * NB + j - rec_p0) * plane +
+                                        (size_t)f.v0 * RW + f.u0;
+                    const uint32_t dst = cell_s + (uint32_t)((slot * NB + j) * ccap) * 16u;
+                    for (int r = lane; r < f.H - 1; r += 32) {
+                        mbar_expect_tx4(&sh.full[slot], rowb);
+                        bulk_g2s(dst + (uint32_t)r * rowb, src + (size_t)r * RW, rowb,
+                                 &sh.full[slot]);
+                    }
+                }
+                mbar_arrive4(&sh.full[slot]);
+                issued = ib + 1;
+            }
+        } else {
         footprint(0, view_of(0));
         stage(0);
         float4 gnext = view_of(1);
@@ -214,15 +285,7 @@ __device__ __forceinline__ uint32_t tile4(const BPParams& kp, const float* __res
             }
             for (int j = pw; j < NB; j += PW) {
                 const Foot3 f = sh.pfoot[ib & 1][j];
-                if (lane == 0) {
-                    sh.foot[slot][j] = f;
-                    sh.vg[slot][j] = sh.pvg[ib & 1][j];
-                    const uint32_t W16 = (uint32_t)(f.W - 1) * 16u;
-                    const uint32_t kb = cell_s + (uint32_t)((slot * NB + j) * ccap) * 16u -
-                                        (uint32_t)(kMagicBits + f.u0) * 16u -
-                                        (uint32_t)(kMagicBits + f.v0) * W16;
-                    sh.kw[slot][j] = make_int2((int)kb, (int)W16);
-                }
+                publish(ib, slot, j, f);
                 if (f.W <= 0) continue;
                 const float* src = raw + ((ib & 1) * NB + j) * rcap;
                 float4* dst = cellbuf + ((size_t)slot * NB + j) * ccap;
@@ -230,11 +293,7 @@ __device__ __forceinline__ uint32_t tile4(const BPParams& kp, const float* __res
                 for (int r = 0; r < f.H - 1; ++r) {
                     for (int c = lane; c < Wc; c += 32) {
                         const float* s0 = src + r * f.W + c;
-                        const float t00 = s0[0], t01 = s0[1], t10 = s0[f.W], t11 = s0[f.W + 1];
-                        const float h0 = t01 - t00, h1 = t11 - t10;
-                        const float g0 = t10 - t00, g1 = t11 - t01;
-                        dst[r * Wc + c] = make_float4(0.25f * ((t00 + t01) + (t10 + t11)),
-                                                      0.5f * (h0 + h1), 0.5f * (g0 + g1), h1 - h0);
+                        dst[r * Wc + c] = cell_record(s0[0], s0[1], s0[f.W], s0[f.W + 1]);
                     }
                 }
             }
@@ -242,6 +301,7 @@ __device__ __forceinline__ uint32_t tile4(const BPParams& kp, const float* __res
             mbar_arrive4(&sh.full[slot]);
         }
         cp_async_wait<0>();
+        }
     } else {
         // ------------------------------------------------------------------ consumers
         const float X = col_ok ? xc[x] : 0.f, Y = col_ok ? yc[y] : 0.f;
@@ -364,6 +424,17 @@ __device__ __forceinline__ uint32_t tile4(const BPParams& kp, const float* __res
         }
     }
     __syncthreads();  // every role is done with the ring; an abort is visible
+    if constexpr (REC) {
+        if (sh.s_abort && !consumer) {
+            // no copy may still be writing the ring when the CTA moves on or exits: wait
+            // (bounded, whatever the error word says) for the blocks not known complete
+            for (int ib = max(0, issued - S); ib < issued; ++ib) {
+                const uint32_t g = iter + ib;
+                tcu::mbar_drain(&sh.full[g % S], (g / S) & 1);
+            }
+        }
+        __syncthreads();
+    }
     if (col_ok && !sh.s_abort) {
 #pragma unroll
         for (int k = 0; k < TZ; ++k) {

@@ -150,7 +150,7 @@ constexpr int kDefaultBPVariant = 2;
 // the last two timed with CUDA events on s; candidates that cannot launch are marked -1.
 Status tune_candidates(ctrecon_tune_result* res, cudaStream_t s,
                        const std::function<Status(int)>& prepare,
-                       const std::function<Status(int)>& run_one);
+                       const std::function<Status(int)>& run_one, int max_variant = 1000);
 
 // One scan of a batched backprojection (batch.cpp, bkproj2.cu)
 struct BatchScanDev {
@@ -185,6 +185,7 @@ struct ctrecon_ctx {
     int opt_bp_variant = 2;  // second form, 8 slices x 8 views
     int opt_verbose = 0;
     int opt_deriv = CTRECON_DERIV_CHAIN;
+    int opt_bp_window = 0;
     cudaStream_t host_stream = nullptr;  // stream for the synchronous host calls
     cudaStream_t up_stream = nullptr;    // host -> device copies of the host calls
     cudaStream_t down_stream = nullptr;  // device -> host copies of the host calls
@@ -202,6 +203,7 @@ struct ctrecon_ctx {
     ctr::DevBuf ws_dual;     // second filter result of FilteringMode 1
     ctr::DevBuf ws_ell;      // phantom ellipsoids
     ctr::DevBuf ws_flag;     // device error word
+    ctr::DevBuf ws_rec;      // cell records of the fifth-form backprojection (one window)
     ctr::PinetState pinet;   // learned PI-line initialiser
     // autotuner: backprojector form per geometry key (tune_key), with its time
     std::map<std::string, std::pair<int, float>> tune;
@@ -229,6 +231,14 @@ Status launch_bkproj_f64out(ctrecon_ctx* ctx, cudaStream_t s, BPPlan& plan,
                             const float* d_fproj, const PiRecord* d_pitab, double* d_image);
 Status launch_convert_f64_to_f32(cudaStream_t s, const double* in, float* out, size_t n);
 Status launch_zero_valid_f64(cudaStream_t s, const PiRecord* d_pitab, double* d_image, size_t n);
+// Fifth form (variants 10..12, bkproj2.cu): cell records of at most kRecBudget bytes of views
+// at a time in `recbuf`, then the backprojection of those views.
+constexpr size_t kRecBudget = (size_t)8 << 30;
+constexpr int kMaxBPVariant = 12;
+template <typename OutT>
+Status launch_bkproj_v5(int variant, cudaStream_t s, BPPlan& plan, const float* d_fproj,
+                        const PiRecord* d_pitab, OutT* d_image, int* err, DevBuf& recbuf,
+                        int max_views);
 Status launch_convert_f32_to_f64(cudaStream_t s, const float* in, double* out, size_t n);
 Status launch_average_into(cudaStream_t s, float* a, const float* b, size_t n);
 Status launch_phantom(cudaStream_t s, const BPGeom& g, const double* d_ell, int n_ell,

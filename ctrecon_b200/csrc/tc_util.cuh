@@ -61,6 +61,18 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* e
     return false;
 }
 
+// Error-path wait for async copies still completing on `bar` (phase of the given parity):
+// bounded by 10 ms of %globaltimer, independent of the error word; returns whether it completed.
+__device__ __forceinline__ bool mbar_drain(uint64_t* bar, uint32_t parity) {
+    const uint32_t a = smem_u32(bar);
+    const uint64_t t0 = globaltimer_ns();
+    for (uint32_t it = 0; it < kWaitIterLimit; ++it) {
+        if (mbar_try_wait(a, parity)) return true;
+        if (globaltimer_ns() - t0 > 10000000ull) break;
+    }
+    return false;
+}
+
 // K-major operand, 128-byte rows, 128-byte swizzle (SBO = 1024 B, version 1, layout 2)
 __device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
     uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);

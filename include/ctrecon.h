@@ -108,10 +108,16 @@ typedef enum ctrecon_option {
                                          form (slices x views) 8x8, 4x8, 8x4; 5, 6, 7 = per-cell
                                          records staged by producer warps (views per block x
                                          ring slots x producer warps) 4x2x1, 2x4x1, 4x2x2;
-                                         8, 9 = the same with 4x2x3, 4x3x4; 100 = first
-                                         form; CTRECON_BP_AUTO = the tuning table's choice */
+                                         8, 9 = the same with 4x2x3, 4x3x4; 10, 11, 12 =
+                                         per-cell records written to device memory first and
+                                         copied in by one producer warp (views per block x
+                                         ring slots x CTAs per SM) 4x3x3, 4x4x2, 8x2x2;
+                                         100 = first form; CTRECON_BP_AUTO = the tuning
+                                         table's choice */
     CTRECON_OPT_VERBOSE = 5,
-    CTRECON_OPT_DERIVATIVE = 6        /* CTRECON_DERIV_*; default CHAIN (the MEX filter's) */
+    CTRECON_OPT_DERIVATIVE = 6,       /* CTRECON_DERIV_*; default CHAIN (the MEX filter's) */
+    CTRECON_OPT_BP_WINDOW = 7         /* views per cell-record window of variants 10..12;
+                                         0 (default) = as many as 8 GiB of records hold */
 } ctrecon_option;
 
 /* ---- context ---------------------------------------------------------------------- */

@@ -162,8 +162,10 @@ def test_pinet_training_inference_and_gain(torch_mod):
 
 @pytest.mark.parametrize("name", ["c1", "c2s"])
 def test_backprojector_variants_agree(torch_mod, name):
-    """Every tiled form (0, 1: per-cell records; 2-4: second form; 5-7: per-cell records
-    staged by producer warps) against the first form.
+    """Every tiled form (0, 1: per-cell records; 2-4: second form; 5-9: per-cell records
+    staged by producer warps; 10-12: per-cell records copied from device memory) against the
+    first form; variant 10 also in windows of 300 views (valid voxels zeroed, then every
+    window accumulated).
     c1's 16-row detector sends most tiles through the direct-read fallback, c2s's 64 rows
     almost none."""
     torch = torch_mod
@@ -178,14 +180,20 @@ def test_backprojector_variants_agree(torch_mod, name):
         cx.phantom_dev(g, s.ellipsoids(), d_proj)
         d_f = torch.empty_like(d_proj)
         cx.filter_dev(ct.scan_filter_params(s), d_proj, d_f)
-        for var in (0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 100):
+        for var in (0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 100):
             cx.set_option(_lib.OPT_BP_VARIANT, var)
             d_img = torch.full(s.vol_shape, 7.25, dtype=torch.float32, device="cuda")
             cx.bkproj_dev(g, d_f, d_img)
             torch.cuda.synchronize()
             outs[var] = d_img.cpu().numpy().astype(np.float64)
+        cx.set_option(_lib.OPT_BP_VARIANT, 10)
+        cx.set_option(_lib.OPT_BP_WINDOW, 300)
+        d_img = torch.full(s.vol_shape, 7.25, dtype=torch.float32, device="cuda")
+        cx.bkproj_dev(g, d_f, d_img)
+        torch.cuda.synchronize()
+        outs["10w"] = d_img.cpu().numpy().astype(np.float64)
     ref = outs[100]
-    for var in (0, 1, 2, 3, 4, 5, 6, 7, 8, 9):
+    for var in (0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, "10w"):
         assert np.array_equal(outs[var] == 7.25, ref == 7.25)  # same untouched voxels
         rel = np.linalg.norm(outs[var] - ref) / np.linalg.norm(ref)
         print(f"{name}: variant {var} vs first form: rel diff {rel:.2e}")

@@ -108,3 +108,29 @@ def test_host_calls_pinned_equal_pageable(torch_mod):
         rel = np.linalg.norm(rec_pg[written] - img_pg[written]) / np.linalg.norm(img_pg[written])
         print(f"windowed vs one-pass host backprojection: rel diff {rel:.2e}")
         assert rel < 1e-6
+
+
+def test_host_bkproj_fifth_form(torch_mod):
+    """The host backprojection accumulates ~2048-view windows; with the fifth form each
+    window's cell records are built for that window only."""
+    torch = torch_mod
+    import ctrecon_b200 as ct
+    from ctrecon_b200 import _lib
+    from ctrecon_b200.geometry import config
+    s = config("c1")
+    with ct.Context(0) as cx:
+        d = torch.empty(s.proj_shape, dtype=torch.float32, device="cuda")
+        cx.phantom_dev(s.geom_struct(), s.ellipsoids(), d)
+        torch.cuda.synchronize()
+        f = cx.filter_host(ct.scan_filter_params(s), d.cpu().numpy().astype(np.float64))
+        imgs = {}
+        for var in (100, 10):
+            cx.set_option(_lib.OPT_BP_VARIANT, var)
+            img = np.full(s.vol_shape, 7.25)
+            cx.bkproj_host(s.geom_struct(), f, img)
+            imgs[var] = img
+    written = imgs[100] != 7.25
+    assert np.array_equal(written, imgs[10] != 7.25)
+    rel = np.linalg.norm(imgs[10][written] - imgs[100][written]) / np.linalg.norm(imgs[100][written])
+    print(f"host backprojection, fifth form vs first form: rel diff {rel:.2e}")
+    assert rel < 1e-6
