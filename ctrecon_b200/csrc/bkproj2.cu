@@ -574,8 +574,11 @@ void bp4_caps(BPPlan& plan) {
                         vmax = std::max(vmax, std::max(va, vb));
                     }
                     if (!ok) continue;
-                    const int u0 = (int)std::floor(umin) - 1, u1 = (int)std::floor(umax) + 2;
-                    const int v0 = (int)std::floor(vmin) - 1, v1 = (int)std::floor(vmax) + 2;
+                    // the kernels' footprint (bp_tile4.cuh), a little wider
+                    const int u0 = (int)std::floor(umin - 2 * kFootMargin);
+                    const int u1 = (int)std::floor(umax + 2 * kFootMargin) + 1;
+                    const int v0 = (int)std::floor(vmin - 2 * kFootMargin);
+                    const int v1 = (int)std::floor(vmax + 2 * kFootMargin) + 1;
                     const int W = u1 - u0 + 1, H = v1 - v0 + 1;
                     if (u0 < 0 || u1 > g.YL - 1 || v0 < 0 || v1 > g.ZL - 1 || W > 64) continue;
                     max_cells = std::max(max_cells, (W - 1) * (H - 1));

@@ -59,6 +59,9 @@ __device__ __forceinline__ float4 cell_record(float t00, float t01, float t10, f
                        h1 - h0);
 }
 
+// slack of the footprint bounds, in detector cells
+constexpr float kFootMargin = 0.0625f;
+
 struct Caps4 {
     int cells;  // cell records per staged view (multiple of 4)
     int raw;    // raw floats per staged view (multiple of 4)
@@ -192,8 +195,17 @@ __device__ __forceinline__ uint32_t tile4(const BPParams& kp, const float* __res
                     f = Foot3{0, 0, -2, 0};
                     if (ok && fabsf(umin) < 1048576.f && fabsf(umax) < 1048576.f &&
                         fabsf(vmin) < 1048576.f && fabsf(vmax) < 1048576.f) {
-                        const int u0 = (int)floorf(umin) - 1, u1 = (int)floorf(umax) + 2;
-                        const int v0 = (int)floorf(vmin) - 1, v1 = (int)floorf(vmax) + 2;
+                        // a voxel at detector position (u, v) reads the cell whose corner is
+                        // (rint(u - 1/2), rint(v - 1/2)), i.e. (floor(u), floor(v)) or one less
+                        // at integer positions; u and v are linear-fractional in the voxel
+                        // coordinates, so their extremes over the tile are at the corners;
+                        // kFootMargin covers the FP32 rounding between these corner values and
+                        // the consumers' per-voxel ones (~1e-3 cells at most). Samples
+                        // [u0, u1] x [v0, v1], cells [u0, u1) x [v0, v1).
+                        const int u0 = (int)floorf(umin - kFootMargin);
+                        const int u1 = (int)floorf(umax + kFootMargin) + 1;
+                        const int v0 = (int)floorf(vmin - kFootMargin);
+                        const int v1 = (int)floorf(vmax + kFootMargin) + 1;
                         const int W = u1 - u0 + 1, H = v1 - v0 + 1;
                         if (u0 >= 0 && u1 <= YL - 1 && v0 >= 0 && v1 <= ZL - 1 &&
                             (REC || (W <= 64 && W * H <= rcap)) && (W - 1) * (H - 1) <= ccap)
@@ -308,6 +320,61 @@ __device__ __forceinline__ uint32_t tile4(const BPParams& kp, const float* __res
         const float z0 = zc[zb];
         const float dzf = kp.dzf;
         const float HalfYm = HalfY - 0.5f, HalfZm = HalfZ - 0.5f;
+        // Slices 4h .. 4h + 3 form group h. A group takes the unweighted path for a block when
+        // every voxel of the group, in every lane of the warp, has weight 1 at all the block's
+        // views: [gflo[h], gfhi[h]] is that warp-wide view range (empty if any voxel of the
+        // group has no PI interval). Deciding per group halves the views whose weights are
+        // tested: the PI ranges of a column's slices are shifted against each other.
+        constexpr int GS = 4, NG = TZ / GS;
+        int gflo[NG], gfhi[NG];
+#pragma unroll
+        for (int h = 0; h < NG; ++h) {
+            int lo = INT_MIN, hi = INT_MAX;
+            bool ok = col_ok;
+#pragma unroll
+            for (int k = h * GS; k < (h + 1) * GS; ++k) {
+                ok = ok && vr.bi[k] != kPiInvalid;
+                if (ok) {
+                    lo = max(lo, vr.bi[k] + 2);  // past both B-side ramp views
+                    hi = min(hi, vr.ti[k] - 1);  // before both T-side ramp views
+                }
+            }
+            if (!ok) { lo = INT_MAX; hi = INT_MIN; }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                lo = max(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+                hi = min(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+            }
+            gflo[h] = lo;
+            gfhi[h] = hi;
+        }
+        // one voxel's update from cell records, weighted (w) or not
+        auto cell_update = [&](int k, float dz0, float kv, float r2, float a, uint32_t W16,
+                               uint32_t cbase) {
+            const float dz = fmaf((float)k, dzf, dz0);
+            const float v = fmaf(dz, kv, HalfZm);  // v - 1/2
+            const float rinv = rsqrt_approx(fmaf(dz, dz, r2));
+            const float tv = v + kMagic;
+            const float b = v - (tv - kMagic);
+            const float4 q = lds128((uint32_t)__float_as_int(tv) * W16 + cbase);
+            acc[k] = fmaf(fmaf(b, fmaf(a, q.w, q.z), fmaf(a, q.y, q.x)), rinv, acc[k]);
+        };
+        auto cell_update_w = [&](int k, int p, float dz0, float kv, float r2, float a,
+                                 uint32_t W16, uint32_t cbase) {
+            const int d0 = p - vr.bi[k];
+            const int d1 = vr.ti[k] + 1 - p;
+            if ((d0 | d1) < 0) return;
+            float w = 1.f;
+            if (d1 <= 1) w = ramp(vr.tf[k] + (float)(d1 - 1));
+            else if (d0 <= 1) w = ramp((float)d0 - vr.bf[k]);
+            const float dz = fmaf((float)k, dzf, dz0);
+            const float v = fmaf(dz, kv, HalfZm);
+            const float rinv = rsqrt_approx(fmaf(dz, dz, r2));
+            const float tv = v + kMagic;
+            const float b = v - (tv - kMagic);
+            const float4 q = lds128((uint32_t)__float_as_int(tv) * W16 + cbase);
+            acc[k] = fmaf(w * fmaf(b, fmaf(a, q.w, q.z), fmaf(a, q.y, q.x)), rinv, acc[k]);
+        };
         for (int ib = 0; ib < nblk; ++ib) {
             const uint32_t g = iter + ib, slot = g % S, use = g / S;
             if (!mbar_wait4(&sh.full[slot], use & 1, err, 12)) {
@@ -315,13 +382,14 @@ __device__ __forceinline__ uint32_t tile4(const BPParams& kp, const float* __res
                 break;
             }
             const int pb = pmin + ib * NB;
-            bool cells = true;
+            bool blk = pb + NB - 1 <= pmax;  // a whole block of views with cell records
 #pragma unroll
-            for (int j = 0; j < NB; ++j) cells = cells && (sh.foot[slot][j].W > 0);
-            const bool fast = __all_sync(0xffffffffu, vr.all_valid && pb >= vr.flo &&
-                                                       pb + NB - 1 <= vr.fhi &&
-                                                       pb + NB - 1 <= pmax && cells);
-            if (fast) {
+            for (int j = 0; j < NB; ++j) blk = blk && (sh.foot[slot][j].W > 0);
+            unsigned fm = 0;  // bit h: group h unweighted for the whole block (warp-uniform)
+#pragma unroll
+            for (int h = 0; h < NG; ++h)
+                fm |= (blk && pb >= gflo[h] && pb + NB - 1 <= gfhi[h]) ? 1u << h : 0u;
+            if (fm == (1u << NG) - 1) {
                 // every view of the block has cell records and weight 1 for all voxels of the
                 // warp: no per-view tests
 #pragma unroll
@@ -340,15 +408,7 @@ __device__ __forceinline__ uint32_t tile4(const BPParams& kp, const float* __res
                     const uint32_t W16 = (uint32_t)kw.y;
                     const uint32_t cbase = (uint32_t)__float_as_int(tu) * 16u + (uint32_t)kw.x;
 #pragma unroll
-                    for (int k = 0; k < TZ; ++k) {
-                        const float dz = fmaf((float)k, dzf, dz0);
-                        const float v = fmaf(dz, kv, HalfZm);  // v - 1/2
-                        const float rinv = rsqrt_approx(fmaf(dz, dz, r2));
-                        const float tv = v + kMagic;
-                        const float b = v - (tv - kMagic);
-                        const float4 q = lds128((uint32_t)__float_as_int(tv) * W16 + cbase);
-                        acc[k] = fmaf(fmaf(b, fmaf(a, q.w, q.z), fmaf(a, q.y, q.x)), rinv, acc[k]);
-                    }
+                    for (int k = 0; k < TZ; ++k) cell_update(k, dz0, kv, r2, a, W16, cbase);
                 }
             } else if (col_ok && wmin <= wmax && !(pb + NB - 1 < wmin || pb > wmax)) {
 #pragma unroll 1
@@ -372,23 +432,16 @@ __device__ __forceinline__ uint32_t tile4(const BPParams& kp, const float* __res
                         const uint32_t W16 = (uint32_t)kw.y;
                         const uint32_t cbase =
                             (uint32_t)__float_as_int(tu) * 16u + (uint32_t)kw.x;
-                        {
 #pragma unroll
-                            for (int k = 0; k < TZ; ++k) {
-                                const int d0 = p - vr.bi[k];
-                                const int d1 = vr.ti[k] + 1 - p;
-                                if ((d0 | d1) < 0) continue;
-                                float w = 1.f;
-                                if (d1 <= 1) w = ramp(vr.tf[k] + (float)(d1 - 1));
-                                else if (d0 <= 1) w = ramp((float)d0 - vr.bf[k]);
-                                const float dz = fmaf((float)k, dzf, dz0);
-                                const float v = fmaf(dz, kv, HalfZm);
-                                const float rinv = rsqrt_approx(fmaf(dz, dz, r2));
-                                const float tv = v + kMagic;
-                                const float b = v - (tv - kMagic);
-                                const float4 q = lds128((uint32_t)__float_as_int(tv) * W16 + cbase);
-                                acc[k] = fmaf(w * fmaf(b, fmaf(a, q.w, q.z), fmaf(a, q.y, q.x)),
-                                              rinv, acc[k]);
+                        for (int h = 0; h < NG; ++h) {
+                            if (fm & (1u << h)) {
+#pragma unroll
+                                for (int k = h * GS; k < (h + 1) * GS; ++k)
+                                    cell_update(k, dz0, kv, r2, a, W16, cbase);
+                            } else {
+#pragma unroll
+                                for (int k = h * GS; k < (h + 1) * GS; ++k)
+                                    cell_update_w(k, p, dz0, kv, r2, a, W16, cbase);
                             }
                         }
                     } else {
