@@ -261,7 +261,8 @@ Status launch_bkproj_f32(ctrecon_ctx* ctx, cudaStream_t s, BPPlan& plan, const f
     if (!ctx->ws_flag.ptr) return make_status(CTRECON_ERR_INTERNAL, "device error word not set up");
     if (variant >= 10)
         return launch_bkproj_v5<float>(variant, s, plan, d_fproj, d_pitab, d_image,
-                                       ctx->ws_flag.as<int>(), ctx->ws_rec, ctx->opt_bp_window);
+                                       ctx->ws_flag.as<int>(), ctx->ws_rec, ctx->ws_boxmaps,
+                                       ctx->boxmap_key, ctx->opt_bp_window);
     return launch_bkproj_v2<float>(variant, s, plan, d_fproj, d_pitab, d_image,
                                    ctx->ws_flag.as<int>());
 }
@@ -273,7 +274,8 @@ Status launch_bkproj_f64out(ctrecon_ctx* ctx, cudaStream_t s, BPPlan& plan,
     if (!ctx->ws_flag.ptr) return make_status(CTRECON_ERR_INTERNAL, "device error word not set up");
     if (variant >= 10)
         return launch_bkproj_v5<double>(variant, s, plan, d_fproj, d_pitab, d_image,
-                                        ctx->ws_flag.as<int>(), ctx->ws_rec, ctx->opt_bp_window);
+                                        ctx->ws_flag.as<int>(), ctx->ws_rec, ctx->ws_boxmaps,
+                                        ctx->boxmap_key, ctx->opt_bp_window);
     return launch_bkproj_v2<double>(variant, s, plan, d_fproj, d_pitab, d_image,
                                     ctx->ws_flag.as<int>());
 }

@@ -16,9 +16,13 @@
 // Also the persistent batched kernel (either form) behind the batch API.
 #include "bp_tile4.cuh"
 
+#include <cudaTypedefs.h>
+
 #include <algorithm>
 #include <climits>
 #include <cmath>
+#include <cstring>
+#include <vector>
 
 namespace ctr {
 
@@ -303,18 +307,18 @@ k_bkproj4(BPParams kp, const float* __restrict__ fproj, const PiRecord* __restri
 }
 
 // Fifth form: the fourth form's consumers fed from the global cell records (k_cell_records) by
-// one producer warp with bulk copies. Three CTAs per SM.
+// one producer warp, one tensor copy per view (tmaps: the box table of bp_tile4.cuh).
 template <int NB, int S, int MINB, typename OutT>
 __global__ void __launch_bounds__(32 * 9, MINB)
 k_bkproj5(BPParams kp, const float* __restrict__ fproj, const PiRecord* __restrict__ pit,
           const float4* __restrict__ views, const float* __restrict__ xyz,
-          OutT* __restrict__ image, Caps4 caps, int* err, const float4* __restrict__ rec,
+          OutT* __restrict__ image, Caps4 caps, int* err, const CUtensorMap* __restrict__ tmaps,
           int rec_p0) {
     extern __shared__ __align__(128) unsigned char dyn5[];
     __shared__ Shared4<NB, S, 1> sh;
     tile4_init(sh);
     tile4<NB, S, 1, true, OutT>(kp, fproj, pit, views, xyz, image, blockIdx.x, blockIdx.y,
-                                blockIdx.z, sh, dyn5, caps, err, 0u, rec, rec_p0);
+                                blockIdx.z, sh, dyn5, caps, err, 0u, tmaps, rec_p0);
 }
 
 // The cell records of views [p0, p0 + nviews): rec[v][r][c] = cell_record of the samples
@@ -547,7 +551,7 @@ void bp4_caps(BPPlan& plan) {
     auto zc = [&](int i) { return (i - g.ZC) * g.dz; };
     const double R = g.ScanR, DdU = g.StdDis / g.DeltaU, DdV = g.StdDis / g.DeltaV;
     const double PI = kRefPi;
-    int max_cells = 0, max_raw = 0;
+    int max_cells = 0, max_raw = 0, max_box = 0;
     for (int tx = 0; tx < ntx; tx += sx)
         for (int ty = 0; ty < nty; ty += sy)
             for (int tz = 0; tz < ntz; tz += sz) {
@@ -583,6 +587,7 @@ void bp4_caps(BPPlan& plan) {
                     if (u0 < 0 || u1 > g.YL - 1 || v0 < 0 || v1 > g.ZL - 1 || W > 64) continue;
                     max_cells = std::max(max_cells, (W - 1) * (H - 1));
                     max_raw = std::max(max_raw, W * H);
+                    max_box = std::max(max_box, ((W - 1 + 3) & ~3) * ((H - 1 + 1) & ~1));
                 }
             }
     auto cap = [](int v, int lo, int hi) {
@@ -592,6 +597,7 @@ void bp4_caps(BPPlan& plan) {
     };
     plan.caps_cells = cap(max_cells, 64, 1024);
     plan.caps_raw = cap(max_raw, 96, 1536);
+    plan.caps_box = cap(max_box, 64, kBoxMaxW * kBoxMaxH);
 }
 
 // Capacities that keep a fourth-form CTA within `budget` bytes of dynamic shared memory
@@ -631,21 +637,22 @@ constexpr size_t smem5_budget(int minb) { return minb >= 3 ? 72 * 1024 : 108 * 1
 
 template <int NB, int S, int MINB, typename OutT>
 static Status launch_v5(cudaStream_t s, BPPlan& plan, const BPParams& kp, const float* d_fproj,
-                        const PiRecord* d_pitab, OutT* d_image, int* err, const float4* rec,
-                        int rec_p0) {
+                        const PiRecord* d_pitab, OutT* d_image, int* err,
+                        const CUtensorMap* tmaps, int rec_p0) {
     bp4_caps(plan);
-    int cells = plan.caps_cells;
-    const size_t budget = smem5_budget(MINB);
+    // slots of whole boxes, a multiple of 8 records (128-byte aligned slots)
+    int cells = (plan.caps_box + 7) / 8 * 8;
+    const size_t budget = smem5_budget(MINB) - 128;
     if ((size_t)S * NB * cells * 16 > budget)
-        cells = std::max(64, (int)(budget / ((size_t)S * NB * 16)) / 4 * 4);
+        cells = std::max(64, (int)(budget / ((size_t)S * NB * 16)) / 8 * 8);
     const Caps4 caps{cells, 0};
     dim3 grid((kp.NX + kTXY2 - 1) / kTXY2, (kp.NY + kTXY2 - 1) / kTXY2, (kp.NZ + 7) / 8);
-    const size_t smem = tile4_smem_bytes<NB, S, 1>(caps);
+    const size_t smem = tile4_smem_bytes<NB, S, 1>(caps) + 128;
     CTR_CUDA(cudaFuncSetAttribute(k_bkproj5<NB, S, MINB, OutT>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k_bkproj5<NB, S, MINB, OutT><<<grid, 32 * 9, smem, s>>>(
         kp, d_fproj, d_pitab, plan.views.as<float4>(), plan.xyz.as<float>(), d_image, caps, err,
-        rec, rec_p0);
+        tmaps, rec_p0);
     CTR_CUDA(cudaGetLastError());
     return Status::Ok();
 }
@@ -655,10 +662,47 @@ static Status launch_v5(cudaStream_t s, BPPlan& plan, const BPParams& kp, const 
 // of at most max_views views when that is > 0);
 // with more than one window the valid voxels are zeroed first (or kept, when the plan
 // accumulates) and every window adds its sum.
+// The box table over records of `nviews` views at `rec`: a tensor map per (bw, bh) box with
+// bw = 4, 8 .. kBoxMaxW and bh = 2, 4 .. kBoxMaxH cells, zeroed where the box exceeds the
+// detector (the kernel never selects those). Uploaded to `maps` only when it changed.
+static Status upload_box_maps(cudaStream_t s, DevBuf& maps, BoxMapKey& key, const float4* rec,
+                              int RW, int RH, int nviews) {
+    const BoxMapKey want{(const void*)rec, RW, RH, nviews};
+    if (maps.ptr && key == want) return Status::Ok();
+    auto enc = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(tensor_map_encoder());
+    if (!enc) return make_status(CTRECON_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+    constexpr int n = kBoxSteps * (kBoxMaxH / 2);
+    std::vector<CUtensorMap> host(n);
+    std::memset(host.data(), 0, sizeof(CUtensorMap) * n);
+    cuuint64_t dims[4] = {4, (cuuint64_t)RW, (cuuint64_t)RH, (cuuint64_t)nviews};
+    cuuint64_t strides[3] = {16, (cuuint64_t)RW * 16, (cuuint64_t)RW * RH * 16};
+    cuuint32_t estr[4] = {1, 1, 1, 1};
+    for (int ih = 0; ih < kBoxMaxH / 2; ++ih)
+        for (int iw = 0; iw < kBoxSteps; ++iw) {
+            const int bw = 4 * (iw + 1), bh = 2 * (ih + 1);
+            if (bw > RW || bh > RH) continue;
+            cuuint32_t box[4] = {4, (cuuint32_t)bw, (cuuint32_t)bh, 1};
+            CUresult r = enc(&host[iw + kBoxSteps * ih], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4,
+                             const_cast<float4*>(rec), dims, strides, box, estr,
+                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+            if (r != CUDA_SUCCESS)
+                return make_status(CTRECON_ERR_CUDA, "cuTensorMapEncodeTiled failed for the "
+                                                     "cell records (" + std::to_string((int)r) + ")");
+        }
+    CTR_TRY(maps.ensure(sizeof(CUtensorMap) * n, "cell-record box maps"));
+    // pageable source: staged by the driver before the call returns, copied in stream order
+    CTR_CUDA(cudaMemcpyAsync(maps.ptr, host.data(), sizeof(CUtensorMap) * n,
+                             cudaMemcpyHostToDevice, s));
+    key = want;
+    return Status::Ok();
+}
+
 template <typename OutT>
 Status launch_bkproj_v5(int variant, cudaStream_t s, BPPlan& plan, const float* d_fproj,
                         const PiRecord* d_pitab, OutT* d_image, int* err, DevBuf& recbuf,
-                        int max_views) {
+                        DevBuf& maps, BoxMapKey& mkey, int max_views) {
     const BPParams& kp0 = plan.kp;
     const int RW = kp0.YL - 1, RH = kp0.ZL - 1;
     const size_t plane = (size_t)RW * RH * sizeof(float4);
@@ -669,6 +713,8 @@ Status launch_bkproj_v5(int variant, cudaStream_t s, BPPlan& plan, const float* 
     if (max_views > 0) per = std::min(per, max_views);
     const int nwin = (nv_all + per - 1) / per;
     CTR_TRY(recbuf.ensure((size_t)std::min(per, nv_all) * plane, "cell records"));
+    CTR_TRY(upload_box_maps(s, maps, mkey, recbuf.as<float4>(), RW, RH, std::min(per, nv_all)));
+    const CUtensorMap* tmaps = maps.as<CUtensorMap>();
     BPParams kp = kp0;
     if (nwin > 1 && !kp0.accum) {
         const size_t n = (size_t)kp0.NX * kp0.NY * kp0.NZ;
@@ -688,17 +734,17 @@ Status launch_bkproj_v5(int variant, cudaStream_t s, BPPlan& plan, const float* 
         kp.win1 = b;
         Status st;
         switch (variant) {
-        case 11: st = launch_v5<4, 4, 2, OutT>(s, plan, kp, d_fproj, d_pitab, d_image, err, rec, a); break;
-        case 12: st = launch_v5<8, 2, 2, OutT>(s, plan, kp, d_fproj, d_pitab, d_image, err, rec, a); break;
-        default: st = launch_v5<4, 3, 3, OutT>(s, plan, kp, d_fproj, d_pitab, d_image, err, rec, a); break;
+        case 11: st = launch_v5<4, 4, 2, OutT>(s, plan, kp, d_fproj, d_pitab, d_image, err, tmaps, a); break;
+        case 12: st = launch_v5<8, 2, 2, OutT>(s, plan, kp, d_fproj, d_pitab, d_image, err, tmaps, a); break;
+        default: st = launch_v5<4, 3, 3, OutT>(s, plan, kp, d_fproj, d_pitab, d_image, err, tmaps, a); break;
         }
         CTR_TRY(st);
     }
     return Status::Ok();
 }
 
-template Status launch_bkproj_v5<float>(int, cudaStream_t, BPPlan&, const float*, const PiRecord*, float*, int*, DevBuf&, int);
-template Status launch_bkproj_v5<double>(int, cudaStream_t, BPPlan&, const float*, const PiRecord*, double*, int*, DevBuf&, int);
+template Status launch_bkproj_v5<float>(int, cudaStream_t, BPPlan&, const float*, const PiRecord*, float*, int*, DevBuf&, DevBuf&, BoxMapKey&, int);
+template Status launch_bkproj_v5<double>(int, cudaStream_t, BPPlan&, const float*, const PiRecord*, double*, int*, DevBuf&, DevBuf&, BoxMapKey&, int);
 
 template Status launch_bkproj_v2<float>(int, cudaStream_t, BPPlan&, const float*, const PiRecord*, float*, int*);
 template Status launch_bkproj_v2<double>(int, cudaStream_t, BPPlan&, const float*, const PiRecord*, double*, int*);

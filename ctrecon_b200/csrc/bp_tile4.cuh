@@ -24,6 +24,8 @@
 #include "bp_tile3.cuh"
 #include "tc_util.cuh"
 
+#include <cuda.h>
+
 namespace ctr {
 namespace bp {
 
@@ -40,6 +42,19 @@ __device__ __forceinline__ bool mbar_wait4(uint64_t* bar, uint32_t parity, int* 
 __device__ __forceinline__ void mbar_expect_tx4(uint64_t* bar, uint32_t bytes) {
     asm volatile("mbarrier.expect_tx.relaxed.cta.shared::cta.b64 [%0], %1;"
                  ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+// Fifth form: the footprint of a view is brought in by one tensor copy of a box of bw x bh cell
+// records (bw a multiple of 4 up to kBoxMaxW, bh a multiple of 2 up to kBoxMaxH), from a table
+// of tensor maps over the records [views][ZL - 1][YL - 1][4 floats] that differ only in the
+// box: map index (bw / 4 - 1) + kBoxSteps * (bh / 2 - 1).
+constexpr int kBoxMaxW = 64, kBoxMaxH = 32, kBoxSteps = 16;
+__device__ __forceinline__ void tma_load_cells(uint32_t dst, const void* map, int u, int v,
+                                               int view, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(dst),
+        "l"((uint64_t)map), "r"(0), "r"(u), "r"(v), "r"(view), "r"(smem_addr(bar))
+        : "memory");
 }
 // global -> shared bulk copy (16-byte aligned addresses, size a multiple of 16) completing
 // `bytes` of the barrier's transaction count
@@ -110,12 +125,15 @@ __device__ __forceinline__ uint32_t tile4(const BPParams& kp, const float* __res
                                           const float* __restrict__ xyz, OutT* __restrict__ image,
                                           int bx, int by, int bz, Shared4<NB, S, PW>& sh,
                                           unsigned char* dyn, Caps4 caps, int* err,
-                                          uint32_t iter, const float4* __restrict__ rec = nullptr,
+                                          uint32_t iter, const CUtensorMap* __restrict__ tmaps = nullptr,
                                           int rec_p0 = 0) {
     constexpr int TZ = 8;
     const int ccap = caps.cells, rcap = caps.raw;
-    float4* cellbuf = reinterpret_cast<float4*>(dyn);                          // S * NB * ccap
-    float* raw = reinterpret_cast<float*>(dyn + (size_t)S * NB * ccap * 16);   // 2 * NB * rcap
+    // cell records S * NB * ccap (the fifth form's tensor copies want 128-byte aligned slots:
+    // ccap is a multiple of 8 and the base rounded up), then 2 * NB * rcap raw floats
+    if constexpr (REC) dyn += (128u - (smem_addr(dyn) & 127u)) & 127u;
+    float4* cellbuf = reinterpret_cast<float4*>(dyn);
+    float* raw = reinterpret_cast<float*>(dyn + (size_t)S * NB * ccap * 16);
     const uint32_t cell_s = smem_addr(cellbuf);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const bool consumer = warp < 8;
@@ -245,9 +263,11 @@ __device__ __forceinline__ uint32_t tile4(const BPParams& kp, const float* __res
             }
         };
         if constexpr (REC) {
-            // fifth form: footprint rows copied from the global cell records
-            const int RW = YL - 1;
-            const size_t plane = (size_t)(ZL - 1) * RW;
+            // fifth form: one tensor copy per view from the global cell records; the footprint
+            // is widened to the copied box (its origin moved in so that the box stays on the
+            // detector), which the consumers then address like any footprint
+            static_assert(PW == 1, "the fifth form has one producer warp");
+            const int RW = YL - 1, RH = ZL - 1;
             float4 gnext = view_of(0);
             for (int ib = 0; ib < nblk; ++ib) {
                 const float4 gv = gnext;
@@ -258,18 +278,30 @@ __device__ __forceinline__ uint32_t tile4(const BPParams& kp, const float* __res
                     sh.s_abort = 1;
                     break;
                 }
-                for (int j = pw; j < NB; j += PW) {
-                    const Foot3 f = sh.pfoot[ib & 1][j];
-                    publish(ib, slot, j, f);
-                    if (f.W <= 0) continue;
-                    const uint32_t rowb = (uint32_t)(f.W - 1) * 16u;
-                    const float4* src = rec + (size_t)(pmin + ib * NB + j - rec_p0) * plane +
-                                        (size_t)f.v0 * RW + f.u0;
-                    const uint32_t dst = cell_s + (uint32_t)((slot * NB + j) * ccap) * 16u;
-                    for (int r = lane; r < f.H - 1; r += 32) {
-                        mbar_expect_tx4(&sh.full[slot], rowb);
-                        bulk_g2s(dst + (uint32_t)r * rowb, src + (size_t)r * RW, rowb,
-                                 &sh.full[slot]);
+                if (vlane) {
+                    Foot3 f = sh.pfoot[ib & 1][jl];
+                    int box = -1, bw = 0, bh = 0;
+                    if (f.W > 0) {
+                        bw = (f.W - 1 + 3) & ~3;
+                        bh = (f.H - 1 + 1) & ~1;
+                        if (bw <= min(kBoxMaxW, RW) && bh <= min(kBoxMaxH, RH) && bw * bh <= ccap) {
+                            f = Foot3{min(f.u0, RW - bw), min(f.v0, RH - bh), bw + 1, bh + 1};
+                            box = (bw / 4 - 1) + kBoxSteps * (bh / 2 - 1);
+                        } else {
+                            f.W = -2;
+                        }
+                    }
+                    sh.foot[slot][jl] = f;
+                    sh.vg[slot][jl] = sh.pvg[ib & 1][jl];
+                    const uint32_t W16 = (uint32_t)(f.W - 1) * 16u;
+                    const uint32_t dst = cell_s + (uint32_t)((slot * NB + jl) * ccap) * 16u;
+                    sh.kw[slot][jl] = make_int2((int)(dst - (uint32_t)(kMagicBits + f.u0) * 16u -
+                                                      (uint32_t)(kMagicBits + f.v0) * W16),
+                                                (int)W16);
+                    if (box >= 0) {
+                        mbar_expect_tx4(&sh.full[slot], (uint32_t)(bw * bh) * 16u);
+                        tma_load_cells(dst, tmaps + box, f.u0, f.v0,
+                                       pmin + ib * NB + jl - rec_p0, &sh.full[slot]);
                     }
                 }
                 mbar_arrive4(&sh.full[slot]);

@@ -284,16 +284,7 @@ k_hilbert_tc(const __grid_constant__ CUtensorMap tA0, const __grid_constant__ CU
 
 // ---- host side -------------------------------------------------------------------------------
 PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-    if (!fn) {
-        cudaDriverEntryPointQueryResult q;
-        void* ptr = nullptr;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) ==
-                cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(ptr);
-    }
-    return fn;
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(tensor_map_encoder());
 }
 
 Status make_map(CUtensorMap* m, const void* base, bool bf16, uint64_t inner, uint64_t rows,
@@ -424,6 +415,19 @@ Status launch_hilbert_tc(ctrecon_ctx* ctx, cudaStream_t s, FilterPlan& plan, con
     }
     CTR_CUDA(cudaGetLastError());
     return Status::Ok();
+}
+
+void* tensor_map_encoder() {
+    static void* fn = nullptr;
+    if (!fn) {
+        cudaDriverEntryPointQueryResult q;
+        void* ptr = nullptr;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = ptr;
+    }
+    return fn;
 }
 
 }  // namespace ctr

@@ -136,6 +136,15 @@ struct BPPlan {
     DevBuf views;   // float4 per view: cos, sin, source z, 0
     DevBuf xyz;     // float voxel coordinates x[NX], y[NY], z[NZ]
     int caps_cells = 0, caps_raw = 0;  // fourth-form staging capacities (bp4_caps)
+    int caps_box = 0;                  // fifth form: cell records per staged view (boxes)
+};
+// the cell records and view count a box-map table was made for
+struct BoxMapKey {
+    const void* rec = nullptr;
+    int RW = 0, RH = 0, nviews = 0;
+    bool operator==(const BoxMapKey& o) const {
+        return rec == o.rec && RW == o.RW && RH == o.RH && nviews == o.nviews;
+    }
 };
 // Sizes the fourth form's staging capacities of a plan (once).
 void bp4_caps(BPPlan& plan);
@@ -204,6 +213,8 @@ struct ctrecon_ctx {
     ctr::DevBuf ws_ell;      // phantom ellipsoids
     ctr::DevBuf ws_flag;     // device error word
     ctr::DevBuf ws_rec;      // cell records of the fifth-form backprojection (one window)
+    ctr::DevBuf ws_boxmaps;  // tensor maps over ws_rec (one per box shape)
+    ctr::BoxMapKey boxmap_key;
     ctr::PinetState pinet;   // learned PI-line initialiser
     // autotuner: backprojector form per geometry key (tune_key), with its time
     std::map<std::string, std::pair<int, float>> tune;
@@ -235,10 +246,12 @@ Status launch_zero_valid_f64(cudaStream_t s, const PiRecord* d_pitab, double* d_
 // at a time in `recbuf`, then the backprojection of those views.
 constexpr size_t kRecBudget = (size_t)8 << 30;
 constexpr int kMaxBPVariant = 12;
+// the driver's cuTensorMapEncodeTiled (nullptr when unavailable), hilbert_tc.cu
+void* tensor_map_encoder();
 template <typename OutT>
 Status launch_bkproj_v5(int variant, cudaStream_t s, BPPlan& plan, const float* d_fproj,
                         const PiRecord* d_pitab, OutT* d_image, int* err, DevBuf& recbuf,
-                        int max_views);
+                        DevBuf& maps, BoxMapKey& mkey, int max_views);
 Status launch_convert_f32_to_f64(cudaStream_t s, const float* in, double* out, size_t n);
 Status launch_average_into(cudaStream_t s, float* a, const float* b, size_t n);
 Status launch_phantom(cudaStream_t s, const BPGeom& g, const double* d_ell, int n_ell,
