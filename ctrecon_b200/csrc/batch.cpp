@@ -7,7 +7,8 @@
 // from a shared counter (scans sorted largest first, so the small ones fill the tail). With
 // use_graph, the first run is executed eagerly (it sizes every work buffer) and the second is
 // captured into a CUDA graph that later runs replay; the graph is re-captured when the buffer
-// pointers change.
+// pointers change. Scans on the fifth form (10..12) get their cell records written right
+// before the persistent launch (the records of all of a group's scans are held at once).
 #include "internal.h"
 
 #include <algorithm>
@@ -33,8 +34,13 @@ struct BatchGroup {
     int variant = 0;
     int nscans = 0;
     long long tiles = 0;
-    int cells = 0, raw = 0;  // fourth-form staging capacities (largest over the group)
+    int cells = 0, raw = 0;  // fourth-form staging capacities (largest over the group); the
+                             // fifth form's box capacity in `cells`
     DevBuf table, counter;
+    // fifth form: every scan's cell records and box-map table
+    DevBuf rec, maps;
+    struct RecJob { const float* fproj; void* rec; int P, YL, ZL; };
+    std::vector<RecJob> jobs;
 };
 
 struct ctrecon_batch {
@@ -75,6 +81,8 @@ static ctrecon_status bfinish(ctrecon_ctx* ctx, const Status& s) {
 static Status batch_backproject(ctrecon_batch* b, cudaStream_t s) {
     for (int g = 0; g < b->ngroups; ++g) {
         BatchGroup& G = *b->groups[g];
+        for (const auto& j : G.jobs)
+            CTR_TRY(launch_cell_records(s, j.fproj, j.rec, 0, j.P, j.YL, j.ZL));
         CTR_TRY(launch_bkproj_batch(G.variant, s, G.table.as<BatchScanDev>(), G.nscans, G.tiles,
                                     G.counter.as<unsigned long long>(), G.cells, G.raw,
                                     b->ctx->ws_flag.as<int>()));
@@ -115,6 +123,25 @@ static Status upload_scans(ctrecon_batch* b, cudaStream_t s, float* const* d_fpr
         std::vector<BatchScanDev> h;
         long long first = 0;
         int cells = 0, raw = 0;
+        const bool rec = G.variant >= 10;
+        size_t rec_bytes = 0;
+        if (rec)
+            for (int k = 0; k < b->n; ++k) {
+                const int i = b->order[k];
+                if (b->svar[i] != G.variant) continue;
+                const BPParams& kp = b->bplans[i]->kp;
+                rec_bytes += (size_t)kp.P * (kp.ZL - 1) * (kp.YL - 1) * 16;
+            }
+        std::vector<unsigned char> hmaps;
+        size_t rec_off = 0;
+        G.jobs.clear();
+        if (rec) {
+            CTR_TRY(G.rec.ensure(rec_bytes, "batch cell records"));
+            int ns = 0;
+            for (int k = 0; k < b->n; ++k) ns += b->svar[b->order[k]] == G.variant;
+            CTR_TRY(G.maps.ensure((size_t)ns * kBoxMaps * 128, "batch box maps"));
+            hmaps.assign((size_t)ns * kBoxMaps * 128, 0);
+        }
         for (int k = 0; k < b->n; ++k) {
             const int i = b->order[k];
             if (b->svar[i] != G.variant) continue;
@@ -127,11 +154,24 @@ static Status upload_scans(ctrecon_batch* b, cudaStream_t s, float* const* d_fpr
             d.xyz = bp.xyz.as<float>();
             d.image = d_image[i];
             d.first_tile = first;
+            d.tmaps = nullptr;
+            d.rec_p0 = 0;
             first += bkproj_batch_tiles(bp.kp, G.variant);
-            h.push_back(d);
             bp4_caps(bp);
-            cells = std::max(cells, bp.caps_cells);
-            raw = std::max(raw, bp.caps_raw);
+            if (rec) {
+                const BPParams& kp = bp.kp;
+                unsigned char* r = G.rec.as<unsigned char>() + rec_off;
+                rec_off += (size_t)kp.P * (kp.ZL - 1) * (kp.YL - 1) * 16;
+                const size_t mi = h.size() * kBoxMaps * 128;
+                CTR_TRY(encode_box_maps(hmaps.data() + mi, r, kp.YL - 1, kp.ZL - 1, kp.P));
+                d.tmaps = G.maps.as<unsigned char>() + mi;
+                G.jobs.push_back({d_fproj[i], r, kp.P, kp.YL, kp.ZL});
+                cells = std::max(cells, bp.caps_box);
+            } else {
+                cells = std::max(cells, bp.caps_cells);
+                raw = std::max(raw, bp.caps_raw);
+            }
+            h.push_back(d);
         }
         G.nscans = (int)h.size();
         G.tiles = first;
@@ -141,7 +181,10 @@ static Status upload_scans(ctrecon_batch* b, cudaStream_t s, float* const* d_fpr
         CTR_TRY(G.counter.ensure(64, "batch work counter"));
         CTR_CUDA(cudaMemcpyAsync(G.table.ptr, h.data(), h.size() * sizeof(BatchScanDev),
                                  cudaMemcpyHostToDevice, s));
-        CTR_CUDA(cudaStreamSynchronize(s));  // `h` is pageable and local
+        if (rec)
+            CTR_CUDA(cudaMemcpyAsync(G.maps.ptr, hmaps.data(), hmaps.size(),
+                                     cudaMemcpyHostToDevice, s));
+        CTR_CUDA(cudaStreamSynchronize(s));  // `h` and `hmaps` are pageable and local
     }
     return Status::Ok();
 }
@@ -158,7 +201,7 @@ ctrecon_status ctrecon_batch_create(ctrecon_ctx* ctx, int n_scans,
         auto b = std::make_unique<ctrecon_batch>();
         b->ctx = ctx;
         b->n = n_scans;
-        b->svar.assign(n_scans, (ctx->opt_bp_variant >= 0 && ctx->opt_bp_variant <= 9)
+        b->svar.assign(n_scans, (ctx->opt_bp_variant >= 0 && ctx->opt_bp_variant <= kMaxBPVariant)
                                     ? ctx->opt_bp_variant
                                     : kDefaultBPVariant);
         b->fp.assign(fp, fp + n_scans);
@@ -201,7 +244,7 @@ void ctrecon_batch_destroy(ctrecon_batch* b) {
 }
 
 ctrecon_status ctrecon_batch_set_variant(ctrecon_batch* b, int variant) {
-    if (!b || variant < 0 || variant > 9) return CTRECON_ERR_INVALID_ARGUMENT;
+    if (!b || variant < 0 || variant > kMaxBPVariant) return CTRECON_ERR_INVALID_ARGUMENT;
     for (int& v : b->svar) v = variant;
     b->key.clear();  // tile counts change: rebuild the scan tables and the graph
     return CTRECON_OK;
@@ -210,7 +253,7 @@ ctrecon_status ctrecon_batch_set_variant(ctrecon_batch* b, int variant) {
 ctrecon_status ctrecon_batch_set_variants(ctrecon_batch* b, const int* variants, int n) {
     if (!b || !variants || n != b->n) return CTRECON_ERR_INVALID_ARGUMENT;
     for (int i = 0; i < n; ++i)
-        if (variants[i] < 0 || variants[i] > 9) return CTRECON_ERR_INVALID_ARGUMENT;
+        if (variants[i] < 0 || variants[i] > kMaxBPVariant) return CTRECON_ERR_INVALID_ARGUMENT;
     b->svar.assign(variants, variants + n);
     b->key.clear();
     return CTRECON_OK;
@@ -305,7 +348,7 @@ ctrecon_status ctrecon_batch_tune(ctrecon_batch* b, void* stream, const float* c
                 return launch_bkproj_f32(ctx, s, *b->bplans[i],
                                          d_fproj[i], b->pitab.as<PiRecord>() + b->pit_off[i],
                                          d_image[i]);
-            }, 9);  // the forms the persistent batched kernel has
+            });
             if (!st.ok()) break;
             best[i] = r.best_variant;
             best_sum += r.best_ms;

@@ -383,6 +383,43 @@ k_bkproj4_batch(const BatchScanDev* __restrict__ scans, int n_scans, long long t
     }
 }
 
+// The persistent batched kernel of the fifth form: as k_bkproj4_batch, each scan's records
+// brought in through its own box-map table.
+template <int NB, int S, int MINB>
+__global__ void __launch_bounds__(32 * 9, MINB)
+k_bkproj5_batch(const BatchScanDev* __restrict__ scans, int n_scans, long long total_tiles,
+                unsigned long long* __restrict__ counter, Caps4 caps, int* err) {
+    extern __shared__ __align__(128) unsigned char dynb5[];
+    __shared__ Shared4<NB, S, 1> sh;
+    __shared__ BatchScanDev sc;
+    tile4_init(sh);
+    uint32_t iter = 0;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const long long item = (long long)atomicAdd(counter, 1ull);
+            sh.s_item = item;
+            if (item < total_tiles) {
+                int s = 0;
+                while (s + 1 < n_scans && scans[s + 1].first_tile <= item) ++s;
+                sc = scans[s];
+            }
+        }
+        __syncthreads();
+        const long long item = sh.s_item;
+        if (item >= total_tiles) break;
+        const int nxt = (sc.kp.NX + kTXY2 - 1) / kTXY2, nyt = (sc.kp.NY + kTXY2 - 1) / kTXY2;
+        const long long local = item - sc.first_tile;
+        const int bx = (int)(local % nxt);
+        const int by = (int)((local / nxt) % nyt);
+        const int bz = (int)(local / ((long long)nxt * nyt));
+        iter = tile4<NB, S, 1, true, float>(sc.kp, sc.fproj, sc.pit, sc.views, sc.xyz, sc.image,
+                                            bx, by, bz, sh, dynb5, caps, err, iter,
+                                            static_cast<const CUtensorMap*>(sc.tmaps),
+                                            sc.rec_p0);
+        if (sh.s_abort) break;  // uniform: read after the tile's closing barrier
+    }
+}
+
 // Many scans in one persistent launch: the CTAs pull tiles of all scans from one atomic
 // counter (largest-first order is the caller's choice of scan order), so uneven scans share
 // the GPU without tails between them.
@@ -469,10 +506,42 @@ static Status launch_batch4(cudaStream_t s, const BatchScanDev* d_scans, int n, 
     return Status::Ok();
 }
 
+// Shared memory per fifth-form CTA: three CTAs per SM (MINB 3) or two.
+constexpr size_t smem5_budget(int minb) { return minb >= 3 ? 72 * 1024 : 108 * 1024; }
+template <int NB, int S, int MINB>
+static Status launch_batch5(cudaStream_t s, const BatchScanDev* d_scans, int n, long long total,
+                            unsigned long long* d_counter, int box_cap, int* err) {
+    int cells = (box_cap + 7) / 8 * 8;
+    const size_t budget = smem5_budget(MINB) - 128;
+    if ((size_t)S * NB * cells * 16 > budget)
+        cells = std::max(64, (int)(budget / ((size_t)S * NB * 16)) / 8 * 8);
+    const Caps4 caps{cells, 0};
+    const size_t smem = tile4_smem_bytes<NB, S, 1>(caps) + 128;
+    const int threads = 32 * 9;
+    CTR_CUDA(cudaFuncSetAttribute(k_bkproj5_batch<NB, S, MINB>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int dev = 0, sms = 148, per_sm = 1;
+    CTR_CUDA(cudaGetDevice(&dev));
+    CTR_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    CTR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bkproj5_batch<NB, S, MINB>,
+                                                           threads, smem));
+    const long long grid = std::min<long long>(total, (long long)std::max(1, per_sm) * sms);
+    CTR_CUDA(cudaMemsetAsync(d_counter, 0, sizeof(unsigned long long), s));
+    if (grid > 0)
+        k_bkproj5_batch<NB, S, MINB><<<(unsigned)grid, threads, smem, s>>>(d_scans, n, total,
+                                                                         d_counter, caps, err);
+    CTR_CUDA(cudaGetLastError());
+    return Status::Ok();
+}
+
+// cells_cap: the group's fourth-form record capacity, or for 10..12 its box capacity
 Status launch_bkproj_batch(int variant, cudaStream_t s, const BatchScanDev* d_scans, int n,
                            long long total, unsigned long long* d_counter, int cells_cap,
                            int raw_cap, int* err) {
     switch (variant) {
+    case 10: return launch_batch5<4, 3, 3>(s, d_scans, n, total, d_counter, cells_cap, err);
+    case 11: return launch_batch5<4, 4, 2>(s, d_scans, n, total, d_counter, cells_cap, err);
+    case 12: return launch_batch5<8, 2, 2>(s, d_scans, n, total, d_counter, cells_cap, err);
     case 5: return launch_batch4<4, 2, 1>(s, d_scans, n, total, d_counter,
                                               caps_within(cells_cap, raw_cap, 4, 2, smem4_budget(1)), err);
     case 6: return launch_batch4<2, 4, 1>(s, d_scans, n, total, d_counter,
@@ -632,8 +701,6 @@ Status launch_bkproj_v2(int variant, cudaStream_t s, BPPlan& plan, const float* 
 }
 
 // ---- fifth form ------------------------------------------------------------------------
-// Shared memory per fifth-form CTA: three CTAs per SM (MINB 3) or two.
-constexpr size_t smem5_budget(int minb) { return minb >= 3 ? 72 * 1024 : 108 * 1024; }
 
 template <int NB, int S, int MINB, typename OutT>
 static Status launch_v5(cudaStream_t s, BPPlan& plan, const BPParams& kp, const float* d_fproj,
@@ -665,15 +732,12 @@ static Status launch_v5(cudaStream_t s, BPPlan& plan, const BPParams& kp, const 
 // The box table over records of `nviews` views at `rec`: a tensor map per (bw, bh) box with
 // bw = 4, 8 .. kBoxMaxW and bh = 2, 4 .. kBoxMaxH cells, zeroed where the box exceeds the
 // detector (the kernel never selects those). Uploaded to `maps` only when it changed.
-static Status upload_box_maps(cudaStream_t s, DevBuf& maps, BoxMapKey& key, const float4* rec,
-                              int RW, int RH, int nviews) {
-    const BoxMapKey want{(const void*)rec, RW, RH, nviews};
-    if (maps.ptr && key == want) return Status::Ok();
+Status encode_box_maps(void* out, const void* rec, int RW, int RH, int nviews) {
+    static_assert(kBoxMaps == kBoxSteps * (kBoxMaxH / 2), "box table size");
     auto enc = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(tensor_map_encoder());
     if (!enc) return make_status(CTRECON_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
-    constexpr int n = kBoxSteps * (kBoxMaxH / 2);
-    std::vector<CUtensorMap> host(n);
-    std::memset(host.data(), 0, sizeof(CUtensorMap) * n);
+    CUtensorMap* host = static_cast<CUtensorMap*>(out);
+    std::memset(host, 0, sizeof(CUtensorMap) * kBoxMaps);
     cuuint64_t dims[4] = {4, (cuuint64_t)RW, (cuuint64_t)RH, (cuuint64_t)nviews};
     cuuint64_t strides[3] = {16, (cuuint64_t)RW * 16, (cuuint64_t)RW * RH * 16};
     cuuint32_t estr[4] = {1, 1, 1, 1};
@@ -683,7 +747,7 @@ static Status upload_box_maps(cudaStream_t s, DevBuf& maps, BoxMapKey& key, cons
             if (bw > RW || bh > RH) continue;
             cuuint32_t box[4] = {4, (cuuint32_t)bw, (cuuint32_t)bh, 1};
             CUresult r = enc(&host[iw + kBoxSteps * ih], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4,
-                             const_cast<float4*>(rec), dims, strides, box, estr,
+                             const_cast<void*>(rec), dims, strides, box, estr,
                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                              CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
@@ -691,6 +755,25 @@ static Status upload_box_maps(cudaStream_t s, DevBuf& maps, BoxMapKey& key, cons
                 return make_status(CTRECON_ERR_CUDA, "cuTensorMapEncodeTiled failed for the "
                                                      "cell records (" + std::to_string((int)r) + ")");
         }
+    return Status::Ok();
+}
+
+Status launch_cell_records(cudaStream_t s, const float* d_fproj, void* rec, int p0, int nviews,
+                           int YL, int ZL) {
+    if (nviews <= 0) return Status::Ok();
+    dim3 g((YL - 1 + 127) / 128, ZL - 1, (unsigned)std::min(nviews, 65535));
+    k_cell_records<<<g, 128, 0, s>>>(d_fproj, static_cast<float4*>(rec), p0, nviews, YL, ZL);
+    CTR_CUDA(cudaGetLastError());
+    return Status::Ok();
+}
+
+static Status upload_box_maps(cudaStream_t s, DevBuf& maps, BoxMapKey& key, const float4* rec,
+                              int RW, int RH, int nviews) {
+    const BoxMapKey want{(const void*)rec, RW, RH, nviews};
+    if (maps.ptr && key == want) return Status::Ok();
+    constexpr int n = kBoxMaps;
+    std::vector<CUtensorMap> host(n);
+    CTR_TRY(encode_box_maps(host.data(), rec, RW, RH, nviews));
     CTR_TRY(maps.ensure(sizeof(CUtensorMap) * n, "cell-record box maps"));
     // pageable source: staged by the driver before the call returns, copied in stream order
     CTR_CUDA(cudaMemcpyAsync(maps.ptr, host.data(), sizeof(CUtensorMap) * n,
@@ -727,9 +810,7 @@ Status launch_bkproj_v5(int variant, cudaStream_t s, BPPlan& plan, const float* 
     for (int w = 0; w < nwin; ++w) {
         const int a = w0 + w * per, b = std::min(w1, a + per - 1);
         const int nv = b - a + 1;
-        dim3 g((RW + 127) / 128, RH, (unsigned)std::min(nv, 65535));
-        k_cell_records<<<g, 128, 0, s>>>(d_fproj, rec, a, nv, kp0.YL, kp0.ZL);
-        CTR_CUDA(cudaGetLastError());
+        CTR_TRY(launch_cell_records(s, d_fproj, rec, a, nv, kp0.YL, kp0.ZL));
         kp.win0 = a;
         kp.win1 = b;
         Status st;

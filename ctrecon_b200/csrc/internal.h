@@ -170,6 +170,10 @@ struct BatchScanDev {
     const float* xyz;
     float* image;
     long long first_tile;
+    // fifth form: the scan's box-map table (CUtensorMap[256] over its cell records) and the
+    // view of its first record plane
+    const void* tmaps;
+    int rec_p0;
 };
 
 // The learned PI-line initialiser (pinet.cu): FP32 master parameters, Adam state, training
@@ -248,6 +252,13 @@ constexpr size_t kRecBudget = (size_t)8 << 30;
 constexpr int kMaxBPVariant = 12;
 // the driver's cuTensorMapEncodeTiled (nullptr when unavailable), hilbert_tc.cu
 void* tensor_map_encoder();
+// Fifth form building blocks (bkproj2.cu): the box-map table over cell records of `nviews`
+// views (kBoxMaps CUtensorMap entries written to `out`, host memory), the records of views
+// [p0, p0 + nviews) of fproj, and the capacity (records per staged view) of a plan.
+constexpr int kBoxMaps = 256;
+Status encode_box_maps(void* out, const void* rec, int RW, int RH, int nviews);
+Status launch_cell_records(cudaStream_t s, const float* d_fproj, void* rec, int p0, int nviews,
+                           int YL, int ZL);
 template <typename OutT>
 Status launch_bkproj_v5(int variant, cudaStream_t s, BPPlan& plan, const float* d_fproj,
                         const PiRecord* d_pitab, OutT* d_image, int* err, DevBuf& recbuf,

@@ -222,8 +222,10 @@ ctrecon_status ctrecon_batch_create(ctrecon_ctx* ctx, int n_scans,
                                     const ctrecon_filter_params* params,
                                     const ctrecon_bp_geom* geoms, ctrecon_batch** out);
 void ctrecon_batch_destroy(ctrecon_batch* batch);
-/* backprojector form of every scan of the batch: 0 .. 9 as CTRECON_OPT_BP_VARIANT (default:
- * the context's); scans that share a form share one persistent launch */
+/* backprojector form of every scan of the batch: 0 .. 12 as CTRECON_OPT_BP_VARIANT (default:
+ * the context's); scans that share a form share one persistent launch. The fifth form
+ * (10 .. 12) holds the cell records of all its scans at once (16 bytes per detector cell and
+ * view) and writes them right before the launch. */
 ctrecon_status ctrecon_batch_set_variant(ctrecon_batch* batch, int variant);
 /* per-scan forms (n = the batch's scan count) */
 ctrecon_status ctrecon_batch_set_variants(ctrecon_batch* batch, const int* variants, int n);

@@ -18,7 +18,7 @@ def _scans():
                          NZ=20, seed=4)]
 
 
-@pytest.mark.parametrize("variant", [0, 2, 5, 7])
+@pytest.mark.parametrize("variant", [0, 2, 5, 7, 10, 12])
 def test_batch_equals_single_scans(variant):
     torch = pytest.importorskip("torch")
     if not torch.cuda.is_available():
@@ -63,7 +63,7 @@ def test_batch_with_per_scan_forms():
     import ctrecon_b200 as ct
     from ctrecon_b200 import _lib
     scans = _scans()
-    forms = [9, 2, 9][:len(scans)]
+    forms = [10, 2, 9][:len(scans)]
     stream = torch.cuda.Stream()
     with torch.cuda.stream(stream), ct.Context(0) as cx:
         projs, singles = [], []
