@@ -321,6 +321,7 @@ ctrecon_status ctrecon_set_option(ctrecon_ctx* ctx, ctrecon_option opt, int valu
             return finish(ctx, make_status(CTRECON_ERR_INVALID_ARGUMENT, "window must be >= 0"));
         ctx->opt_bp_window = value;
         break;
+    case CTRECON_OPT_PINET_FAST: ctx->opt_pinet_fast = value != 0; break;
     default: return finish(ctx, make_status(CTRECON_ERR_INVALID_ARGUMENT, "unknown option"));
     }
     return finish(ctx, Status::Ok());
@@ -336,6 +337,7 @@ ctrecon_status ctrecon_get_option(const ctrecon_ctx* ctx, ctrecon_option opt, in
     case CTRECON_OPT_VERBOSE: *value = ctx->opt_verbose; break;
     case CTRECON_OPT_DERIVATIVE: *value = ctx->opt_deriv; break;
     case CTRECON_OPT_BP_WINDOW: *value = ctx->opt_bp_window; break;
+    case CTRECON_OPT_PINET_FAST: *value = ctx->opt_pinet_fast; break;
     default: return CTRECON_ERR_INVALID_ARGUMENT;
     }
     return CTRECON_OK;

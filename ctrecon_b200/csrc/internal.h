@@ -199,6 +199,7 @@ struct ctrecon_ctx {
     int opt_verbose = 0;
     int opt_deriv = CTRECON_DERIV_CHAIN;
     int opt_bp_window = 0;
+    int opt_pinet_fast = 1;  // CTRECON_OPT_PINET_FAST
     cudaStream_t host_stream = nullptr;  // stream for the synchronous host calls
     cudaStream_t up_stream = nullptr;    // host -> device copies of the host calls
     cudaStream_t down_stream = nullptr;  // device -> host copies of the host calls

@@ -12,6 +12,12 @@
 // For the learned PI solve the kernel stores each voxel's predicted sb offset; the FP64 Newton
 // kernel (pi.cu) then starts from 2 pi z - pi/2 + offset and writes the voxel's PI record
 // exactly as the plain solver does.
+//
+// k_pinet_voxels is the learned solve's fast form (CTRECON_OPT_PINET_FAST): the same network
+// with FP32 features, every SiLU in packed BF16 arithmetic (one MUFU tanh per two neurons,
+// the hidden pre-activations cut to BF16 by a byte permute) and the output layer as a fourth
+// tensor-core product; its output only starts the FP64 Newton solve, which still decides every
+// endpoint.
 #include "internal.h"
 #include "pi_device.cuh"
 #include "pinet.h"
@@ -158,7 +164,7 @@ k_pinet_infer(BPParams kp, const unsigned char* __restrict__ net, long long n_it
                 tcu::mma_commit(bar);
             }
             __syncwarp();
-            ok = __all_sync(0xffffffffu, tcu::mbar_wait(bar, phase, err, 5)) && ok;
+            ok = __all_sync(0xffffffffu, tcu::mbar_wait_poll(bar, phase, err, 5)) && ok;
             phase ^= 1u;
             tcu::fence_after();
             const float* bl = B0 + 64 * (l + 1);
@@ -203,11 +209,198 @@ k_pinet_infer(BPParams kp, const unsigned char* __restrict__ net, long long n_it
     if (warp == 0) tcu::tmem_dealloc(tmem, 64);
 }
 
+// ---- fast voxel-mode inference ---------------------------------------------------------------
+// shared memory (offsets from a 1024-byte aligned base)
+constexpr int kVsA = 0;                 // activation tile 128 x 128 B
+constexpr int kVsW = 16384;             // hidden weight tiles, 3 x 64 x 128 B
+constexpr int kVsO = kVsW + 3 * 8192;   // output weight tile 16 x 128 B (rows 0, 1 = W4)
+constexpr int kVsP0 = kVsO + 2048;      // layer 0: 64 x float4 {w0, w1, w2, b} / 2
+constexpr int kVsPB = kVsP0 + 1024;     // hidden biases / 2 as BF16 pairs, 3 x 32 x 4 B
+constexpr int kVsBar = kVsPB + 384;
+constexpr int kVsSlot = kVsBar + 8;
+constexpr int kVsBytes = kVsSlot + 8 + 1024;
+constexpr int kVsPerSM = 233472 / (kVsBytes + 1024) < 8 ? 233472 / (kVsBytes + 1024) : 8;
+
+__device__ __forceinline__ uint32_t bf16x2_cut(float a, float b) {  // upper halves of a, b
+    uint32_t x;
+    asm("prmt.b32 %0, %1, %2, 0x7632;" : "=r"(x) : "r"(__float_as_uint(a)), "r"(__float_as_uint(b)));
+    return x;
+}
+// y = h tanh(h) + h = SiLU(2h) for a BF16 pair h
+__device__ __forceinline__ uint32_t silu2_half(uint32_t h) {
+    uint32_t t, y;
+    asm("tanh.approx.bf16x2 %0, %1;" : "=r"(t) : "r"(h));
+    asm("fma.rn.bf16x2 %0, %1, %2, %1;" : "=r"(y) : "r"(h), "r"(t));
+    return y;
+}
+__device__ __forceinline__ uint32_t hfma2(uint32_t a, uint32_t b, uint32_t c) {
+    uint32_t d;
+    asm("fma.rn.bf16x2 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
+    return d;
+}
+
+__global__ void __launch_bounds__(kT)
+k_pinet_voxels(BPParams kp, const unsigned char* __restrict__ net, long long n_items,
+               float* __restrict__ guess, int* __restrict__ err) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* sm = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint8_t* A = sm + kVsA;
+    uint8_t* Wt = sm + kVsW;
+    uint8_t* Wo = sm + kVsO;
+    float4* P0 = reinterpret_cast<float4*>(sm + kVsP0);
+    uint32_t* PB = reinterpret_cast<uint32_t*>(sm + kVsPB);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + kVsBar);
+    uint32_t* slot = reinterpret_cast<uint32_t*>(sm + kVsSlot);
+    const int t = threadIdx.x, warp = t >> 5;
+
+    const uint4* src = reinterpret_cast<const uint4*>(net);
+    for (int q = t; q < 3 * 64 * 8; q += kT) {
+        const int l = q >> 9, r = (q >> 3) & 63, c = q & 7;
+        *reinterpret_cast<uint4*>(Wt + l * 8192 + tcu::sw128_offset(r, c)) = src[q];
+    }
+    const float* fsrc = reinterpret_cast<const float*>(net + kNetBf16Bytes);
+    // output tile: row n < 2 = W4[n][0..63] in BF16, rows 2..15 zero
+    for (int q = t; q < 16 * 8; q += kT) {
+        const int r = q >> 3, c = q & 7;
+        uint32_t w[4] = {0, 0, 0, 0};
+        if (r < 2)
+            for (int k = 0; k < 4; ++k)
+                w[k] = pack_bf16(fsrc[kNetF32_W4 + 64 * r + 8 * c + 2 * k],
+                                 fsrc[kNetF32_W4 + 64 * r + 8 * c + 2 * k + 1]);
+        *reinterpret_cast<uint4*>(Wo + tcu::sw128_offset(r, c)) = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+    // layer 0 halved and scaled by 1 + 2^-9, so that cutting its pre-activations to BF16
+    // rounds to nearest on average
+    constexpr float kHalfUp = 0.5f * (1.0f + 1.0f / 512.0f);
+    for (int q = t; q < 64; q += kT) {
+        const float* w = fsrc + kNetF32_W0 + 3 * q;
+        P0[q] = make_float4(kHalfUp * w[0], kHalfUp * w[1], kHalfUp * w[2],
+                            kHalfUp * fsrc[kNetF32_B0 + q]);
+    }
+    for (int q = t; q < 96; q += kT) {
+        const float* b = fsrc + kNetF32_B0 + 64 + 2 * q;
+        PB[q] = pack_bf16(0.5f * b[0], 0.5f * b[1]);
+    }
+    const float b4 = fsrc[kNetF32_B4];
+    if (t == 0) {
+        tcu::mbar_init(bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) tcu::tmem_alloc(slot, 64);
+    tcu::fence_proxy_async();
+    tcu::fence_before();
+    __syncthreads();
+    tcu::fence_after();
+    const uint32_t tmem = *slot;
+    const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+    const uint32_t idesc = tcu::idesc_bf16_f32(128, 64), idesc_o = tcu::idesc_bf16_f32(128, 16);
+    const uint32_t a_addr = tcu::smem_u32(A), w_addr = tcu::smem_u32(Wt), o_addr = tcu::smem_u32(Wo);
+    const uint32_t half2 = 0x3F003F00u;  // (0.5, 0.5)
+    uint32_t phase = 0;
+    const long long ntiles = (n_items + kT - 1) / kT;
+    const float XC = (float)kp.XC, YC = (float)kp.YC, ZC = (float)kp.ZC;
+    const float dx = (float)kp.dx, dy = (float)kp.dy, dz = (float)kp.dz;
+    const float iR = (float)(1.0 / kp.ScanR), iH = (float)(1.0 / kp.HelicP);
+    bool ok = true;
+
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const long long idx = tile * kT + t;
+        const bool valid = idx < n_items;
+        float f0 = 0.f, f1 = 1.f, f2 = 0.f;
+        bool inside = false;
+        if (valid) {
+            // the volume has fewer than 2^31 voxels (ctrecon_bp_geom checks)
+            const int ii = (int)idx;
+            const int zi = ii % kp.NZ, xy = ii / kp.NZ;
+            const int yi = xy % kp.NY, xi = xy / kp.NY;
+            const double Xd = (xi - kp.XC) * kp.dx, Yd = (yi - kp.YC) * kp.dy;
+            inside = Xd * Xd + Yd * Yd < kp.ObjR2;  // KatsevichBkProj.cpp:168
+            const float x = ((float)xi - XC) * dx * iR, y = ((float)yi - YC) * dy * iR;
+            const float z = ((float)zi - ZC) * dz * iH;
+            const float r = sqrtf(x * x + y * y);
+            float s2, c2;
+            sincospif(2.f * (z - rintf(z)), &s2, &c2);
+            const float ir = r > 0.f ? 1.f / r : 0.f;
+            const float cph = r > 0.f ? x * ir : 1.f, sph = y * ir;
+            f0 = r * (float)kPinetRInv;
+            f1 = cph * c2 + sph * s2;  // cos(phi - 2 pi z)
+            f2 = sph * c2 - cph * s2;  // sin(phi - 2 pi z)
+        }
+        // layer 0 (FP32, halved): h = (w . f + b) / 2 cut to BF16, SiLU(2h)
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            uint32_t pk[4];
+#pragma unroll
+            for (int h = 0; h < 4; ++h) {
+                const float4 p = P0[c * 8 + 2 * h], q = P0[c * 8 + 2 * h + 1];
+                pk[h] = silu2_half(bf16x2_cut(fmaf(p.z, f2, fmaf(p.y, f1, fmaf(p.x, f0, p.w))),
+                                              fmaf(q.z, f2, fmaf(q.y, f1, fmaf(q.x, f0, q.w)))));
+            }
+            *reinterpret_cast<uint4*>(A + tcu::sw128_offset(t, c)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+        }
+        // hidden layers 1..3 on the tensor core, then the output layer (N = 16, column 0 = sb)
+#pragma unroll 1
+        for (int l = 0; l < 4; ++l) {
+            tcu::fence_proxy_async();
+            tcu::fence_before();
+            __syncthreads();
+            tcu::fence_after();
+            if (t == 0) {
+#pragma unroll
+                for (int ks = 0; ks < 4; ++ks)
+                    tcu::mma_bf16(tmem, tcu::sw128_desc(a_addr + 32 * ks),
+                                  tcu::sw128_desc((l < 3 ? w_addr + l * 8192 : o_addr) + 32 * ks),
+                                  l < 3 ? idesc : idesc_o, ks > 0);
+                tcu::mma_commit(bar);
+            }
+            __syncwarp();
+            ok = __all_sync(0xffffffffu, tcu::mbar_wait_poll(bar, phase, err, 5)) && ok;
+            phase ^= 1u;
+            tcu::fence_after();
+            if (l == 3) {
+                float h[16];
+                if (ok) tcu::tmem_ld16(lane_addr, h);
+                else h[0] = 0.f;
+                if (valid) guess[idx] = inside ? (h[0] + b4) / (float)kPinetOutScale : 0.f;
+                break;
+            }
+            const uint32_t* pb = PB + 32 * l;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                float h[16];
+                if (ok) tcu::tmem_ld16(lane_addr + 16 * q, h);
+                else {
+#pragma unroll
+                    for (int i = 0; i < 16; ++i) h[i] = 0.f;
+                }
+#pragma unroll
+                for (int cc = 0; cc < 2; ++cc) {
+                    const int c = 2 * q + cc;
+                    const float* hv = h + 8 * cc;
+                    const uint4 bb = *reinterpret_cast<const uint4*>(pb + 4 * c);
+                    const uint4 v = make_uint4(
+                        silu2_half(hfma2(bf16x2_cut(hv[0], hv[1]), half2, bb.x)),
+                        silu2_half(hfma2(bf16x2_cut(hv[2], hv[3]), half2, bb.y)),
+                        silu2_half(hfma2(bf16x2_cut(hv[4], hv[5]), half2, bb.z)),
+                        silu2_half(hfma2(bf16x2_cut(hv[6], hv[7]), half2, bb.w)));
+                    *reinterpret_cast<uint4*>(A + tcu::sw128_offset(t, c)) = v;
+                }
+            }
+        }
+    }
+    tcu::fence_before();
+    __syncthreads();
+    if (warp == 0) tcu::tmem_dealloc(tmem, 64);
+}
+
+// CTAs per SM of k_pinet_infer: as many as the shared memory holds (1 KB reserved per CTA), at
+// most 8 (TMEM: 64 columns each)
 int persistent_blocks() {
+    constexpr int per_sm = 233472 / (kSmBytes + 1024) < 8 ? 233472 / (kSmBytes + 1024) : 8;
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    return sms * 4;
+    return sms * per_sm;
 }
 
 }  // namespace
@@ -230,8 +423,21 @@ static Status launch_infer(ctrecon_ctx* ctx, cudaStream_t s, const BPParams& kp,
                            const float* feat, float2* raw, float* guess) {
     CTR_TRY(pinet_prepare(ctx, s));
     if (!ctx->ws_flag.ptr) return make_status(CTRECON_ERR_INTERNAL, "device error word not set up");
-    CTR_CUDA(cudaFuncSetAttribute(k_pinet_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmBytes));
     const long long ntiles = (n + kT - 1) / kT;
+    if (!feat && ctx->opt_pinet_fast) {
+        CTR_CUDA(cudaFuncSetAttribute(k_pinet_voxels, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      kVsBytes));
+        int dev = 0, sms = 148;
+        CTR_CUDA(cudaGetDevice(&dev));
+        CTR_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        const int grid = (int)std::min<long long>(ntiles, (long long)sms * kVsPerSM);
+        if (grid <= 0) return Status::Ok();
+        k_pinet_voxels<<<grid, kT, kVsBytes, s>>>(kp, ctx->pinet.infer.as<unsigned char>(), n,
+                                                  guess, ctx->ws_flag.as<int>());
+        CTR_CUDA(cudaGetLastError());
+        return Status::Ok();
+    }
+    CTR_CUDA(cudaFuncSetAttribute(k_pinet_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmBytes));
     const int grid = (int)std::min<long long>(ntiles, persistent_blocks());
     if (grid <= 0) return Status::Ok();
     k_pinet_infer<<<grid, kT, kSmBytes, s>>>(kp, ctx->pinet.infer.as<unsigned char>(), n, feat,

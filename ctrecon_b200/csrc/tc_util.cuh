@@ -61,6 +61,35 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* e
     return false;
 }
 
+// As mbar_wait, polling with test_wait (never suspending the thread): for short waits on work
+// that was just issued, such as a tensor-core product, where a suspended thread would wake late.
+__device__ __forceinline__ bool mbar_test(uint32_t a, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(a), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait_poll(uint64_t* bar, uint32_t parity, int* err, int code) {
+    const uint32_t a = smem_u32(bar);
+    uint64_t t0 = 0;
+    for (uint32_t it = 0; it < kWaitIterLimit; ++it) {
+        if (mbar_test(a, parity)) return true;
+        if ((it & 255) == 255) {
+            if (*(volatile int*)err) return false;
+            const uint64_t t = globaltimer_ns();
+            if (t0 == 0) t0 = t;
+            else if (t - t0 > kWaitLimitNs) break;
+        }
+    }
+    atomicCAS(err, 0, code);
+    return false;
+}
+
 // Error-path wait for async copies still completing on `bar` (phase of the given parity):
 // bounded by 10 ms of %globaltimer, independent of the error word; returns whether it completed.
 __device__ __forceinline__ bool mbar_drain(uint64_t* bar, uint32_t parity) {

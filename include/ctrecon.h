@@ -116,8 +116,12 @@ typedef enum ctrecon_option {
                                          table's choice */
     CTRECON_OPT_VERBOSE = 5,
     CTRECON_OPT_DERIVATIVE = 6,       /* CTRECON_DERIV_*; default CHAIN (the MEX filter's) */
-    CTRECON_OPT_BP_WINDOW = 7         /* views per cell-record window of variants 10..12;
+    CTRECON_OPT_BP_WINDOW = 7,        /* views per cell-record window of variants 10..12;
                                          0 (default) = as many as 8 GiB of records hold */
+    CTRECON_OPT_PINET_FAST = 8        /* learned PI solve: 1 (default) = BF16 SiLU arithmetic
+                                         in the network's inference (its output only starts
+                                         the FP64 Newton solve); 0 = FP32 SiLU as in
+                                         ctrecon_pinet_predict */
 } ctrecon_option;
 
 /* ---- context ---------------------------------------------------------------------- */
