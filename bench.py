@@ -536,6 +536,20 @@ def run_report_extras(args):
     ctx.close()
 
 
+def _train_pinet(ctx, s, out, stream, torch):
+    """Trains the learned PI-line initialiser on the GPU (2^22 FP64 Newton pairs, 8 epochs)."""
+    import ctypes
+    from ctrecon_b200 import _lib
+    loss = ctypes.c_float()
+    t0 = time.perf_counter()
+    _lib.check(_lib.lib().ctrecon_pinet_train(
+        ctx.handle, stream.cuda_stream, 1 << 22, 8192, 8, s.ObjR / s.ScanR * 1.05, 2024,
+        ctypes.byref(loss)), ctx.handle)
+    torch.cuda.synchronize()
+    out["pinet"] = {"train_pairs": 1 << 22, "epochs": 8, "train_s": time.perf_counter() - t0,
+                    "final_loss": loss.value}
+
+
 def run_report(args):
     """Reports of the c3 and c5 configurations (not the headline line)."""
     if args.report == "extras":
@@ -631,14 +645,7 @@ def run_report(args):
                                     "pi_solver": "bisection (the reference's) for the block"},
                     "pi_solver_in_timing": "newton"})
     else:  # c5: the learned PI-line initialiser at scale
-        import ctypes
-        loss = ctypes.c_float()
-        t0 = time.perf_counter()
-        _lib.check(_lib.lib().ctrecon_pinet_train(
-            ctx.handle, stream.cuda_stream, 1 << 22, 8192, 8, s.ObjR / s.ScanR * 1.05, 2024,
-            ctypes.byref(loss)), ctx.handle)
-        torch.cuda.synchronize()
-        train_s = time.perf_counter() - t0
+        _train_pinet(ctx, s, out, stream, torch)
         d_tab_b = d_tab.clone()  # the bisection table (the judge)
         res = {}
         for name, solver in (("bisect", _lib.PI_BISECT), ("newton", _lib.PI_NEWTON),
@@ -663,20 +670,52 @@ def run_report(args):
         out["newton_iterations_saved_per_voxel"] = (
             (res["newton"]["iterations"] - res["learned"]["iterations"]) /
             max(1, int((d_tab_b.view(torch.int32).view(-1, 4)[:, 0] != 0x7FFFFFFF).sum())))
-        out["pinet"] = {"train_pairs": 1 << 22, "epochs": 8, "train_s": train_s,
-                        "final_loss": loss.value}
-        forms = {"plain_fp32_bisect": (_lib.HILBERT_FP32, _lib.PI_BISECT),
-                 "fp32_newton": (_lib.HILBERT_FP32, _lib.PI_NEWTON),
-                 "fp32_learned": (_lib.HILBERT_FP32, _lib.PI_LEARNED),
-                 "bf16x3_newton": (_lib.HILBERT_BF16X3, _lib.PI_NEWTON),
-                 "bf16x3_learned": (_lib.HILBERT_BF16X3, _lib.PI_LEARNED)}
-        out["chain_ms"] = {}
-        for name, (hil, pis) in forms.items():
-            ctx.set_option(_lib.OPT_HILBERT, hil)
-            ctx.set_option(_lib.OPT_PI_SOLVER, pis)
-            ph = chain_ms(1)
-            ph["gups"] = updates / (ph["step"] / 1e3) / 1e9
-            out["chain_ms"][name] = ph
+        del d_tab_b
+    # the forms of the headline comparison on this workload: plain (FP32 Hilbert, bisection)
+    # against the mixed forms, device-resident chain, CUDA events
+    if "pinet" not in out:
+        _train_pinet(ctx, s, out, stream, torch)
+    forms = {"plain_fp32_bisect": (_lib.HILBERT_FP32, _lib.PI_BISECT),
+             "fp32_newton": (_lib.HILBERT_FP32, _lib.PI_NEWTON),
+             "fp32_learned": (_lib.HILBERT_FP32, _lib.PI_LEARNED),
+             "bf16x3_newton": (_lib.HILBERT_BF16X3, _lib.PI_NEWTON),
+             "bf16x3_learned": (_lib.HILBERT_BF16X3, _lib.PI_LEARNED)}
+    out["chain_ms"] = {}
+    for name, (hil, pis) in forms.items():
+        ctx.set_option(_lib.OPT_HILBERT, hil)
+        ctx.set_option(_lib.OPT_PI_SOLVER, pis)
+        ph = chain_ms(1 if args.report == "c5" else 2)
+        ph["gups"] = updates / (ph["step"] / 1e3) / 1e9
+        out["chain_ms"][name] = ph
+    if args.report == "c3":
+        # mixed + learned + batched: two copies of the scan through the batch API (filters, PI
+        # solves, one persistent backprojection launch over both volumes), replayed as a graph
+        ctx.set_option(_lib.OPT_HILBERT, _lib.HILBERT_BF16X3)
+        ctx.set_option(_lib.OPT_PI_SOLVER, _lib.PI_LEARNED)
+        del d_tab
+        b = ct.Batch(ctx, [s, s])
+        bform = out.get("bp_tune", {}).get("best_variant", args.bp_variant)
+        b.set_variant(bform if 0 <= bform < 100 else 10)
+        d_fproj2, d_img2 = torch.empty_like(d_proj), torch.zeros_like(d_img)
+        bargs = ([d_proj, d_proj], [d_fproj, d_fproj2], [d_img, d_img2])
+        sb = torch.cuda.Stream()
+        with torch.cuda.stream(sb):
+            for _ in range(3):
+                b.run(*bargs, stream=sb, use_graph=True)
+            sb.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(sb)
+            for _ in range(2):
+                b.run(*bargs, stream=sb, use_graph=True)
+            e1.record(sb)
+            sb.synchronize()
+        ms = e0.elapsed_time(e1) / 2
+        out["chain_ms"]["bf16x3_learned_batched_x2"] = {
+            "step": ms, "scans": 2, "bp_variant": b.variants()[0],
+            "gups": 2 * updates / (ms / 1e3) / 1e9}
+        b.close()
+    plain = out["chain_ms"]["plain_fp32_bisect"]["gups"]
+    out["vs_plain"] = {k: v["gups"] / plain for k, v in out["chain_ms"].items()}
     print(json.dumps(out))
     ctx.close()
 
@@ -790,6 +829,11 @@ def main():
         launches_per_step += nchunks
     if pis == _lib.PI_LEARNED:
         launches_per_step += 1  # the network's inference kernel before the Newton solve
+    if 10 <= bp_form < 100:
+        # the fifth form writes the cell records of each view window (8 GiB) before its launch
+        plane = (s.ZL - 1) * (s.YL - 1) * 16
+        per = max(1, (8 << 30) // plane)
+        launches_per_step += 2 * ((s.P + per - 1) // per) - 1
 
     # ---- e2e through the MEX-equivalent host calls (FP64 pinned host buffers) -----------------
     e2e = None
@@ -820,7 +864,8 @@ def main():
     peak, peak_kind = load_peaks()
     achieved = BYTES_PER_UPDATE * updates / (bp_ms / 1e3) / 1e9
     bp_kernel = ("k_bkproj" if bp_form >= 100 else "k_bkproj3" if bp_form in (0, 1)
-                 else "k_bkproj2" if bp_form in (2, 3, 4) else "k_bkproj4")
+                 else "k_bkproj2" if bp_form in (2, 3, 4) else "k_bkproj5" if bp_form >= 10
+                 else "k_bkproj4")
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_source": peak_kind,
                 "kernel": bp_kernel, "model": "16 B per voxel-view update",
