@@ -96,7 +96,8 @@ __global__ void k_deriv_rebin(const float* __restrict__ proj, int proj_view0, in
         if (j < 2) { jl = 0; jr = 2; }
         else if (j > YL - 3) { jl = YL - 3; jr = YL - 1; }
         const float2 cy = cuy[j];  // (u coefficient, y coordinate)
-#pragma unroll 2
+        // sixteen rows' loads in flight per thread (the kernel is load-latency bound)
+#pragma unroll 16
         for (int k = ry; k < ZL; k += RG) {
             int kl = k - 1, kr = k + 1;  // v stencil, same edge rule (:85-95)
             if (k < 2) { kl = 0; kr = 2; }
@@ -114,7 +115,7 @@ __global__ void k_deriv_rebin(const float* __restrict__ proj, int proj_view0, in
         for (int a = ry; a < AL; a += RG) store_kappa(X, xv + (size_t)a * YLp + j, plane, 0.f, mode);
         return;
     }
-#pragma unroll 2
+#pragma unroll 8
     for (int a = ry; a < AL; a += RG) {
         const FwEntry f = fw[(size_t)a * YL + j];
         store_kappa(X, xv + (size_t)a * YLp + j, plane,
