@@ -54,8 +54,9 @@ def parse():
     ap.add_argument("--config", default="c2")
     ap.add_argument("--hilbert", default="fp32", choices=["fp32", "bf16x3", "tf32"])
     ap.add_argument("--pi", default="bisect", choices=["bisect", "newton", "learned"])
-    ap.add_argument("--pinet-accurate", action="store_true",
-                    help="learned PI solve: FP32 SiLU in the network's inference (default BF16)")
+    ap.add_argument("--pinet-mode", default="grid", choices=["voxel-fp32", "voxel-bf16", "grid"],
+                    help="learned PI solve: the network per voxel (FP32 or packed BF16 SiLU) or "
+                         "on the (r, psi) screw-symmetry grid, interpolated (default)")
     ap.add_argument("--bp-variant", type=int, default=-1,
                     help="backprojector form: -1 autotuned on the workload before timing "
                          "(default), 0, 1 per-cell records (4 / 8 views per block), 2-4 second "
@@ -744,7 +745,9 @@ def main():
     pis = {"bisect": _lib.PI_BISECT, "newton": _lib.PI_NEWTON, "learned": _lib.PI_LEARNED}[args.pi]
     ctx = ct.Context(local, hilbert=hil, pi_solver=_lib.PI_BISECT)
     ctx.set_option(_lib.OPT_BP_VARIANT, args.bp_variant)
-    ctx.set_option(_lib.OPT_PINET_FAST, 0 if args.pinet_accurate else 1)
+    ctx.set_option(_lib.OPT_PINET_MODE, {"voxel-fp32": _lib.PINET_VOXEL_FP32,
+                                         "voxel-bf16": _lib.PINET_VOXEL_BF16,
+                                         "grid": _lib.PINET_GRID}[args.pinet_mode])
     geom = s.geom_struct()
     fpar = ct.scan_filter_params(s)
     pinet_info = None

@@ -29,7 +29,8 @@ PI_BISECT, PI_NEWTON, PI_LEARNED = 0, 1, 2
 OPT_HILBERT, OPT_PI_SOLVER, OPT_FILTER_CHUNK, OPT_BP_VARIANT, OPT_VERBOSE = 1, 2, 3, 4, 5
 OPT_DERIVATIVE = 6
 OPT_BP_WINDOW = 7
-OPT_PINET_FAST = 8
+OPT_PINET_MODE = 8
+PINET_VOXEL_FP32, PINET_VOXEL_BF16, PINET_GRID = 0, 1, 2
 DERIV_DIRECT, DERIV_CHAIN = 0, 1
 
 

@@ -321,7 +321,11 @@ ctrecon_status ctrecon_set_option(ctrecon_ctx* ctx, ctrecon_option opt, int valu
             return finish(ctx, make_status(CTRECON_ERR_INVALID_ARGUMENT, "window must be >= 0"));
         ctx->opt_bp_window = value;
         break;
-    case CTRECON_OPT_PINET_FAST: ctx->opt_pinet_fast = value != 0; break;
+    case CTRECON_OPT_PINET_MODE:
+        if (value < CTRECON_PINET_VOXEL_FP32 || value > CTRECON_PINET_GRID)
+            return finish(ctx, make_status(CTRECON_ERR_INVALID_ARGUMENT, "bad network mode"));
+        ctx->opt_pinet_mode = value;
+        break;
     default: return finish(ctx, make_status(CTRECON_ERR_INVALID_ARGUMENT, "unknown option"));
     }
     return finish(ctx, Status::Ok());
@@ -337,7 +341,7 @@ ctrecon_status ctrecon_get_option(const ctrecon_ctx* ctx, ctrecon_option opt, in
     case CTRECON_OPT_VERBOSE: *value = ctx->opt_verbose; break;
     case CTRECON_OPT_DERIVATIVE: *value = ctx->opt_deriv; break;
     case CTRECON_OPT_BP_WINDOW: *value = ctx->opt_bp_window; break;
-    case CTRECON_OPT_PINET_FAST: *value = ctx->opt_pinet_fast; break;
+    case CTRECON_OPT_PINET_MODE: *value = ctx->opt_pinet_mode; break;
     default: return CTRECON_ERR_INVALID_ARGUMENT;
     }
     return CTRECON_OK;

@@ -180,6 +180,7 @@ struct BatchScanDev {
 // data, and the BF16 inference copy.
 struct PinetState {
     DevBuf theta, adam_m, adam_v, grad, data, infer, guess;
+    DevBuf grid_feat, grid_out;  // CTRECON_PINET_GRID: features and outputs on the (r, psi) grid
     bool trained = false;
     double r_max = 0;
     int version = 0;        // bumped by every training run
@@ -199,7 +200,7 @@ struct ctrecon_ctx {
     int opt_verbose = 0;
     int opt_deriv = CTRECON_DERIV_CHAIN;
     int opt_bp_window = 0;
-    int opt_pinet_fast = 1;  // CTRECON_OPT_PINET_FAST
+    int opt_pinet_mode = CTRECON_PINET_GRID;  // CTRECON_OPT_PINET_MODE
     cudaStream_t host_stream = nullptr;  // stream for the synchronous host calls
     cudaStream_t up_stream = nullptr;    // host -> device copies of the host calls
     cudaStream_t down_stream = nullptr;  // device -> host copies of the host calls

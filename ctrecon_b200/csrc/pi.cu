@@ -14,12 +14,22 @@
 //   LEARNED the same Newton started at the trained network's prediction (pinet_infer.cu).
 #include "internal.h"
 #include "pi_device.cuh"
+#include "pinet.h"
 
 namespace ctr {
 
+// The learned start from the network's predictions on the (r, psi) grid (CTRECON_PINET_GRID):
+// gtab[i * np + j].x = network output at r = i / rinv_step (r normalised by ScanR),
+// psi = 2 pi j / np; bilinear in r and (periodic) psi.
+struct PiGrid {
+    const float2* tab;
+    int nr, np;
+    float rinv_step;
+};
+
 __global__ void k_pi_solve(BPParams kp, double Ctr, double Beg, int solver,
-                           const float* __restrict__ guess, PiRecord* __restrict__ out,
-                           unsigned long long* __restrict__ count,
+                           const float* __restrict__ guess, PiGrid grid,
+                           PiRecord* __restrict__ out, unsigned long long* __restrict__ count,
                            unsigned long long* __restrict__ iters_total) {
     const long long n = (long long)kp.NX * kp.NY * kp.NZ;
     const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -41,6 +51,22 @@ __global__ void k_pi_solve(BPParams kp, double Ctr, double Beg, int solver,
                 // plus the learned offset when there is one
                 double s0 = z * 2 * kRefPi - 0.5 * kRefPi;
                 if (guess) s0 += (double)guess[idx];
+                if (grid.tab) {
+                    // psi = phi - 2 pi z in turns, reduced to [0, 1)
+                    const float t = atan2f((float)y, (float)x) * (float)(0.5 / kRefPi) -
+                                    (float)(z - floor(z));
+                    const float fp = (t - floorf(t)) * (float)grid.np;
+                    const float fr = fminf(sqrtf((float)(x * x + y * y)) * grid.rinv_step,
+                                           (float)(grid.nr - 1) - 1e-3f);
+                    const int i0 = (int)fr, j0 = min((int)fp, grid.np - 1);
+                    const int j1 = j0 + 1 == grid.np ? 0 : j0 + 1;
+                    const float a = fr - (float)i0, b = fp - (float)j0;
+                    const float2* r0 = grid.tab + (size_t)i0 * grid.np;
+                    const float2* r1 = r0 + grid.np;
+                    const float o = (1.f - a) * ((1.f - b) * __ldg(&r0[j0].x) + b * __ldg(&r0[j1].x)) +
+                                    a * ((1.f - b) * __ldg(&r1[j0].x) + b * __ldg(&r1[j1].x));
+                    s0 += (double)(o / (float)kPinetOutScale);
+                }
                 int it = 0;
                 pi_newton(x, y, z, s0, &sb, &st, &it);
                 its = (unsigned long long)it;
@@ -66,23 +92,26 @@ Status launch_pi_learned(ctrecon_ctx* ctx, cudaStream_t s, BPPlan& plan, PiRecor
 
 static Status launch_solve(cudaStream_t s, BPPlan& plan, int solver, const float* guess,
                            PiRecord* d_pitab, unsigned long long* d_updates,
-                           unsigned long long* d_iters) {
+                           unsigned long long* d_iters, PiGrid grid = PiGrid{nullptr, 0, 0, 0.f}) {
     const long long n = (long long)plan.kp.NX * plan.kp.NY * plan.kp.NZ;
     const int bs = 128;
     long long nb = (n + bs - 1) / bs;
     if (nb > 0x7fffffffLL) return make_status(CTRECON_ERR_UNSUPPORTED, "volume too large");
     k_pi_solve<<<(unsigned)nb, bs, 0, s>>>(plan.kp, plan.g.ProjCtr, (double)plan.g.ProjBegin,
-                                           solver, guess, d_pitab, d_updates, d_iters);
+                                           solver, guess, grid, d_pitab, d_updates, d_iters);
     CTR_CUDA(cudaGetLastError());
     return Status::Ok();
 }
 
-// Newton from per-voxel offsets of the start point (the learned path, pinet_infer.cu)
+// Newton from per-voxel offsets of the start point (the learned path, pinet_infer.cu), or from
+// the network's (r, psi) grid (d_grid: nr x np float2 outputs, r from 0 to r_max)
 Status launch_pi_guess(ctrecon_ctx* ctx, cudaStream_t s, BPPlan& plan, PiRecord* d_pitab,
                        unsigned long long* d_updates, unsigned long long* d_iters,
-                       const float* d_guess) {
+                       const float* d_guess, const void* d_grid, int nr, int np, double r_max) {
     (void)ctx;
-    return launch_solve(s, plan, CTRECON_PI_LEARNED, d_guess, d_pitab, d_updates, d_iters);
+    PiGrid grid{static_cast<const float2*>(d_grid), nr, np,
+                d_grid ? (float)((nr - 1) / r_max) : 0.f};
+    return launch_solve(s, plan, CTRECON_PI_LEARNED, d_guess, d_pitab, d_updates, d_iters, grid);
 }
 
 Status launch_pi_stats(ctrecon_ctx* ctx, cudaStream_t s, BPPlan& plan, PiRecord* d_pitab,

@@ -13,11 +13,16 @@
 // kernel (pi.cu) then starts from 2 pi z - pi/2 + offset and writes the voxel's PI record
 // exactly as the plain solver does.
 //
-// k_pinet_voxels is the learned solve's fast form (CTRECON_OPT_PINET_FAST): the same network
-// with FP32 features, every SiLU in packed BF16 arithmetic (one MUFU tanh per two neurons,
-// the hidden pre-activations cut to BF16 by a byte permute) and the output layer as a fourth
-// tensor-core product; its output only starts the FP64 Newton solve, which still decides every
-// endpoint.
+// k_pinet_voxels is the per-voxel learned start in packed BF16 (CTRECON_PINET_VOXEL_BF16): the
+// same network with FP32 features, every SiLU in packed BF16 arithmetic (the hidden
+// pre-activations cut to BF16 by a byte permute) and the output layer as a fourth tensor-core
+// product; its output only starts the FP64 Newton solve, which still decides every endpoint.
+// Either per-voxel form is bounded by the MUFU pipe (one tanh per neuron: 256 per voxel, 16 per
+// SM and clock in every precision).
+//
+// CTRECON_PINET_GRID (the default): the network's inputs depend on (r, psi = phi - 2 pi z)
+// only, so k_pinet_infer evaluates it once per point of a 256 x 1024 grid of (r, psi) and the
+// Newton kernel (pi.cu) starts every voxel from the bilinear interpolation of those outputs.
 #include "internal.h"
 #include "pi_device.cuh"
 #include "pinet.h"
@@ -32,7 +37,7 @@ namespace ctr {
 Status pinet_ensure(ctrecon_ctx* ctx);
 Status launch_pi_guess(ctrecon_ctx* ctx, cudaStream_t s, BPPlan& plan, PiRecord* d_pitab,
                        unsigned long long* d_updates, unsigned long long* d_iters,
-                       const float* d_guess);
+                       const float* d_guess, const void* d_grid, int nr, int np, double r_max);
 
 namespace {
 
@@ -424,7 +429,7 @@ static Status launch_infer(ctrecon_ctx* ctx, cudaStream_t s, const BPParams& kp,
     CTR_TRY(pinet_prepare(ctx, s));
     if (!ctx->ws_flag.ptr) return make_status(CTRECON_ERR_INTERNAL, "device error word not set up");
     const long long ntiles = (n + kT - 1) / kT;
-    if (!feat && ctx->opt_pinet_fast) {
+    if (!feat && ctx->opt_pinet_mode == CTRECON_PINET_VOXEL_BF16) {
         CTR_CUDA(cudaFuncSetAttribute(k_pinet_voxels, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       kVsBytes));
         int dev = 0, sms = 148;
@@ -446,13 +451,42 @@ static Status launch_infer(ctrecon_ctx* ctx, cudaStream_t s, const BPParams& kp,
     return Status::Ok();
 }
 
+// features of the (r, psi) grid: r = i r_max / (nr - 1) (normalised by ScanR), psi = 2 pi j / np
+__global__ void k_grid_feat(float* __restrict__ feat, int nr, int np, double r_max) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nr * np) return;
+    const int i = q / np, j = q % np;
+    double sp, cp;
+    sincospi(2.0 * j / np, &sp, &cp);
+    feat[3 * q] = (float)(r_max * i / (nr - 1) * kPinetRInv);
+    feat[3 * q + 1] = (float)cp;
+    feat[3 * q + 2] = (float)sp;
+}
+
+constexpr int kGridNR = 256, kGridNP = 1024;
+
 Status launch_pi_learned(ctrecon_ctx* ctx, cudaStream_t s, BPPlan& plan, PiRecord* d_pitab,
                          unsigned long long* d_updates, unsigned long long* d_iters) {
     const long long n = (long long)plan.kp.NX * plan.kp.NY * plan.kp.NZ;
+    if (ctx->opt_pinet_mode == CTRECON_PINET_GRID) {
+        // the network once per grid point (FP32 SiLU, feature mode), then the Newton solve
+        // interpolates its outputs; r up to the cylinder's radius
+        const int ng = kGridNR * kGridNP;
+        const double r_max = plan.g.ObjR / plan.g.ScanR;
+        CTR_TRY(ctx->pinet.grid_feat.ensure((size_t)ng * 3 * sizeof(float), "network grid features"));
+        CTR_TRY(ctx->pinet.grid_out.ensure((size_t)ng * sizeof(float2), "network grid outputs"));
+        k_grid_feat<<<(ng + 255) / 256, 256, 0, s>>>(ctx->pinet.grid_feat.as<float>(), kGridNR,
+                                                     kGridNP, r_max);
+        CTR_CUDA(cudaGetLastError());
+        CTR_TRY(launch_infer(ctx, s, plan.kp, ng, ctx->pinet.grid_feat.as<float>(),
+                             ctx->pinet.grid_out.as<float2>(), nullptr));
+        return launch_pi_guess(ctx, s, plan, d_pitab, d_updates, d_iters, nullptr,
+                               ctx->pinet.grid_out.ptr, kGridNR, kGridNP, r_max);
+    }
     CTR_TRY(ctx->pinet.guess.ensure((size_t)n * sizeof(float), "learned PI guesses"));
     float* g = ctx->pinet.guess.as<float>();
     CTR_TRY(launch_infer(ctx, s, plan.kp, n, nullptr, nullptr, g));
-    return launch_pi_guess(ctx, s, plan, d_pitab, d_updates, d_iters, g);
+    return launch_pi_guess(ctx, s, plan, d_pitab, d_updates, d_iters, g, nullptr, 0, 0, 0.0);
 }
 
 Status pinet_predict(ctrecon_ctx* ctx, cudaStream_t s, const float* d_feat, long long n,

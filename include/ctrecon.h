@@ -99,6 +99,16 @@ enum {
     CTRECON_DERIV_CHAIN = 1    /* DerMode 1: KatsevichFiltering.m:52-95, chain rule (default) */
 };
 
+/* CTRECON_OPT_PINET_MODE. The network's inputs are (r, cos psi, sin psi) with
+ * psi = phi - 2 pi z / pitch (the helix's screw symmetry), so its prediction is a function of
+ * (r, psi) alone. Whatever the mode, the FP64 Newton solve decides every endpoint. */
+enum {
+    CTRECON_PINET_VOXEL_FP32 = 0, /* per voxel, FP32 SiLU (as ctrecon_pinet_predict) */
+    CTRECON_PINET_VOXEL_BF16 = 1, /* per voxel, packed BF16 SiLU */
+    CTRECON_PINET_GRID = 2        /* default: the network (FP32 SiLU) on a 256 x 1024 grid of
+                                     (r, psi) each solve, bilinear in (r, psi) per voxel */
+};
+
 typedef enum ctrecon_option {
     CTRECON_OPT_HILBERT = 1,          /* CTRECON_HILBERT_*; default FP32 */
     CTRECON_OPT_PI_SOLVER = 2,        /* CTRECON_PI_*; default BISECT */
@@ -118,10 +128,8 @@ typedef enum ctrecon_option {
     CTRECON_OPT_DERIVATIVE = 6,       /* CTRECON_DERIV_*; default CHAIN (the MEX filter's) */
     CTRECON_OPT_BP_WINDOW = 7,        /* views per cell-record window of variants 10..12;
                                          0 (default) = as many as 8 GiB of records hold */
-    CTRECON_OPT_PINET_FAST = 8        /* learned PI solve: 1 (default) = BF16 SiLU arithmetic
-                                         in the network's inference (its output only starts
-                                         the FP64 Newton solve); 0 = FP32 SiLU as in
-                                         ctrecon_pinet_predict */
+    CTRECON_OPT_PINET_MODE = 8        /* how the learned PI solve evaluates the network:
+                                         CTRECON_PINET_* below */
 } ctrecon_option;
 
 /* ---- context ---------------------------------------------------------------------- */
