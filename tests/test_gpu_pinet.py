@@ -148,16 +148,24 @@ def test_pinet_training_inference_and_gain(torch_mod):
         err = np.abs(dO.cpu().numpy() - out_ref).max()
         print(f"inference max |BF16 kernel - FP64 forward| = {err:.3e}")
         assert err < 0.05
-        # the learned start: same records as the judge, fewer Newton steps than the plain start
+        # the learned start in each network mode (per voxel FP32 / packed BF16, and the
+        # screw-symmetry grid): same records as the judge, fewer Newton steps than the plain start
         bis = _pi(cx, torch, s, _lib.PI_BISECT)
         newt = _pi(cx, torch, s, _lib.PI_NEWTON)
-        lrn = _pi(cx, torch, s, _lib.PI_LEARNED)
+        lrn = {}
+        for name, mode in (("voxel-fp32", _lib.PINET_VOXEL_FP32),
+                           ("voxel-bf16", _lib.PINET_VOXEL_BF16), ("grid", _lib.PINET_GRID)):
+            cx.set_option(_lib.OPT_PINET_MODE, mode)
+            lrn[name] = _pi(cx, torch, s, _lib.PI_LEARNED)
     tol = 5e-6 * s.views_per_turn / (2 * np.pi) * 2
-    _compare(bis, lrn, tol)
     nv = int(bis["valid"].sum())
-    print(f"Newton iterations/voxel: plain start {newt['iters'] / nv:.2f}, learned start "
-          f"{lrn['iters'] / nv:.2f}")
-    assert lrn["iters"] < newt["iters"]
+    for name, r in lrn.items():
+        _compare(bis, r, tol)
+        print(f"Newton iterations/voxel: plain start {newt['iters'] / nv:.2f}, learned start "
+              f"({name}) {r['iters'] / nv:.2f}")
+        assert r["iters"] < newt["iters"]
+    # the grid interpolates the same network: as good a start as evaluating it per voxel
+    assert lrn["grid"]["iters"] <= 1.02 * lrn["voxel-fp32"]["iters"]
 
 
 @pytest.mark.parametrize("name", ["c1", "c2s"])
