@@ -649,9 +649,14 @@ def run_report(args):
         _train_pinet(ctx, s, out, stream, torch)
         d_tab_b = d_tab.clone()  # the bisection table (the judge)
         res = {}
-        for name, solver in (("bisect", _lib.PI_BISECT), ("newton", _lib.PI_NEWTON),
-                             ("learned", _lib.PI_LEARNED)):
+        for name, solver, nmode in (("bisect", _lib.PI_BISECT, None),
+                                    ("newton", _lib.PI_NEWTON, None),
+                                    ("learned_voxel_fp32", _lib.PI_LEARNED, _lib.PINET_VOXEL_FP32),
+                                    ("learned_voxel_bf16", _lib.PI_LEARNED, _lib.PINET_VOXEL_BF16),
+                                    ("learned", _lib.PI_LEARNED, _lib.PINET_GRID)):
             ctx.set_option(_lib.OPT_PI_SOLVER, solver)
+            if nmode is not None:
+                ctx.set_option(_lib.OPT_PINET_MODE, nmode)
             cnt, its = _pi_stats(ctx, torch, geom, d_tab)
             ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
             ev[0].record(stream)
@@ -659,7 +664,7 @@ def run_report(args):
             ev[1].record(stream)
             torch.cuda.synchronize()
             r = {"updates": cnt, "iterations": its, "pi_ms": ev[0].elapsed_time(ev[1])}
-            if name != "bisect":
+            if name != "bisect" and not name.startswith("learned_voxel"):
                 r["vs_bisection"] = _compare_pi_tables(torch, d_tab, d_tab_b)
             if name == "newton":
                 d_tab_n = d_tab.clone()
