@@ -110,6 +110,29 @@ static Status enqueue(ctrecon_batch* b, cudaStream_t s, const float* const* d_pr
 // table; the group buffers are reused, so a stable configuration allocates nothing.
 static Status upload_scans(ctrecon_batch* b, cudaStream_t s, float* const* d_fproj,
                            float* const* d_image) {
+    // The fifth form holds the cell records of all its scans at once: when they would take
+    // more than half of the free device memory (beside what the batch already holds), its
+    // largest scans move to the fourth form (variant 9) until they fit.
+    {
+        size_t held = 0;
+        for (const auto& G : b->groups) held += G->rec.bytes;
+        size_t free_b = 0, total_b = 0;
+        CTR_CUDA(cudaMemGetInfo(&free_b, &total_b));
+        const size_t budget = (free_b + held) / 2;
+        auto rec_of = [&](int i) {
+            const BPParams& kp = b->bplans[i]->kp;
+            return (size_t)kp.P * (kp.ZL - 1) * (kp.YL - 1) * 16;
+        };
+        std::vector<int> five;
+        size_t need = 0;
+        for (int i = 0; i < b->n; ++i)
+            if (b->svar[i] >= 10) { five.push_back(i); need += rec_of(i); }
+        std::sort(five.begin(), five.end(), [&](int x, int y) { return rec_of(x) > rec_of(y); });
+        for (size_t k = 0; k < five.size() && need > budget; ++k) {
+            need -= rec_of(five[k]);
+            b->svar[five[k]] = 9;
+        }
+    }
     std::vector<int> forms;
     for (int k = 0; k < b->n; ++k) {
         const int v = b->svar[b->order[k]];
