@@ -594,21 +594,30 @@ static Status host_filter_pipeline(ctrecon_ctx* ctx, const ctrecon_filter_params
     if (fproj_host) CTR_TRY(ctx->ws_d.ensure(n * sizeof(double), "FP64 result staging"));
     const int nch = (P + kHostChunkViews - 1) / kHostChunkViews;
     cudaStream_t up = ctx->up_stream, comp = ctx->host_stream, down = ctx->down_stream;
+    // the up stream carries copies only: a conversion kernel there would wait for SMs behind
+    // the filter and stall the copy engine; each chunk is converted on the compute stream
     for (int c = 0; c < nch; ++c) {
         const size_t v0 = (size_t)c * kHostChunkViews, v1 = std::min<size_t>(P, v0 + kHostChunkViews);
         CTR_CUDA(cudaMemcpyAsync(ctx->ws_a.as<double>() + v0 * S, proj + v0 * S,
                                  (v1 - v0) * S * sizeof(double), cudaMemcpyHostToDevice, up));
-        CTR_TRY(launch_convert_f64_to_f32(up, ctx->ws_a.as<double>() + v0 * S,
-                                          ctx->ws_b.as<float>() + v0 * S, (v1 - v0) * S));
         cudaEvent_t e = nullptr;
         CTR_TRY(event_at(ctx, c, &e));
         CTR_CUDA(cudaEventRecord(e, up));
     }
+    int converted = 0;  // chunks [0, converted) are in FP32
     for (int c = 0; c < nch; ++c) {
         const int v0 = c * kHostChunkViews, v1 = std::min(P, v0 + kHostChunkViews);
-        cudaEvent_t need = nullptr;  // this chunk and the first view of the next (derivative neighbour)
-        CTR_TRY(event_at(ctx, std::min(c + 1, nch - 1), &need));
-        CTR_CUDA(cudaStreamWaitEvent(comp, need, 0));
+        // this chunk and the first view of the next (derivative neighbour)
+        const int need = std::min(c + 1, nch - 1);
+        for (; converted <= need; ++converted) {
+            cudaEvent_t e = nullptr;
+            CTR_TRY(event_at(ctx, converted, &e));
+            CTR_CUDA(cudaStreamWaitEvent(comp, e, 0));
+            const size_t w0 = (size_t)converted * kHostChunkViews;
+            const size_t w1 = std::min<size_t>(P, w0 + kHostChunkViews);
+            CTR_TRY(launch_convert_f64_to_f32(comp, ctx->ws_a.as<double>() + w0 * S,
+                                              ctx->ws_b.as<float>() + w0 * S, (w1 - w0) * S));
+        }
         CTR_TRY(launch_filter(ctx, comp, *plan, ctx->ws_b.as<float>(), 0, P,
                               ctx->ws_c.as<float>(), 0, v0, v1));
         if (fproj_host) {
@@ -717,9 +726,6 @@ static Status host_bkproj_windowed(ctrecon_ctx* ctx, BPPlan& plan, const double*
                                             fproj + (size_t)c0 * S, m * sizeof(double),
                                             cudaMemcpyHostToDevice, up);
             if (e != cudaSuccess) st = cuda_status(e, "FProj upload");
-            if (st.ok())
-                st = launch_convert_f64_to_f32(up, ctx->ws_a.as<double>() + (size_t)c0 * S,
-                                               ctx->ws_c.as<float>() + (size_t)c0 * S, m);
         }
         cudaEvent_t ev = nullptr;
         if (st.ok()) st = event_at(ctx, 2 + (size_t)w, &ev);
@@ -728,6 +734,12 @@ static Status host_bkproj_windowed(ctrecon_ctx* ctx, BPPlan& plan, const double*
             if (e == cudaSuccess) e = cudaStreamWaitEvent(comp, ev, 0);
             if (e != cudaSuccess) st = cuda_status(e, "window event");
         }
+        // the window's conversion on the compute stream (copies only on the up stream: a
+        // kernel there would wait for SMs behind the backprojection and stall the copy engine)
+        if (st.ok())
+            st = launch_convert_f64_to_f32(comp, ctx->ws_a.as<double>() + (size_t)v0 * S,
+                                           ctx->ws_c.as<float>() + (size_t)v0 * S,
+                                           (size_t)(v1 - v0) * S);
         if (st.ok()) {
             plan.kp.win0 = v0;
             plan.kp.win1 = v1 - 1;
