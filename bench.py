@@ -14,6 +14,8 @@ loop count sum(LoopEnd - LoopBegin + 1) over written voxels (KatsevichBkProj.cpp
 taken from the bisection PI solve and used for every variant. `value` is updates / step
 time of the device-resident chain (all ranks' updates / max-over-ranks time); `e2e` is the
 same through the MEX-equivalent host calls (FP64 host buffers, copies in the timed region).
+With the plain options (the default), `mixed_learned` times the other side of the metric on
+the same resident inputs: BF16x3 Hilbert and the learned PI start (`vs_plain` = its speed-up).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--hilbert fp32|bf16x3|tf32] [--pi bisect|newton|learned]
@@ -54,6 +56,8 @@ def parse():
     ap.add_argument("--config", default="c2")
     ap.add_argument("--hilbert", default="fp32", choices=["fp32", "bf16x3", "tf32"])
     ap.add_argument("--pi", default="bisect", choices=["bisect", "newton", "learned"])
+    ap.add_argument("--no-mixed", action="store_true",
+                    help="skip the mixed + learned measurement beside the plain line")
     ap.add_argument("--pinet-mode", default="grid", choices=["voxel-fp32", "voxel-bf16", "grid"],
                     help="learned PI solve: the network per voxel (FP32 or packed BF16 SiLU) or "
                          "on the (r, psi) screw-symmetry grid, interpolated (default)")
@@ -843,6 +847,43 @@ def main():
         per = max(1, (8 << 30) // plane)
         launches_per_step += 2 * ((s.P + per - 1) // per) - 1
 
+    # ---- the mixed-precision + learned form on the same resident inputs ----------------------
+    # (the metric compares plain FP32 against it): BF16x3 Hilbert, the learned PI start, the same
+    # backprojector form; reported beside the plain line, not as its value
+    mixed = None
+    if hil == _lib.HILBERT_FP32 and pis == _lib.PI_BISECT and not args.no_mixed:
+        import ctypes
+        if pinet_info is None:
+            loss = ctypes.c_float()
+            _lib.check(_lib.lib().ctrecon_pinet_train(
+                ctx.handle, stream.cuda_stream, 1 << 22, 8192, 8, s.ObjR / s.ScanR * 1.05,
+                2024, ctypes.byref(loss)), ctx.handle)
+        ctx.set_option(_lib.OPT_HILBERT, _lib.HILBERT_BF16X3)
+        ctx.set_option(_lib.OPT_PI_SOLVER, _lib.PI_LEARNED)
+        for k in ev:
+            ev[k].clear()
+        for _ in range(max(3, args.warmup)):
+            step(False)
+        torch.cuda.synchronize()
+        barrier(ws)
+        m0, m1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        m0.record(stream)
+        for _ in range(args.steps):
+            step(True)
+        m1.record(stream)
+        torch.cuda.synchronize()
+        barrier(ws)
+        mms = max_over_ranks(m0.elapsed_time(m1) / args.steps, ws)
+        mixed = {"value": ws * updates / (mms / 1e3) / 1e9, "unit": "GUPS", "ms_per_step": mms,
+                 "hilbert": "bf16x3", "pi_solver": "learned",
+                 "phase_ms": {
+                     "filter": statistics.mean(a.elapsed_time(b) for a, b in zip(ev["f0"], ev["f1"])),
+                     "pi": statistics.mean(a.elapsed_time(b) for a, b in zip(ev["f1"], ev["p1"])),
+                     "bkproj": statistics.mean(a.elapsed_time(b) for a, b in zip(ev["p1"], ev["b1"]))},
+                 "vs_plain": ms_step / mms}
+        ctx.set_option(_lib.OPT_HILBERT, hil)
+        ctx.set_option(_lib.OPT_PI_SOLVER, pis)
+
     # ---- e2e through the MEX-equivalent host calls (FP64 pinned host buffers) -----------------
     e2e = None
     if not args.no_e2e:
@@ -920,7 +961,8 @@ def main():
                 "bkproj_gups": updates / (bp_ms / 1e3) / 1e9,
                 "pinet": pinet_info, "bp_tune": tune,
                 "gpu_launches": launches_per_step * args.steps,
-                "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks}
+                "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
+                "mixed_learned": mixed}
         print(json.dumps(line))
     ctx.close()
     if ws > 1:
