@@ -842,9 +842,10 @@ def main():
     if pis == _lib.PI_LEARNED:
         launches_per_step += 1  # the network's inference kernel before the Newton solve
     if 10 <= bp_form < 100:
-        # the fifth form writes the cell records of each view window (8 GiB) before its launch
+        # the fifth form writes the cell records of each view window (up to 32 GiB) before its
+        # launch
         plane = (s.ZL - 1) * (s.YL - 1) * 16
-        per = max(1, (8 << 30) // plane)
+        per = max(1, (32 << 30) // plane)
         launches_per_step += 2 * ((s.P + per - 1) // per) - 1
 
     # ---- the mixed-precision + learned form on the same resident inputs ----------------------

@@ -725,7 +725,8 @@ static Status launch_v5(cudaStream_t s, BPPlan& plan, const BPParams& kp, const 
 }
 
 // Variants 10, 11, 12: (NB, S, CTAs per SM) = (4, 3, 3), (4, 4, 2), (8, 2, 2). The loop views
-// [win0, win1] of the plan are backprojected in windows whose cell records fit kRecBudget (and
+// [win0, win1] of the plan are backprojected in windows whose cell records fit kRecBudget and
+// half of the free device memory (beside the records already held) (and
 // of at most max_views views when that is > 0);
 // with more than one window the valid voxels are zeroed first (or kept, when the plan
 // accumulates) and every window adds its sum.
@@ -792,7 +793,10 @@ Status launch_bkproj_v5(int variant, cudaStream_t s, BPPlan& plan, const float* 
     const int w0 = std::max(0, kp0.win0), w1 = std::min(kp0.P - 1, kp0.win1);
     if (w1 < w0) return Status::Ok();
     const int nv_all = w1 - w0 + 1;
-    int per = (int)std::max<size_t>(1, std::min<size_t>(nv_all, kRecBudget / plane));
+    size_t free_b = 0, total_b = 0;
+    CTR_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    const size_t budget = std::min(kRecBudget, (free_b + recbuf.bytes) / 2);
+    int per = (int)std::max<size_t>(1, std::min<size_t>(nv_all, budget / plane));
     if (max_views > 0) per = std::min(per, max_views);
     const int nwin = (nv_all + per - 1) / per;
     CTR_TRY(recbuf.ensure((size_t)std::min(per, nv_all) * plane, "cell records"));

@@ -249,8 +249,9 @@ Status launch_bkproj_f64out(ctrecon_ctx* ctx, cudaStream_t s, BPPlan& plan,
 Status launch_convert_f64_to_f32(cudaStream_t s, const double* in, float* out, size_t n);
 Status launch_zero_valid_f64(cudaStream_t s, const PiRecord* d_pitab, double* d_image, size_t n);
 // Fifth form (variants 10..12, bkproj2.cu): cell records of at most kRecBudget bytes of views
-// at a time in `recbuf`, then the backprojection of those views.
-constexpr size_t kRecBudget = (size_t)8 << 30;
+// at a time in `recbuf` (and no more than half of the free device memory), then the
+// backprojection of those views.
+constexpr size_t kRecBudget = (size_t)32 << 30;
 constexpr int kMaxBPVariant = 12;
 // the driver's cuTensorMapEncodeTiled (nullptr when unavailable), hilbert_tc.cu
 void* tensor_map_encoder();

@@ -127,7 +127,8 @@ typedef enum ctrecon_option {
     CTRECON_OPT_VERBOSE = 5,
     CTRECON_OPT_DERIVATIVE = 6,       /* CTRECON_DERIV_*; default CHAIN (the MEX filter's) */
     CTRECON_OPT_BP_WINDOW = 7,        /* views per cell-record window of variants 10..12;
-                                         0 (default) = as many as 8 GiB of records hold */
+                                         0 (default) = as many as 32 GiB of records hold,
+                                         and at most half of the free device memory */
     CTRECON_OPT_PINET_MODE = 8        /* how the learned PI solve evaluates the network:
                                          CTRECON_PINET_* below */
 } ctrecon_option;
