@@ -17,8 +17,10 @@
 //    border, is read directly from FProj with the first form's clamped indices.
 //  * REC = true (the fifth form): the cell records of every view were written to global memory
 //    beforehand (k_cell_records); a single producer warp computes the footprints and brings
-//    each footprint row into the ring with one cp.async.bulk (complete_tx on `full`), so no
-//    thread builds records and no raw rows are staged.
+//    each into the ring with ONE tensor copy of the smallest box of the box-map table that
+//    holds it (complete_tx on `full`), so no thread builds records and no raw rows are staged.
+//    One copy per view instead of one per footprint row: the copies were bound by their
+//    request rate, not their bytes.
 #pragma once
 
 #include "bp_tile3.cuh"
@@ -56,15 +58,6 @@ __device__ __forceinline__ void tma_load_cells(uint32_t dst, const void* map, in
         "l"((uint64_t)map), "r"(0), "r"(u), "r"(v), "r"(view), "r"(smem_addr(bar))
         : "memory");
 }
-// global -> shared bulk copy (16-byte aligned addresses, size a multiple of 16) completing
-// `bytes` of the barrier's transaction count
-__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes,
-                                         uint64_t* bar) {
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-        ::"r"(dst), "l"(src), "r"(bytes), "r"(smem_addr(bar)) : "memory");
-}
-
 // The bilinear record of the cell between detector samples (r, c) .. (r + 1, c + 1), for
 // offsets alpha - 1/2, beta - 1/2 from the cell centre: value = A + a B + b (C + a D).
 __device__ __forceinline__ float4 cell_record(float t00, float t01, float t10, float t11) {
