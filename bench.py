@@ -154,7 +154,10 @@ class ClockSampler:
         return out
 
 
-def dist_setup(n):
+def dist_setup(n, backend=None):
+    """One process per GPU (torchrun's RANK / LOCAL_RANK / WORLD_SIZE). The ranks are
+    replicas: each reconstructs its own scan and only the timing is reduced. NCCL on GPUs,
+    gloo without them (the CPU tests of this plumbing)."""
     import torch
     import torch.distributed as dist
     ws = int(os.environ.get("WORLD_SIZE", "1"))
@@ -162,9 +165,11 @@ def dist_setup(n):
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if ws > 1:
         from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
-    torch.cuda.set_device(local)
+        backend = backend or ("nccl" if torch.cuda.is_available() else "gloo")
+        extra = {"device_id": torch.device("cuda", local)} if backend == "nccl" else {}
+        dist.init_process_group(backend, timeout=timedelta(seconds=300), **extra)
+    if torch.cuda.is_available():
+        torch.cuda.set_device(local)
     return ws, rank, local
 
 
@@ -175,13 +180,21 @@ def barrier(ws):
 
 
 def max_over_ranks(x, ws):
+    """The largest of the ranks' x (every rank gets it): step times are the slowest rank's."""
     if ws == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def replica_gups(updates, ms_step, ws):
+    """Whole-job throughput of ws replicas, each doing `updates` per step, timed by the
+    slowest (ms_step = max over ranks)."""
+    return ws * updates / (ms_step / 1e3) / 1e9
 
 
 # ---------------------------------------------------------------------------------------------
@@ -833,7 +846,7 @@ def main():
     filt_ms = statistics.mean(a.elapsed_time(b) for a, b in zip(ev["f0"], ev["f1"]))
     pi_ms = statistics.mean(a.elapsed_time(b) for a, b in zip(ev["f1"], ev["p1"]))
     bp_ms = statistics.mean(a.elapsed_time(b) for a, b in zip(ev["p1"], ev["b1"]))
-    value = ws * updates / (ms_step / 1e3) / 1e9
+    value = replica_gups(updates, ms_step, ws)
     chunk = ctx.get_option(_lib.OPT_FILTER_CHUNK)
     nchunks = (s.P + chunk - 1) // chunk
     launches_per_step = 2 * nchunks + 1 + 1
@@ -875,7 +888,7 @@ def main():
         torch.cuda.synchronize()
         barrier(ws)
         mms = max_over_ranks(m0.elapsed_time(m1) / args.steps, ws)
-        mixed = {"value": ws * updates / (mms / 1e3) / 1e9, "unit": "GUPS", "ms_per_step": mms,
+        mixed = {"value": replica_gups(updates, mms, ws), "unit": "GUPS", "ms_per_step": mms,
                  "hilbert": "bf16x3", "pi_solver": "learned",
                  "phase_ms": {
                      "filter": statistics.mean(a.elapsed_time(b) for a, b in zip(ev["f0"], ev["f1"])),
