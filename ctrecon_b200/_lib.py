@@ -94,6 +94,7 @@ SIGNATURES = [
     ("ctrecon_bkproj_dev_f32", _st, [_vp, _vp, ctypes.POINTER(BPGeom), _vp, _vp, _vp]),
     ("ctrecon_filter_mode1_dev_f32", _st, [_vp, _vp, ctypes.POINTER(FilterParams), _vp, _vp]),
     ("ctrecon_filter_noalloc_dev_f32", _st, [_vp, ctypes.POINTER(FilterParams), _vp, _vp]),
+    ("ctrecon_selftest_bounded_wait", _st, [_vp, _vp, ctypes.c_int]),
     ("ctrecon_sync", _st, [_vp, _vp]),
     ("ctrecon_pi_dev_stats", _st, [_vp, _vp, ctypes.POINTER(BPGeom), _vp, _vp, _vp]),
     ("ctrecon_batch_create", _st, [_vp, ctypes.c_int, ctypes.POINTER(FilterParams),

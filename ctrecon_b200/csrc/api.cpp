@@ -209,6 +209,17 @@ extern "C" {
 
 int ctrecon_abi_version(void) { return CTRECON_ABI_VERSION; }
 
+ctrecon_status ctrecon_selftest_bounded_wait(ctrecon_ctx* ctx, void* stream, int limit_ms) {
+    if (!ctx) return CTRECON_ERR_INVALID_ARGUMENT;
+    API_BEGIN
+    if (limit_ms < 1 || limit_ms > 10000)
+        return finish(ctx, make_status(CTRECON_ERR_INVALID_ARGUMENT, "limit_ms must be 1..10000"));
+    Status s = use_device(ctx);
+    if (s.ok()) s = selftest_bounded_wait(ctx, (cudaStream_t)stream, limit_ms);
+    return finish(ctx, s);
+    API_END(ctx)
+}
+
 const char* ctrecon_status_string(ctrecon_status s) {
     switch (s) {
     case CTRECON_OK: return "ok";

@@ -253,6 +253,9 @@ Status launch_zero_valid_f64(cudaStream_t s, const PiRecord* d_pitab, double* d_
 // backprojection of those views.
 constexpr size_t kRecBudget = (size_t)32 << 30;
 constexpr int kMaxBPVariant = 12;
+// selftest.cu: a bounded wait that nothing completes must give up within limit_ms and be
+// reported (returns CTRECON_ERR_TIMEOUT when the mechanism works)
+Status selftest_bounded_wait(ctrecon_ctx* ctx, cudaStream_t s, int limit_ms);
 // the driver's cuTensorMapEncodeTiled (nullptr when unavailable), hilbert_tc.cu
 void* tensor_map_encoder();
 // Fifth form building blocks (bkproj2.cu): the box-map table over cell records of `nviews`

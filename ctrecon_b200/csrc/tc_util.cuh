@@ -44,7 +44,8 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t a, uint32_t parity) {
 // bounded wait on the phase with the given parity; false if it gave up (error recorded) or
 // another thread of the launch already gave up. The error word and the timer are read every
 // 64 tries only, so a short wait costs little more than its try_wait instructions.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err, int code) {
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err, int code,
+                                          uint64_t limit_ns = kWaitLimitNs) {
     const uint32_t a = smem_u32(bar);
     if (mbar_try_wait(a, parity)) return true;
     uint64_t t0 = 0;
@@ -54,7 +55,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* e
             if (*(volatile int*)err) return false;
             const uint64_t t = globaltimer_ns();
             if (t0 == 0) t0 = t;
-            else if (t - t0 > kWaitLimitNs) break;
+            else if (t - t0 > limit_ns) break;
         }
     }
     atomicCAS(err, 0, code);

@@ -395,6 +395,14 @@ ctrecon_status ctrecon_imgfile_read(const char* path, ctrecon_imgfile_header* h,
 ctrecon_status ctrecon_imgfile_write(const char* path, const ctrecon_imgfile_header* h,
                                      const double* data);
 
+/* ---- failure detection ------------------------------------------------------------------ */
+/* Every pipelined kernel of the library bounds its waits (2 s of %globaltimer): a wait that
+ * gives up records a code in the context's device error word, the kernel returns, and the call
+ * reports CTRECON_ERR_TIMEOUT. This self-test runs that mechanism on a wait that nothing ever
+ * completes (limit_ms, 1..10000): it returns CTRECON_ERR_TIMEOUT when the wait gave up and was
+ * reported, CTRECON_ERR_INTERNAL otherwise; the context stays usable. */
+ctrecon_status ctrecon_selftest_bounded_wait(ctrecon_ctx* ctx, void* stream, int limit_ms);
+
 #ifdef __cplusplus
 }
 #endif
