@@ -168,19 +168,24 @@ def test_pinet_training_inference_and_gain(torch_mod):
     assert lrn["grid"]["iters"] <= 1.02 * lrn["voxel-fp32"]["iters"]
 
 
-@pytest.mark.parametrize("name", ["c1", "c2s"])
+@pytest.mark.parametrize("name", ["c1", "c2s", "ragged"])
 def test_backprojector_variants_agree(torch_mod, name):
     """Every tiled form (0, 1: per-cell records; 2-4: second form; 5-9: per-cell records
     staged by producer warps; 10-12: per-cell records copied from device memory) against the
     first form; variant 10 also in windows of 300 views (valid voxels zeroed, then every
     window accumulated).
     c1's 16-row detector sends most tiles through the direct-read fallback, c2s's 64 rows
-    almost none."""
+    almost none; "ragged" has partial tiles in x, y and z (45 x 37 x 13 voxels)."""
     torch = torch_mod
     import ctrecon_b200 as ct
     from ctrecon_b200 import _lib
     from ctrecon_b200.geometry import config
-    s = config(name)
+    if name == "ragged":  # partial tiles in x, y and z; footprints on the cell path
+        from ctrecon_b200.geometry import small_config
+        s = small_config(name="ragged", YL=200, ZL=48, views_per_turn=120, turns=2.5, NX=45,
+                         NY=37, NZ=13, voxel=(0.5, 0.5, 0.5), seed=5)
+    else:
+        s = config(name)
     outs = {}
     with ct.Context(0) as cx:
         g = s.geom_struct()
