@@ -70,6 +70,32 @@ __device__ __forceinline__ float4 cell_record(float t00, float t01, float t10, f
 // slack of the footprint bounds, in detector cells
 constexpr float kFootMargin = 0.0625f;
 
+// packed FP32 pairs (sm_100 f32x2 arithmetic): two slices' v coordinate, floor and distance
+// in one instruction each; the halves are the two 32-bit registers of the pair
+__device__ __forceinline__ uint64_t pk2(float lo, float hi) {
+    uint64_t r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ void upk2(uint64_t v, float& lo, float& hi) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ uint64_t ffma2(uint64_t a, uint64_t b, uint64_t c) {
+    uint64_t d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+__device__ __forceinline__ uint64_t fadd2(uint64_t a, uint64_t b) {
+    uint64_t d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ uint64_t fsub2(uint64_t a, uint64_t b) {
+    uint64_t d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+
 struct Caps4 {
     int cells;  // cell records per staged view (multiple of 4)
     int raw;    // raw floats per staged view (multiple of 4)
@@ -110,8 +136,9 @@ __device__ __forceinline__ void tile4_init(Shared4<NB, S, PW>& sh) {
 // One CTA tile: columns [16 bx, 16 bx + 16) x [16 by, 16 by + 16), slices [8 bz, 8 bz + 8).
 // Called by all 32 * (8 + PW) threads with the same `iter` (blocks of views this CTA has
 // processed before); returns the new count. Returns with no copies in flight. Sets
-// sh.s_abort (and leaves the tile unwritten) when a wait gave up.
-template <int NB, int S, int PW, bool REC, typename OutT>
+// sh.s_abort (and leaves the tile unwritten) when a wait gave up. PK2: unweighted updates of
+// two slices share their packed FP32x2 arithmetic (needs about 8 more registers per thread).
+template <int NB, int S, int PW, bool REC, typename OutT, bool PK2 = false>
 __device__ __forceinline__ uint32_t tile4(const BPParams& kp, const float* __restrict__ fproj,
                                           const PiRecord* __restrict__ pit,
                                           const float4* __restrict__ views,
@@ -384,6 +411,26 @@ __device__ __forceinline__ uint32_t tile4(const BPParams& kp, const float* __res
             const float4 q = lds128((uint32_t)__float_as_int(tv) * W16 + cbase);
             acc[k] = fmaf(fmaf(b, fmaf(a, q.w, q.z), fmaf(a, q.y, q.x)), rinv, acc[k]);
         };
+        // slices k and k + 1 (k even) with their v coordinate, rounding floor and squared
+        // distance in packed pairs; the same operations as cell_update, rounded the same way
+        const uint64_t dzf2 = pk2(dzf, dzf), hz2 = pk2(HalfZm, HalfZm), mag2 = pk2(kMagic, kMagic);
+        auto cell_update2 = [&](int k, uint64_t dz02, uint64_t kv2, uint64_t r22, float a,
+                                uint32_t W16, uint32_t cbase) {
+            const uint64_t dz = ffma2(pk2((float)k, (float)(k + 1)), dzf2, dz02);
+            const uint64_t v = ffma2(dz, kv2, hz2);  // v - 1/2
+            const uint64_t tv = fadd2(v, mag2);
+            const uint64_t b = fsub2(v, fsub2(tv, mag2));
+            float t0, t1, tv0, tv1, b0, b1;
+            upk2(ffma2(dz, dz, r22), t0, t1);
+            upk2(tv, tv0, tv1);
+            upk2(b, b0, b1);
+            const float4 q0 = lds128((uint32_t)__float_as_int(tv0) * W16 + cbase);
+            const float4 q1 = lds128((uint32_t)__float_as_int(tv1) * W16 + cbase);
+            acc[k] = fmaf(fmaf(b0, fmaf(a, q0.w, q0.z), fmaf(a, q0.y, q0.x)), rsqrt_approx(t0),
+                          acc[k]);
+            acc[k + 1] = fmaf(fmaf(b1, fmaf(a, q1.w, q1.z), fmaf(a, q1.y, q1.x)),
+                              rsqrt_approx(t1), acc[k + 1]);
+        };
         auto cell_update_w = [&](int k, int p, float dz0, float kv, float r2, float a,
                                  uint32_t W16, uint32_t cbase) {
             const int d0 = p - vr.bi[k];
@@ -432,8 +479,15 @@ __device__ __forceinline__ uint32_t tile4(const BPParams& kp, const float* __res
                     const float a = u - (tu - kMagic);           // alpha - 1/2
                     const uint32_t W16 = (uint32_t)kw.y;
                     const uint32_t cbase = (uint32_t)__float_as_int(tu) * 16u + (uint32_t)kw.x;
+                    if constexpr (PK2) {
+                        const uint64_t dz02 = pk2(dz0, dz0), kv2 = pk2(kv, kv), r22 = pk2(r2, r2);
 #pragma unroll
-                    for (int k = 0; k < TZ; ++k) cell_update(k, dz0, kv, r2, a, W16, cbase);
+                        for (int k = 0; k < TZ; k += 2)
+                            cell_update2(k, dz02, kv2, r22, a, W16, cbase);
+                    } else {
+#pragma unroll
+                        for (int k = 0; k < TZ; ++k) cell_update(k, dz0, kv, r2, a, W16, cbase);
+                    }
                 }
             } else if (col_ok && wmin <= wmax && !(pb + NB - 1 < wmin || pb > wmax)) {
 #pragma unroll 1
@@ -460,9 +514,17 @@ __device__ __forceinline__ uint32_t tile4(const BPParams& kp, const float* __res
 #pragma unroll
                         for (int h = 0; h < NG; ++h) {
                             if (fm & (1u << h)) {
+                                if constexpr (PK2) {
+                                    const uint64_t dz02 = pk2(dz0, dz0), kv2 = pk2(kv, kv),
+                                                   r22 = pk2(r2, r2);
 #pragma unroll
-                                for (int k = h * GS; k < (h + 1) * GS; ++k)
-                                    cell_update(k, dz0, kv, r2, a, W16, cbase);
+                                    for (int k = h * GS; k < (h + 1) * GS; k += 2)
+                                        cell_update2(k, dz02, kv2, r22, a, W16, cbase);
+                                } else {
+#pragma unroll
+                                    for (int k = h * GS; k < (h + 1) * GS; ++k)
+                                        cell_update(k, dz0, kv, r2, a, W16, cbase);
+                                }
                             } else {
 #pragma unroll
                                 for (int k = h * GS; k < (h + 1) * GS; ++k)
