@@ -6,7 +6,7 @@
 //  * Warp roles. Warps 0-7 (the 16 x 16 voxel columns of the tile, 8 slices each) only
 //    accumulate. PW producer warps compute the footprints of each block of NB views, copy the
 //    raw footprint rows with cp.async two blocks ahead, and build the 16-byte cell records
-//    {A, B, C, D} into a ring of S slots.
+//    {A, C, B, D} into a ring of S slots.
 //  * Hand-off. Slot s has a `full` mbarrier (every producer thread arrives after writing its
 //    records) and an `empty` one (every consumer thread arrives after its last read); phases
 //    follow a per-CTA block counter, so the ring runs on across the tiles of the persistent
@@ -59,11 +59,13 @@ __device__ __forceinline__ void tma_load_cells(uint32_t dst, const void* map, in
         : "memory");
 }
 // The bilinear record of the cell between detector samples (r, c) .. (r + 1, c + 1), for
-// offsets alpha - 1/2, beta - 1/2 from the cell centre: value = A + a B + b (C + a D).
+// offsets alpha - 1/2, beta - 1/2 from the cell centre: value = A + a B + b (C + a D), stored
+// {A, C, B, D} so that the two halves of the 16-byte record give (A + a B, C + a D) in one
+// packed FP32x2 fma.
 __device__ __forceinline__ float4 cell_record(float t00, float t01, float t10, float t11) {
     const float h0 = t01 - t00, h1 = t11 - t10;
     const float g0 = t10 - t00, g1 = t11 - t01;
-    return make_float4(0.25f * ((t00 + t01) + (t10 + t11)), 0.5f * (h0 + h1), 0.5f * (g0 + g1),
+    return make_float4(0.25f * ((t00 + t01) + (t10 + t11)), 0.5f * (g0 + g1), 0.5f * (h0 + h1),
                        h1 - h0);
 }
 
@@ -94,6 +96,20 @@ __device__ __forceinline__ uint64_t fsub2(uint64_t a, uint64_t b) {
     uint64_t d;
     asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
     return d;
+}
+
+// a cell record as its two 64-bit halves {A, C} and {B, D}
+__device__ __forceinline__ void lds_record(uint32_t addr, uint64_t& ac, uint64_t& bd) {
+    asm volatile("ld.shared.v2.b64 {%0, %1}, [%2];" : "=l"(ac), "=l"(bd) : "r"(addr));
+}
+// the record's value at cell offsets (a, b), a2 = (a, a): A + a B + b (C + a D), rounded as
+// fma(b, fma(a, D, C), fma(a, B, A))
+__device__ __forceinline__ float record_value(uint32_t addr, uint64_t a2, float b) {
+    uint64_t ac, bd;
+    lds_record(addr, ac, bd);
+    float lo, hi;
+    upk2(ffma2(a2, bd, ac), lo, hi);
+    return fmaf(b, hi, lo);
 }
 
 struct Caps4 {
@@ -372,11 +388,12 @@ __device__ __forceinline__ uint32_t tile4(const BPParams& kp, const float* __res
         const float z0 = zc[zb];
         const float dzf = kp.dzf;
         const float HalfYm = HalfY - 0.5f, HalfZm = HalfZ - 0.5f;
-        // Slices 4h .. 4h + 3 form group h. A group takes the unweighted path for a block when
-        // every voxel of the group, in every lane of the warp, has weight 1 at all the block's
-        // views: [gflo[h], gfhi[h]] is that warp-wide view range (empty if any voxel of the
-        // group has no PI interval). Deciding per group halves the views whose weights are
-        // tested: the PI ranges of a column's slices are shifted against each other.
+        // Slices 4h .. 4h + 3 form group h. A group takes the unweighted path at a view when
+        // every voxel of the group, in every lane of the warp, has weight 1 there: [gflo[h],
+        // gfhi[h]] is that warp-wide view range (empty if any voxel of the group has no PI
+        // interval). A block whose views all lie in both groups' ranges skips the per-view
+        // tests. Deciding per group halves the views whose weights are tested: the PI ranges of
+        // a column's slices are shifted against each other.
         constexpr int GS = 4, NG = TZ / GS;
         int gflo[NG], gfhi[NG];
 #pragma unroll
@@ -401,20 +418,20 @@ __device__ __forceinline__ uint32_t tile4(const BPParams& kp, const float* __res
             gfhi[h] = hi;
         }
         // one voxel's update from cell records, weighted (w) or not
-        auto cell_update = [&](int k, float dz0, float kv, float r2, float a, uint32_t W16,
+        auto cell_update = [&](int k, float dz0, float kv, float r2, uint64_t a2, uint32_t W16,
                                uint32_t cbase) {
             const float dz = fmaf((float)k, dzf, dz0);
             const float v = fmaf(dz, kv, HalfZm);  // v - 1/2
             const float rinv = rsqrt_approx(fmaf(dz, dz, r2));
             const float tv = v + kMagic;
             const float b = v - (tv - kMagic);
-            const float4 q = lds128((uint32_t)__float_as_int(tv) * W16 + cbase);
-            acc[k] = fmaf(fmaf(b, fmaf(a, q.w, q.z), fmaf(a, q.y, q.x)), rinv, acc[k]);
+            const float val = record_value((uint32_t)__float_as_int(tv) * W16 + cbase, a2, b);
+            acc[k] = fmaf(val, rinv, acc[k]);
         };
         // slices k and k + 1 (k even) with their v coordinate, rounding floor and squared
         // distance in packed pairs; the same operations as cell_update, rounded the same way
         const uint64_t dzf2 = pk2(dzf, dzf), hz2 = pk2(HalfZm, HalfZm), mag2 = pk2(kMagic, kMagic);
-        auto cell_update2 = [&](int k, uint64_t dz02, uint64_t kv2, uint64_t r22, float a,
+        auto cell_update2 = [&](int k, uint64_t dz02, uint64_t kv2, uint64_t r22, uint64_t a2,
                                 uint32_t W16, uint32_t cbase) {
             const uint64_t dz = ffma2(pk2((float)k, (float)(k + 1)), dzf2, dz02);
             const uint64_t v = ffma2(dz, kv2, hz2);  // v - 1/2
@@ -424,14 +441,12 @@ __device__ __forceinline__ uint32_t tile4(const BPParams& kp, const float* __res
             upk2(ffma2(dz, dz, r22), t0, t1);
             upk2(tv, tv0, tv1);
             upk2(b, b0, b1);
-            const float4 q0 = lds128((uint32_t)__float_as_int(tv0) * W16 + cbase);
-            const float4 q1 = lds128((uint32_t)__float_as_int(tv1) * W16 + cbase);
-            acc[k] = fmaf(fmaf(b0, fmaf(a, q0.w, q0.z), fmaf(a, q0.y, q0.x)), rsqrt_approx(t0),
-                          acc[k]);
-            acc[k + 1] = fmaf(fmaf(b1, fmaf(a, q1.w, q1.z), fmaf(a, q1.y, q1.x)),
-                              rsqrt_approx(t1), acc[k + 1]);
+            const float val0 = record_value((uint32_t)__float_as_int(tv0) * W16 + cbase, a2, b0);
+            const float val1 = record_value((uint32_t)__float_as_int(tv1) * W16 + cbase, a2, b1);
+            acc[k] = fmaf(val0, rsqrt_approx(t0), acc[k]);
+            acc[k + 1] = fmaf(val1, rsqrt_approx(t1), acc[k + 1]);
         };
-        auto cell_update_w = [&](int k, int p, float dz0, float kv, float r2, float a,
+        auto cell_update_w = [&](int k, int p, float dz0, float kv, float r2, uint64_t a2,
                                  uint32_t W16, uint32_t cbase) {
             const int d0 = p - vr.bi[k];
             const int d1 = vr.ti[k] + 1 - p;
@@ -444,8 +459,8 @@ __device__ __forceinline__ uint32_t tile4(const BPParams& kp, const float* __res
             const float rinv = rsqrt_approx(fmaf(dz, dz, r2));
             const float tv = v + kMagic;
             const float b = v - (tv - kMagic);
-            const float4 q = lds128((uint32_t)__float_as_int(tv) * W16 + cbase);
-            acc[k] = fmaf(w * fmaf(b, fmaf(a, q.w, q.z), fmaf(a, q.y, q.x)), rinv, acc[k]);
+            const float val = record_value((uint32_t)__float_as_int(tv) * W16 + cbase, a2, b);
+            acc[k] = fmaf(w * val, rinv, acc[k]);
         };
         for (int ib = 0; ib < nblk; ++ib) {
             const uint32_t g = iter + ib, slot = g % S, use = g / S;
@@ -457,11 +472,11 @@ __device__ __forceinline__ uint32_t tile4(const BPParams& kp, const float* __res
             bool blk = pb + NB - 1 <= pmax;  // a whole block of views with cell records
 #pragma unroll
             for (int j = 0; j < NB; ++j) blk = blk && (sh.foot[slot][j].W > 0);
-            unsigned fm = 0;  // bit h: group h unweighted for the whole block (warp-uniform)
+            bool all_fast = blk;  // every group unweighted for the whole block (warp-uniform)
 #pragma unroll
             for (int h = 0; h < NG; ++h)
-                fm |= (blk && pb >= gflo[h] && pb + NB - 1 <= gfhi[h]) ? 1u << h : 0u;
-            if (fm == (1u << NG) - 1) {
+                all_fast = all_fast && pb >= gflo[h] && pb + NB - 1 <= gfhi[h];
+            if (all_fast) {
                 // every view of the block has cell records and weight 1 for all voxels of the
                 // warp: no per-view tests
 #pragma unroll
@@ -477,16 +492,17 @@ __device__ __forceinline__ uint32_t tile4(const BPParams& kp, const float* __res
                     const float u = fmaf(YY * DdU, inv, HalfYm);  // u - 1/2
                     const float tu = u + kMagic;
                     const float a = u - (tu - kMagic);           // alpha - 1/2
+                    const uint64_t a2 = pk2(a, a);
                     const uint32_t W16 = (uint32_t)kw.y;
                     const uint32_t cbase = (uint32_t)__float_as_int(tu) * 16u + (uint32_t)kw.x;
                     if constexpr (PK2) {
                         const uint64_t dz02 = pk2(dz0, dz0), kv2 = pk2(kv, kv), r22 = pk2(r2, r2);
 #pragma unroll
                         for (int k = 0; k < TZ; k += 2)
-                            cell_update2(k, dz02, kv2, r22, a, W16, cbase);
+                            cell_update2(k, dz02, kv2, r22, a2, W16, cbase);
                     } else {
 #pragma unroll
-                        for (int k = 0; k < TZ; ++k) cell_update(k, dz0, kv, r2, a, W16, cbase);
+                        for (int k = 0; k < TZ; ++k) cell_update(k, dz0, kv, r2, a2, W16, cbase);
                     }
                 }
             } else if (col_ok && wmin <= wmax && !(pb + NB - 1 < wmin || pb > wmax)) {
@@ -507,28 +523,30 @@ __device__ __forceinline__ uint32_t tile4(const BPParams& kp, const float* __res
                         const float u = fmaf(YY * DdU, inv, HalfYm);  // u - 1/2
                         const float tu = u + kMagic;
                         const float a = u - (tu - kMagic);           // alpha - 1/2
+                        const uint64_t a2 = pk2(a, a);
                         const int2 kw = sh.kw[slot][j];
                         const uint32_t W16 = (uint32_t)kw.y;
                         const uint32_t cbase =
                             (uint32_t)__float_as_int(tu) * 16u + (uint32_t)kw.x;
 #pragma unroll
                         for (int h = 0; h < NG; ++h) {
-                            if (fm & (1u << h)) {
+                            // group h unweighted at this view for every lane (warp-uniform)
+                            if (p >= gflo[h] && p <= gfhi[h]) {
                                 if constexpr (PK2) {
                                     const uint64_t dz02 = pk2(dz0, dz0), kv2 = pk2(kv, kv),
                                                    r22 = pk2(r2, r2);
 #pragma unroll
                                     for (int k = h * GS; k < (h + 1) * GS; k += 2)
-                                        cell_update2(k, dz02, kv2, r22, a, W16, cbase);
+                                        cell_update2(k, dz02, kv2, r22, a2, W16, cbase);
                                 } else {
 #pragma unroll
                                     for (int k = h * GS; k < (h + 1) * GS; ++k)
-                                        cell_update(k, dz0, kv, r2, a, W16, cbase);
+                                        cell_update(k, dz0, kv, r2, a2, W16, cbase);
                                 }
                             } else {
 #pragma unroll
                                 for (int k = h * GS; k < (h + 1) * GS; ++k)
-                                    cell_update_w(k, p, dz0, kv, r2, a, W16, cbase);
+                                    cell_update_w(k, p, dz0, kv, r2, a2, W16, cbase);
                             }
                         }
                     } else {
