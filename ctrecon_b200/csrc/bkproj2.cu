@@ -328,17 +328,33 @@ k_bkproj5(BPParams kp, const float* __restrict__ fproj, const PiRecord* __restri
 }
 
 // The cell records of views [p0, p0 + nviews): rec[v][r][c] = cell_record of the samples
-// (r, c) .. (r + 1, c + 1) of view p0 + v, (ZL - 1) x (YL - 1) cells per view.
-__global__ void k_cell_records(const float* __restrict__ fproj, float4* __restrict__ rec, int p0,
-                               int nviews, int YL, int ZL) {
+// (r, c) .. (r + 1, c + 1) of view p0 + v, (ZL - 1) x (YL - 1) cells per view. A thread makes
+// the records of kRecRows rows of one column: all its loads are in flight at once (one cell per
+// thread was bound by the latency of its dependent loads), every sample row is read once, and
+// each store of a warp is 512 contiguous bytes.
+constexpr int kRecRows = 8;
+__global__ void __launch_bounds__(128) k_cell_records(const float* __restrict__ fproj,
+                                                      float4* __restrict__ rec, int p0,
+                                                      int nviews, int YL, int ZL) {
     const int RW = YL - 1, RH = ZL - 1;
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    const int r = blockIdx.y;
+    const int r0 = blockIdx.y * kRecRows;
     if (c >= RW) return;
+    const int nr = min(kRecRows, RH - r0);  // rows of records here; samples r0 .. r0 + nr
     for (int v = blockIdx.z; v < nviews; v += gridDim.z) {
-        const float* t = fproj + ((size_t)(p0 + v) * ZL + r) * YL + c;
-        rec[((size_t)v * RH + r) * RW + c] =
-            cell_record(__ldg(t), __ldg(t + 1), __ldg(t + YL), __ldg(t + YL + 1));
+        const float* t = fproj + ((size_t)(p0 + v) * ZL + r0) * YL + c;
+        float s0[kRecRows + 1], s1[kRecRows + 1];
+#pragma unroll
+        for (int i = 0; i <= kRecRows; ++i) {
+            if (i <= nr) {
+                s0[i] = __ldg(t + (size_t)i * YL);
+                s1[i] = __ldg(t + (size_t)i * YL + 1);
+            }
+        }
+        float4* o = rec + ((size_t)v * RH + r0) * RW + c;
+#pragma unroll
+        for (int i = 0; i < kRecRows; ++i)
+            if (i < nr) o[(size_t)i * RW] = cell_record(s0[i], s1[i], s0[i + 1], s1[i + 1]);
     }
 }
 
@@ -767,7 +783,8 @@ Status encode_box_maps(void* out, const void* rec, int RW, int RH, int nviews) {
 Status launch_cell_records(cudaStream_t s, const float* d_fproj, void* rec, int p0, int nviews,
                            int YL, int ZL) {
     if (nviews <= 0) return Status::Ok();
-    dim3 g((YL - 1 + 127) / 128, ZL - 1, (unsigned)std::min(nviews, 65535));
+    dim3 g((YL - 1 + 127) / 128, (ZL - 1 + kRecRows - 1) / kRecRows,
+           (unsigned)std::min(nviews, 65535));
     k_cell_records<<<g, 128, 0, s>>>(d_fproj, static_cast<float4*>(rec), p0, nviews, YL, ZL);
     CTR_CUDA(cudaGetLastError());
     return Status::Ok();
