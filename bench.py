@@ -65,7 +65,8 @@ def parse():
                     help="backprojector form: -1 autotuned on the workload before timing "
                          "(default), 0, 1 per-cell records (4 / 8 views per block), 2-4 second "
                          "form tile shapes, 5-9 per-cell records staged by producer warps, "
-                         "100 first form")
+                         "10-12 cell records written to HBM first and brought in by tensor "
+                         "copies, 100 first form")
     ap.add_argument("--batched", action="store_true",
                     help="16 uneven scans (c4): one-at-a-time vs one batched graph replay")
     ap.add_argument("--report", choices=["c3", "c5", "extras"],
