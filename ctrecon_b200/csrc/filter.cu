@@ -192,12 +192,26 @@ __global__ void k_hilbert_simt(const float* __restrict__ X, int AL, int ALpad, i
             for (int m = 0; m < 8; ++m) xs[(a0 + r) * kXS + q + 2 * (8 * s + m)] = acc[r][m];
     }
     __syncthreads();
-    // post-weight + backward rebin (:181-284): a gather across the kappa rows of the tile
-    for (int idx = tid; idx < ZL * kTileI; idx += nt) {
-        const int k = idx >> 6, t = idx & 63, i = i0 + t;
-        if (i >= YL) continue;
-        const BkEntry e = bk[(size_t)k * YL + i];
-        fproj[((size_t)v * ZL + k) * YL + i] = fmaf(e.gb, xs[e.b * kXS + t], e.ge * xs[e.e * kXS + t]);
+    // post-weight + backward rebin (:181-284): a gather across the kappa rows of the tile; the
+    // table entries of four outputs are loaded (read-only path) before their stores, so their
+    // latencies overlap
+    const int4* bk4 = reinterpret_cast<const int4*>(bk);
+    for (int idx0 = tid; idx0 < ZL * kTileI; idx0 += 4 * nt) {
+        int4 e[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const int idx = idx0 + r * nt, k = idx >> 6, i = i0 + (idx & 63);
+            e[r] = (idx < ZL * kTileI && i < YL) ? __ldg(bk4 + (size_t)k * YL + i)
+                                                 : make_int4(0, 0, 0, 0);
+        }
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const int idx = idx0 + r * nt, k = idx >> 6, t = idx & 63, i = i0 + t;
+            if (idx >= ZL * kTileI || i >= YL) continue;
+            fproj[((size_t)v * ZL + k) * YL + i] =
+                fmaf(__int_as_float(e[r].z), xs[e[r].x * kXS + t],
+                     __int_as_float(e[r].w) * xs[e[r].y * kXS + t]);
+        }
     }
 }
 

@@ -266,11 +266,27 @@ k_hilbert_tc(const __grid_constant__ CUtensorMap tA0, const __grid_constant__ CU
         const float* row = trq + lane * p.ALt;
         float* o = p.out + (size_t)vg0 * p.ZL * p.YL + i;
         const size_t vstride = (size_t)p.ZL * p.YL;
-        for (int k = h; k < p.ZL; k += 2) {
-            const BkEntry e = p.bk[(size_t)k * p.YL + i];
-            float* ok = o + (size_t)k * p.YL;
-            for (int vl = 0; vl < nv; ++vl)
-                ok[vl * vstride] = fmaf(e.gb, row[vl * p.AL + e.b], e.ge * row[vl * p.AL + e.e]);
+        // the table entries of kEpiRows rows are loaded (read-only path) before any of their
+        // stores, so their latencies overlap instead of queueing behind the previous row's
+        constexpr int kEpiRows = 8;
+        const int4* bk4 = reinterpret_cast<const int4*>(p.bk);
+        for (int k0 = h; k0 < p.ZL; k0 += 2 * kEpiRows) {
+            int4 e[kEpiRows];
+#pragma unroll
+            for (int r = 0; r < kEpiRows; ++r) {
+                const int k = k0 + 2 * r;
+                e[r] = k < p.ZL ? __ldg(bk4 + (size_t)k * p.YL + i) : make_int4(0, 0, 0, 0);
+            }
+#pragma unroll
+            for (int r = 0; r < kEpiRows; ++r) {
+                const int k = k0 + 2 * r;
+                if (k >= p.ZL) break;
+                const float gb = __int_as_float(e[r].z), ge = __int_as_float(e[r].w);
+                float* ok = o + (size_t)k * p.YL;
+                for (int vl = 0; vl < nv; ++vl)
+                    ok[vl * vstride] =
+                        fmaf(gb, row[vl * p.AL + e[r].x], ge * row[vl * p.AL + e[r].y]);
+            }
         }
     }
     tc_fence_before();
