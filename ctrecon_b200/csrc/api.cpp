@@ -483,7 +483,8 @@ ctrecon_status ctrecon_pi_dev(ctrecon_ctx* ctx, void* stream, const ctrecon_bp_g
     if (!ctx) return CTRECON_ERR_INVALID_ARGUMENT;
     API_BEGIN
     if (!g || !d_pitab) return finish(ctx, make_status(CTRECON_ERR_INVALID_ARGUMENT, "NULL argument"));
-    Status s = use_device(ctx);
+    Status s = check_pitab_alignment(d_pitab);
+    if (s.ok()) s = use_device(ctx);
     BPPlan* plan = nullptr;
     if (s.ok()) s = get_bp_plan(ctx, *g, &plan);
     if (s.ok()) s = reset_device_flag(ctx, (cudaStream_t)stream);
@@ -500,7 +501,8 @@ ctrecon_status ctrecon_bkproj_dev_f32(ctrecon_ctx* ctx, void* stream, const ctre
     if (!g || !d_fproj || !d_image)
         return finish(ctx, make_status(CTRECON_ERR_INVALID_ARGUMENT, "NULL argument"));
     cudaStream_t st = (cudaStream_t)stream;
-    Status s = use_device(ctx);
+    Status s = check_pitab_alignment(d_pitab);
+    if (s.ok()) s = use_device(ctx);
     BPPlan* plan = nullptr;
     if (s.ok()) s = get_bp_plan(ctx, *g, &plan);
     const PiRecord* pit = (const PiRecord*)d_pitab;

@@ -132,6 +132,7 @@ ctrecon_status ctrecon_tune_bkproj(ctrecon_ctx* ctx, void* stream, const ctrecon
         cudaStream_t s = (cudaStream_t)stream;
         const cudaError_t e0 = cudaSetDevice(ctx->device);
         Status st = e0 == cudaSuccess ? Status::Ok() : cuda_status(e0, "cudaSetDevice");
+        if (st.ok()) st = check_pitab_alignment(d_pitab);
         BPPlan* plan = nullptr;
         if (st.ok()) st = get_bp_plan(ctx, *g, &plan);
         if (st.ok()) st = reset_device_flag(ctx, s);

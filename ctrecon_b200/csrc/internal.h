@@ -61,10 +61,10 @@ constexpr size_t kPlanCacheSize = 32;
 
 // ---- filter tables -----------------------------------------------------------------------
 // forward rebin entry per (kappa row a, column y): X = wa*GF[r0] + wb*GF[r1]
-struct FwEntry { int r0, r1; float wa, wb; };
+struct alignas(16) FwEntry { int r0, r1; float wa, wb; };
 // backward rebin entry per (row z, column y): FProj = gb*H[b] + ge*H[e], H the unsigned
 // Hilbert sum (the sign and the post-weight 1/coef are folded into gb/ge)
-struct BkEntry { int b, e; float gb, ge; };
+struct alignas(16) BkEntry { int b, e; float gb, ge; };
 
 struct FilterTables {
     int YL = 0, ZL = 0, AL = 0, QQ = 0, P = 0;
@@ -86,7 +86,7 @@ struct FilterTables {
 Status build_filter_tables(const ctrecon_filter_params& p, FilterTables& t);
 
 // DerMode 0 resampling of one column (one side): columns, fraction, row scale
-struct DresCol { int yd, yu; float alfa, dzc; };
+struct alignas(16) DresCol { int yd, yu; float alfa, dzc; };
 
 // Device form of the tables for one parameter set.
 struct FilterPlan {
@@ -114,8 +114,14 @@ Status parse_bp_geom(const ctrecon_bp_geom& g, BPGeom& out);
 
 // Per-voxel PI-interval record (16 bytes): B = bi + bf and T = ti + tf are the fractional
 // view indices of KatsevichBkProj.cpp:177-178; bi == kPiInvalid marks an unwritten voxel.
-struct PiRecord { int bi; float bf; int ti; float tf; };
+struct alignas(16) PiRecord { int bi; float bf; int ti; float tf; };
 constexpr int kPiInvalid = 0x7fffffff;
+// A caller's PI table is read and written as 16-byte records: it must be 16-byte aligned.
+inline Status check_pitab_alignment(const void* p) {
+    return ((uintptr_t)p & 15u)
+               ? make_status(CTRECON_ERR_INVALID_ARGUMENT, "PI table must be 16-byte aligned")
+               : Status::Ok();
+}
 
 // Kernel parameter block of the PI solve and the backprojector.
 struct BPParams {

@@ -429,7 +429,8 @@ ctrecon_status ctrecon_pi_dev_stats(ctrecon_ctx* ctx, void* stream, const ctreco
     PINET_GUARD({
         cudaSetDevice(ctx->device);
         BPPlan* plan = nullptr;
-        Status s = get_bp_plan(ctx, *g, &plan);
+        Status s = check_pitab_alignment(d_pitab);
+        if (s.ok()) s = get_bp_plan(ctx, *g, &plan);
         if (s.ok()) s = reset_device_flag(ctx, (cudaStream_t)stream);
         if (s.ok())
             s = launch_pi_stats(ctx, (cudaStream_t)stream, *plan, (PiRecord*)d_pitab, d_updates,

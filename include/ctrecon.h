@@ -180,7 +180,9 @@ ctrecon_status ctrecon_filter_mode1_dev_f32(ctrecon_ctx* ctx, void* stream,
                                             const ctrecon_filter_params* p, const float* d_proj,
                                             float* d_fproj);
 
-/* Bytes of the per-voxel PI-interval table written by ctrecon_pi_dev. */
+/* Bytes of the per-voxel PI-interval table written by ctrecon_pi_dev. The table holds 16-byte
+ * records: every d_pitab argument must be 16-byte aligned (device allocations are), else the
+ * call returns CTRECON_ERR_INVALID_ARGUMENT before any work. */
 ctrecon_status ctrecon_pi_table_bytes(const ctrecon_bp_geom* g, size_t* bytes);
 
 /* PI-line solve for every voxel (PISegment, KatsevichBkProj.cpp:283-312 and the interval

@@ -181,6 +181,33 @@ def test_pi_table_matches_oracle(ctx, torch_mod, oracle_mod, case):
     assert abs(n_gpu - n_orc) <= max(2, n_orc * 1e-7)
 
 
+def test_pi_table_alignment_is_checked(ctx, torch_mod):
+    """The PI table holds 16-byte records: a caller's table that is not 16-byte aligned is
+    refused by every entry point that takes one, before any work is enqueued."""
+    import ctrecon_b200 as ct
+    torch = torch_mod
+    s = _scan("tiny")
+    g = s.geom_struct()
+    nbytes = ctx.pi_table_bytes(g)
+    d_buf = torch.zeros(nbytes + 16, dtype=torch.uint8, device="cuda")
+    bad = d_buf[4:4 + nbytes]
+    assert bad.data_ptr() % 16 == 4
+    d_f = torch.zeros(s.proj_shape, dtype=torch.float32, device="cuda")
+    img = torch.full(s.vol_shape, SENTINEL, dtype=torch.float32, device="cuda")
+    with pytest.raises(ct.CtreconError, match="16-byte aligned"):
+        ctx.pi_dev(g, bad)
+    with pytest.raises(ct.CtreconError, match="16-byte aligned"):
+        ctx.bkproj_dev(g, d_f, img, d_pitab=bad)
+    with pytest.raises(ct.CtreconError, match="16-byte aligned"):
+        ctx.tune_bkproj(g, d_f, img, d_pitab=bad)
+    torch.cuda.synchronize()
+    assert int(d_buf.sum().item()) == 0 and bool(torch.all(img == SENTINEL))
+    # an aligned table of the same buffer works
+    good = d_buf[16:16 + nbytes]
+    ctx.pi_dev(g, good)
+    torch.cuda.synchronize()
+
+
 def test_bkproj_matches_oracle_tiny(ctx, tiny_case):
     s = tiny_case["s"]
     img = np.full(s.vol_shape, SENTINEL)
