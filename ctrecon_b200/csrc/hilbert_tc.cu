@@ -12,7 +12,7 @@
 //   BF16X3: T and X split into BF16 hi + lo; D = Thi*Xhi + Thi*Xlo + Tlo*Xhi (kind::f16,
 //           FP32 accumulation) -- the dropped Tlo*Xlo term is ~2^-16 relative;
 //   TF32:   one kind::tf32 product of RN-rounded operands (about 2^-11 relative per term).
-// Epilogue (8 warps, two per TMEM lane quarter): the tile's accumulators go through a shared
+// Epilogue (kEpiGroups warps per TMEM lane quarter): the tile's accumulators go through a shared
 // transpose buffer, then FProj[v][z][i] = gb*D[i][b] + ge*D[i][e] (the backward-rebin rows b, e
 // and weights gb, ge of the host table) is gathered for all views of the tile per table entry,
 // storing coalesced rows.
@@ -35,6 +35,10 @@ namespace ctr {
 namespace {
 
 constexpr int kM = 128;
+// Epilogue warps per TMEM lane quarter: the CTA has 4 * kEpiGroups warps (warps 0 and 1 also
+// issue the TMA loads and the MMAs). A warp may only read the TMEM lanes of its quarter (warp % 4).
+constexpr int kEpiGroups = 4;
+constexpr int kThreads = 128 * kEpiGroups;
 
 struct TcParams {
     int AL, YL, ZL, nviews, vpt, ntile, nk, ALt;  // ALt: odd row stride >= vpt * AL
@@ -144,7 +148,7 @@ __host__ __device__ inline uint32_t tmem_cols_for(int ntile) {
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(256, 1)
+__global__ void __launch_bounds__(kThreads, 1)
 k_hilbert_tc(const __grid_constant__ CUtensorMap tA0, const __grid_constant__ CUtensorMap tA1,
              const __grid_constant__ CUtensorMap tB0, const __grid_constant__ CUtensorMap tB1,
              TcParams p) {
@@ -232,10 +236,10 @@ k_hilbert_tc(const __grid_constant__ CUtensorMap tA0, const __grid_constant__ CU
     }
     __syncwarp();
 
-    // epilogue: eight warps. Warp w reads TMEM lanes [32 (w & 3), +32) (= output columns) for
-    // the views vl = (w >> 2), (w >> 2) + 2, ... of the tile into the shared transpose buffer
-    // of its lane quarter; after a barrier, each warp gathers rows z = (w >> 2), +2, ... of
-    // every view of the tile, so each backward-rebin table entry is loaded once per tile.
+    // epilogue: all 4 * kEpiGroups warps. Warp w reads TMEM lanes [32 (w & 3), +32) (= output
+    // columns) of its share of the tile's accumulator columns into the shared transpose buffer
+    // of its lane quarter; after a barrier, each warp gathers rows z = (w >> 2), + kEpiGroups, ...
+    // of every view of the tile, so each backward-rebin table entry is loaded once per tile.
     const bool have = __all_sync(0xffffffffu, mbar_wait(done, 0, p.err, 3));
     tc_fence_after();
     const int q = warp & 3, h = warp >> 2;
@@ -247,18 +251,25 @@ k_hilbert_tc(const __grid_constant__ CUtensorMap tA0, const __grid_constant__ CU
         // (view, column range) pieces this warp moves: per view when the tile holds several
         // views, per TMEM half when one view spans both halves
         const int npiece = p.nh == 2 ? 2 : nv;
-        for (int pc = h; pc < npiece; pc += 2) {
+        // work units: the 16-column chunks of every piece, then its remaining single columns,
+        // dealt round-robin to the kEpiGroups warps of the lane quarter (warp-uniform test)
+        int u = 0;
+        for (int pc = 0; pc < npiece; ++pc) {
             const int c0 = p.nh == 2 ? pc * p.ntile : pc * p.AL;             // logical column
             const int c1 = p.nh == 2 ? min(p.AL, c0 + p.ntile) : c0 + p.AL;
             const int t0 = p.nh == 2 ? pc * 256 : c0;                        // TMEM column
-            int c = c0;
-            for (; c + 16 <= c1; c += 16) {
+            const int nfull = (c1 - c0) / 16;
+            for (int m = 0; m < nfull; ++m, ++u) {
+                if (u % kEpiGroups != h) continue;
+                const int c = c0 + 16 * m;
                 float r[16];
                 tmem_ld16(lane_addr + (uint32_t)(t0 + c - c0), r);
 #pragma unroll
                 for (int k = 0; k < 16; ++k) trq[lane * p.ALt + c + k] = r[k];
             }
-            for (; c < c1; ++c) trq[lane * p.ALt + c] = tmem_ld1(lane_addr + (uint32_t)(t0 + c - c0));
+            for (int c = c0 + 16 * nfull; c < c1; ++c, ++u)
+                if (u % kEpiGroups == h)
+                    trq[lane * p.ALt + c] = tmem_ld1(lane_addr + (uint32_t)(t0 + c - c0));
         }
     }
     __syncthreads();
@@ -270,16 +281,16 @@ k_hilbert_tc(const __grid_constant__ CUtensorMap tA0, const __grid_constant__ CU
         // stores, so their latencies overlap instead of queueing behind the previous row's
         constexpr int kEpiRows = 8;
         const int4* bk4 = reinterpret_cast<const int4*>(p.bk);
-        for (int k0 = h; k0 < p.ZL; k0 += 2 * kEpiRows) {
+        for (int k0 = h; k0 < p.ZL; k0 += kEpiGroups * kEpiRows) {
             int4 e[kEpiRows];
 #pragma unroll
             for (int r = 0; r < kEpiRows; ++r) {
-                const int k = k0 + 2 * r;
+                const int k = k0 + kEpiGroups * r;
                 e[r] = k < p.ZL ? __ldg(bk4 + (size_t)k * p.YL + i) : make_int4(0, 0, 0, 0);
             }
 #pragma unroll
             for (int r = 0; r < kEpiRows; ++r) {
-                const int k = k0 + 2 * r;
+                const int k = k0 + kEpiGroups * r;
                 if (k >= p.ZL) break;
                 const float gb = __int_as_float(e[r].z), ge = __int_as_float(e[r].w);
                 float* ok = o + (size_t)k * p.YL;
@@ -423,11 +434,11 @@ Status launch_hilbert_tc(ctrecon_ctx* ctx, cudaStream_t s, FilterPlan& plan, con
     if (bf) {
         CTR_CUDA(cudaFuncSetAttribute(k_hilbert_tc<CTRECON_HILBERT_BF16X3>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_hilbert_tc<CTRECON_HILBERT_BF16X3><<<grid, 256, smem, s>>>(tA0, tA1, tB0, tB1, p);
+        k_hilbert_tc<CTRECON_HILBERT_BF16X3><<<grid, kThreads, smem, s>>>(tA0, tA1, tB0, tB1, p);
     } else {
         CTR_CUDA(cudaFuncSetAttribute(k_hilbert_tc<CTRECON_HILBERT_TF32>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_hilbert_tc<CTRECON_HILBERT_TF32><<<grid, 256, smem, s>>>(tA0, tA1, tB0, tB1, p);
+        k_hilbert_tc<CTRECON_HILBERT_TF32><<<grid, kThreads, smem, s>>>(tA0, tA1, tB0, tB1, p);
     }
     CTR_CUDA(cudaGetLastError());
     return Status::Ok();
