@@ -116,9 +116,6 @@ static Status upload_scans(ctrecon_batch* b, cudaStream_t s, float* const* d_fpr
     {
         size_t held = 0;
         for (const auto& G : b->groups) held += G->rec.bytes;
-        size_t free_b = 0, total_b = 0;
-        CTR_CUDA(cudaMemGetInfo(&free_b, &total_b));
-        const size_t budget = (free_b + held) / 2;
         auto rec_of = [&](int i) {
             const BPParams& kp = b->bplans[i]->kp;
             return (size_t)kp.P * (kp.ZL - 1) * (kp.YL - 1) * 16;
@@ -127,6 +124,14 @@ static Status upload_scans(ctrecon_batch* b, cudaStream_t s, float* const* d_fpr
         size_t need = 0;
         for (int i = 0; i < b->n; ++i)
             if (b->svar[i] >= 10) { five.push_back(i); need += rec_of(i); }
+        // the driver is asked for free memory only when the batch would need more than it holds
+        // (a query per run can stall the host while other processes hold the driver)
+        size_t budget = need;
+        if (need > held) {
+            size_t free_b = 0, total_b = 0;
+            CTR_CUDA(cudaMemGetInfo(&free_b, &total_b));
+            budget = (free_b + held) / 2;
+        }
         std::sort(five.begin(), five.end(), [&](int x, int y) { return rec_of(x) > rec_of(y); });
         for (size_t k = 0; k < five.size() && need > budget; ++k) {
             need -= rec_of(five[k]);

@@ -815,9 +815,15 @@ Status launch_bkproj_v5(int variant, cudaStream_t s, BPPlan& plan, const float* 
     const int w0 = std::max(0, kp0.win0), w1 = std::min(kp0.P - 1, kp0.win1);
     if (w1 < w0) return Status::Ok();
     const int nv_all = w1 - w0 + 1;
-    size_t free_b = 0, total_b = 0;
-    CTR_CUDA(cudaMemGetInfo(&free_b, &total_b));
-    const size_t budget = std::min(kRecBudget, (free_b + recbuf.bytes) / 2);
+    // record budget: whatever the buffer already holds when all views fit in it (the steady
+    // state: no driver query per call, which can stall the host while other processes hold the
+    // driver), else at most kRecBudget and half of the free device memory
+    size_t budget = kRecBudget;
+    if ((size_t)nv_all * plane > recbuf.bytes) {
+        size_t free_b = 0, total_b = 0;
+        CTR_CUDA(cudaMemGetInfo(&free_b, &total_b));
+        budget = std::min(kRecBudget, (free_b + recbuf.bytes) / 2);
+    }
     int per = (int)std::max<size_t>(1, std::min<size_t>(nv_all, budget / plane));
     if (max_views > 0) per = std::min(per, max_views);
     const int nwin = (nv_all + per - 1) / per;
