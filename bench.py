@@ -665,7 +665,7 @@ def run_report(args):
                     "pi_solver_in_timing": "newton"})
     else:  # c5: the learned PI-line initialiser at scale
         _train_pinet(ctx, s, out, stream, torch)
-        d_tab_b = d_tab.clone()  # the bisection table (the judge)
+        d_tab_b = d_tab.clone()  # the bisection table (the arbiter)
         res = {}
         for name, solver, nmode in (("bisect", _lib.PI_BISECT, None),
                                     ("newton", _lib.PI_NEWTON, None),

@@ -8,7 +8,7 @@
 // the backprojector can rebuild the reference's endpoint weights (:182-234) exactly.
 //
 // Solvers (ctx option CTRECON_OPT_PI_SOLVER):
-//   BISECT  the reference's bisection, step for step (the judge of the others);
+//   BISECT  the reference's bisection, step for step (the arbiter of the others);
 //   NEWTON  safeguarded Newton with the closed-form derivative inside the same bracket,
 //           started at the PI line of the axis point at the same height;
 //   LEARNED the same Newton started at the trained network's prediction (pinet_infer.cu).

@@ -85,7 +85,7 @@ enum {
 
 /* PI-line solver (CTRECON_OPT_PI_SOLVER). All are FP64 and converge to the same tau. */
 enum {
-    CTRECON_PI_BISECT = 0,  /* bisection of KatsevichBkProj.cpp:283-312 (the judge) */
+    CTRECON_PI_BISECT = 0,  /* bisection of KatsevichBkProj.cpp:283-312 (the arbiter) */
     CTRECON_PI_NEWTON = 1,  /* safeguarded Newton from the bracket midpoint */
     CTRECON_PI_LEARNED = 2  /* Newton seeded by the trained PI-line network */
 };

@@ -1,6 +1,6 @@
 """PI-line solvers and the learned initialiser on the GPU.
 
-* Newton (closed-form derivative) converges to the bisection judge's endpoints within the
+* Newton (closed-form derivative) converges to the bisection arbiter's endpoints within the
   bisection's own tolerance, on every voxel, with the same written-voxel set;
 * the network's loss gradient from the CUDA training kernel equals the FP64 CPU reference
   (oracle/pinet_oracle.py) at the same parameters;
@@ -149,7 +149,7 @@ def test_pinet_training_inference_and_gain(torch_mod):
         print(f"inference max |BF16 kernel - FP64 forward| = {err:.3e}")
         assert err < 0.05
         # the learned start in each network mode (per voxel FP32 / packed BF16, and the
-        # screw-symmetry grid): same records as the judge, fewer Newton steps than the plain start
+        # screw-symmetry grid): same records as the arbiter, fewer Newton steps than the plain start
         bis = _pi(cx, torch, s, _lib.PI_BISECT)
         newt = _pi(cx, torch, s, _lib.PI_NEWTON)
         lrn = {}
