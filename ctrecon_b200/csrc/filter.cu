@@ -277,8 +277,10 @@ Status launch_filter(ctrecon_ctx* ctx, cudaStream_t s, FilterPlan& plan, const f
     (void)proj_nviews;
     const int mode = ctx->opt_hilbert;
     const int chunk = std::max(1, ctx->opt_filter_chunk);
-    // 4 bytes per kappa sample in every format (FP32, TF32, or BF16 hi + lo planes)
-    CTR_TRY(ctx->ws_kappa.ensure((size_t)chunk * AL * YLp * sizeof(float), "filter kappa rows"));
+    // 4 bytes per kappa sample in every format (FP32, TF32, or BF16 hi + lo planes), for the
+    // views of one chunk or of the whole call when it has fewer
+    const int nbuf = std::max(1, std::min(chunk, view_end - view_begin));
+    CTR_TRY(ctx->ws_kappa.ensure((size_t)nbuf * AL * YLp * sizeof(float), "filter kappa rows"));
     void* X = ctx->ws_kappa.ptr;
     const DresCol* dres = nullptr;  // DerMode 0 resampling columns
     if (ctx->opt_deriv == CTRECON_DERIV_DIRECT) {

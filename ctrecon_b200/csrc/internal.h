@@ -201,7 +201,7 @@ struct ctrecon_ctx {
     std::string last_error;
     int opt_hilbert = CTRECON_HILBERT_FP32;
     int opt_pi = CTRECON_PI_BISECT;
-    int opt_filter_chunk = 512;
+    int opt_filter_chunk = 2048;  // larger chunks fill the GPU better (c2: 512 -> 2048, -4 %)
     int opt_bp_variant = 2;  // second form, 8 slices x 8 views
     int opt_verbose = 0;
     int opt_deriv = CTRECON_DERIV_CHAIN;

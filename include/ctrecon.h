@@ -112,7 +112,7 @@ enum {
 typedef enum ctrecon_option {
     CTRECON_OPT_HILBERT = 1,          /* CTRECON_HILBERT_*; default FP32 */
     CTRECON_OPT_PI_SOLVER = 2,        /* CTRECON_PI_*; default BISECT */
-    CTRECON_OPT_FILTER_CHUNK = 3,     /* views per filter work chunk; default 512 */
+    CTRECON_OPT_FILTER_CHUNK = 3,     /* views per filter work chunk; default 2048 */
     CTRECON_OPT_BP_VARIANT = 4,       /* backprojector variant, default 2: 0, 1 = per-cell
                                          records, blocks of 4 / 8 views; 2, 3, 4 = second
                                          form (slices x views) 8x8, 4x8, 8x4; 5, 6, 7 = per-cell
