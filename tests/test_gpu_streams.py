@@ -134,3 +134,31 @@ def test_host_bkproj_fifth_form(torch_mod):
     rel = np.linalg.norm(imgs[10][written] - imgs[100][written]) / np.linalg.norm(imgs[100][written])
     print(f"host backprojection, fifth form vs first form: rel diff {rel:.2e}")
     assert rel < 1e-6
+
+
+@pytest.mark.parametrize("hilbert", ["fp32", "bf16x3", "tf32"])
+def test_filter_chunk_size_does_not_change_the_result(torch_mod, hilbert):
+    """The filter works through the views in chunks (CTRECON_OPT_FILTER_CHUNK, default 2048) with
+    a kappa-row buffer sized to the call; every view is filtered independently, so any chunk
+    size -- one that does not divide the view count, one larger than it -- gives the same bits."""
+    torch = torch_mod
+    import ctrecon_b200 as ct
+    from ctrecon_b200 import _lib
+    from ctrecon_b200.geometry import config
+    mode = {"fp32": _lib.HILBERT_FP32, "bf16x3": _lib.HILBERT_BF16X3,
+            "tf32": _lib.HILBERT_TF32}[hilbert]
+    s = config("c1")  # 2160 views
+    with ct.Context(0, hilbert=mode) as cx:
+        assert cx.get_option(_lib.OPT_FILTER_CHUNK) == 2048
+        d = torch.empty(s.proj_shape, dtype=torch.float32, device="cuda")
+        cx.phantom_dev(s.geom_struct(), s.ellipsoids(), d)
+        p = ct.scan_filter_params(s)
+        outs = []
+        for chunk in (2048, 97, 5000):
+            cx.set_option(_lib.OPT_FILTER_CHUNK, chunk)
+            f = torch.full_like(d, 7.25)
+            cx.filter_dev(p, d, f)
+            outs.append(f)
+        torch.cuda.synchronize()
+    assert torch.equal(outs[0], outs[1]) and torch.equal(outs[0], outs[2])
+    assert not bool(torch.any(outs[0] == 7.25))
