@@ -91,7 +91,7 @@ def _check(s, n_tiles, view_stride, seed=0):
     return slack, n_cell
 
 
-@pytest.mark.parametrize("name", ["c1", "c2s", "fine", "thin"])
+@pytest.mark.parametrize("name", ["c1", "c2s", "c3", "c5", "fine", "thin"])
 def test_footprint_covers_every_cell_read(name):
     if name == "fine":  # 0.5 mm voxels, few views per turn
         s = small_config(name="fine", YL=200, ZL=48, views_per_turn=120, turns=2.5, NX=64,
