@@ -29,7 +29,9 @@ constexpr size_t kNoAllocBytes = (size_t)16 << 20;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
 // In host code g_noalloc_scratch names a host-side stand-in, not device memory; the device
-// address is looked up once per device (with that device current) and cached here.
+// address is looked up once per device (with that device current) and cached here for the life
+// of the process. The cache assumes that the device's primary context (the one the CUDA runtime
+// uses) stays alive: after cudaDeviceReset the cached address is stale.
 static std::mutex g_addr_mu;
 static void* g_addr[128];
 
@@ -110,15 +112,25 @@ extern "C" ctrecon_status ctrecon_filter_noalloc_dev_f32(void* stream,
     using namespace ctr;
     Status s;
     try {
+        cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+        const cudaError_t ce = cudaStreamIsCapturing((cudaStream_t)stream, &cap);
         if (!p || !d_proj || !d_fproj)
             s = make_status(CTRECON_ERR_INVALID_ARGUMENT, "NULL argument");
         else if ((const void*)d_proj == (const void*)d_fproj)
             s = make_status(CTRECON_ERR_INVALID_ARGUMENT, "input and output must differ");
+        else if (ce != cudaSuccess)
+            s = cuda_status(ce, "cudaStreamIsCapturing");
+        else if (cap != cudaStreamCaptureStatusNone)
+            // every call copies its tables from a temporary host buffer; a captured copy would
+            // keep reading that buffer after it is gone, so nothing is enqueued
+            s = make_status(CTRECON_ERR_UNSUPPORTED,
+                            "the no-allocation filter cannot be called on a stream that is "
+                            "being captured");
         else
             s = filter_noalloc((cudaStream_t)stream, *p, d_proj, d_fproj);
     } catch (const std::exception& e) {
         s = make_status(CTRECON_ERR_INTERNAL, e.what());
     }
-    if (!s.ok()) set_noctx_error(s.msg);
+    set_noctx_error(s.ok() ? std::string() : s.msg);
     return s.code;
 }

@@ -207,9 +207,13 @@ ctrecon_status ctrecon_bkproj_dev_f32(ctrecon_ctx* ctx, void* stream,
  * (tables + one view of kappa rows > 16 MiB) return CTRECON_ERR_UNSUPPORTED with the sizes
  * in ctrecon_last_error(NULL). The caller passes the input and output buffers (distinct) and
  * a stream; the call is stream-ordered. The first call on a device looks up the array's
- * device address (cudaGetSymbolAddress) with that device current; make that first call
- * before any stream capture. Every call shares the array, so calls that overlap on the GPU
- * (concurrent streams, or several host threads) race; serialise them. */
+ * device address (cudaGetSymbolAddress) with that device current and keeps it for the life of
+ * the process (it assumes the device's primary context is not reset); make that first call
+ * before any stream capture. Every call copies its tables into the array from a temporary host
+ * buffer, so it must not be called while its stream is being captured: it then returns
+ * CTRECON_ERR_UNSUPPORTED and enqueues nothing. Every call shares the array and leaves its
+ * contents behind, so calls that overlap on the GPU (concurrent streams, or several host
+ * threads) race; serialise them. A successful call clears ctrecon_last_error(NULL). */
 ctrecon_status ctrecon_filter_noalloc_dev_f32(void* stream, const ctrecon_filter_params* p,
                                               const float* d_proj, float* d_fproj);
 
