@@ -47,6 +47,14 @@ class MexModule:
                                    ctypes.POINTER(vp), ctypes.c_char_p, sz]
         L.mexshim_set_print.restype = None
         L.mexshim_set_print.argtypes = [ctypes.c_int]
+        L.mxGetPr.restype = vp
+        L.mxGetPr.argtypes = [vp]
+        L.mxGetClassID.restype = ctypes.c_int
+        L.mxGetClassID.argtypes = [vp]
+        L.mxGetNumberOfDimensions.restype = sz
+        L.mxGetNumberOfDimensions.argtypes = [vp]
+        L.mxGetDimensions.restype = ctypes.POINTER(sz)
+        L.mxGetDimensions.argtypes = [vp]
         self._entry = ctypes.cast(L.mexFunction, vp)
 
     def set_print(self, enabled: bool) -> None:
@@ -88,8 +96,27 @@ class MexModule:
             return self._wrap(v, keep, dims=(1, 1)), False
         raise TypeError(f"unsupported MEX argument type {type(value)}")
 
-    def call(self, args: Iterable, nlhs: int = 0) -> None:
-        """Invoke mexFunction(nlhs, plhs, nrhs, prhs) with the given right-hand sides."""
+    def _take(self, h) -> np.ndarray:
+        """Copy a left-hand side the MEX function created into numpy (C order, the MATLAB
+        dimensions reversed) and free it."""
+        try:
+            nd = int(self.lib.mxGetNumberOfDimensions(h))
+            dims = self.lib.mxGetDimensions(h)
+            shape = tuple(int(dims[i]) for i in range(nd))[::-1]
+            cls = int(self.lib.mxGetClassID(h))
+            if cls not in (MX_DOUBLE_CLASS, MX_SINGLE_CLASS):
+                raise MexError(f"unsupported output class {cls}")
+            ct = ctypes.c_double if cls == MX_DOUBLE_CLASS else ctypes.c_float
+            n = int(np.prod(shape)) if shape else 1
+            ptr = self.lib.mxGetPr(h)
+            buf = (ct * n).from_address(ptr) if n else (ct * 0)()
+            return np.ctypeslib.as_array(buf).reshape(shape).copy()
+        finally:
+            self.lib.mxDestroyArray(h)
+
+    def call(self, args: Iterable, nlhs: int = 0) -> list:
+        """Invoke mexFunction(nlhs, plhs, nrhs, prhs) with the given right-hand sides; returns
+        the nlhs outputs it created, as numpy arrays."""
         keep: list = []
         handles, owned = [], []
         try:
@@ -104,6 +131,7 @@ class MexModule:
             rc = self.lib.mexshim_call(self._entry, nlhs, plhs, n, prhs, err, len(err))
             if rc != 0:
                 raise MexError(err.value.decode(errors="replace"))
+            return [self._take(plhs[i]) for i in range(nlhs) if plhs[i]]
         finally:
             for h in owned:
                 self.lib.mxDestroyArray(h)

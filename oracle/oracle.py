@@ -20,6 +20,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liborc.so")
 REF_BKPROJ_PATH = os.path.join(HERE, "_ref", "libkatsevich_bkproj_ref.so")
+REF_PROJSLICE_PATH = os.path.join(HERE, "_ref", "libcreateprojslice_ref.so")
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int)
@@ -255,6 +256,50 @@ def ref_bkproj(geom: dict, fproj: np.ndarray, image: np.ndarray):
     m.set_print(False)
     m.call([geom, fproj, image], nlhs=0)
     return image
+
+
+# The head phantom of CreateProjSlice.cpp:13-24, rows (a, b, c, x0, y0, z0, phi in degrees,
+# density) in units of the object radius: the reference's own projector, kept here as the test
+# input that pins the analytic projectors against it.
+HEAD_PHANTOM = np.array([
+    [0.6900, 0.920, 0.900, 0, 0, 0, 0, 2.0],
+    [0.6624, 0.874, 0.880, 0, 0, 0, 0, -0.98],
+    [0.4100, 0.160, 0.210, -0.22, 0, -0.25, 108, -0.02],
+    [0.3100, 0.110, 0.220, 0.22, 0, -0.25, 72, -0.02],
+    [0.2100, 0.250, 0.500, 0, 0.35, -0.25, 0, 0.02],
+    [0.0460, 0.046, 0.046, 0, 0.1, -0.25, 0, 0.02],
+    [0.0460, 0.023, 0.020, -0.08, -0.65, -0.25, 0, 0.01],
+    [0.0460, 0.023, 0.020, 0.06, -0.65, -0.25, 90, 0.01],
+    [0.0560, 0.040, 0.100, 0.06, -0.105, 0.625, 90, 0.02],
+    [0.0560, 0.056, 0.100, 0, 0.100, 0.625, 0, -0.02]])
+
+
+def head_phantom_ellipsoids(pi=3.14159265358979):
+    """HEAD_PHANTOM as rows (cx cy cz a b c phi theta psi rho) of the analytic projectors: a
+    rotation about z by phi (CreateProjSlice.cpp:79-81,106-111), no tilt."""
+    H = HEAD_PHANTOM
+    z = np.zeros(len(H))
+    return np.column_stack([H[:, 3], H[:, 4], H[:, 5], H[:, 0], H[:, 1], H[:, 2],
+                            H[:, 6] * pi / 180, z, z, H[:, 7]])
+
+
+def ref_projslice_available() -> bool:
+    return os.path.exists(REF_PROJSLICE_PATH)
+
+
+def ref_create_proj_slice(theta, pou, heli, YL, ZL, DW, DH):
+    """Run the reference's own CreateProjSlice.cpp mexFunction (FunctionKat_v6.m:73): one view
+    of the head phantom at source angle theta, source radius pou, pitch heli, a YL x ZL flat
+    detector through the axis of width DW and height DH. Returns numpy (ZL, YL)."""
+    import sys
+    root = os.path.dirname(HERE)
+    if root not in sys.path:
+        sys.path.insert(0, root)
+    from ctrecon_b200.mexharness import MexModule
+    m = MexModule(REF_PROJSLICE_PATH)
+    m.set_print(False)
+    return m.call([float(theta), float(pou), float(heli), float(YL), float(ZL), float(DW),
+                   float(DH)], nlhs=1)[0]
 
 
 def rebin_to_panel(proj, c, w, D):
