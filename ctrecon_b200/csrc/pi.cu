@@ -10,7 +10,9 @@
 // Solvers (ctx option CTRECON_OPT_PI_SOLVER):
 //   BISECT  the reference's bisection, step for step (the arbiter of the others);
 //   NEWTON  safeguarded Newton with the closed-form derivative inside the same bracket,
-//           started at the PI line of the axis point at the same height;
+//           started at the PI line of the axis point at the same height, then the bisection
+//           replayed from Newton's root (pi_bisect_replay): the endpoints are BISECT's bit for
+//           bit, for about one chord evaluation more;
 //   LEARNED the same Newton started at the trained network's prediction (pinet_infer.cu).
 #include "internal.h"
 #include "pi_device.cuh"
@@ -67,8 +69,20 @@ __global__ void k_pi_solve(BPParams kp, double Ctr, double Beg, int solver,
                                     a * ((1.f - b) * __ldg(&r1[j0].x) + b * __ldg(&r1[j1].x));
                     s0 += (double)(o / (float)kPinetOutScale);
                 }
+                // Newton finds the root; the bisection, replayed from it, decides the endpoints
+                // (bit for bit those of CTRECON_PI_BISECT). Should Newton not converge, the plain
+                // bisection runs instead.
                 int it = 0;
-                pi_newton(x, y, z, s0, &sb, &st, &it);
+                double dz = 0;
+                bool conv = false;
+                pi_newton(x, y, z, s0, &sb, &st, &it, &dz, &conv);
+                if (conv && dz > 0) {
+                    it += pi_bisect_replay(x, y, z, sb, dz, &sb, &st);
+                } else {
+                    int ib = 0;
+                    pi_bisect(x, y, z, &sb, &st, &ib);
+                    it += ib;
+                }
                 its = (unsigned long long)it;
             }
             cnt = make_record(kp, Ctr, Beg, sb, st, &rec);

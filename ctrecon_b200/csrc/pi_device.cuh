@@ -80,7 +80,8 @@ __device__ __forceinline__ double pi_chord_d(double x, double y, double r2, doub
 // stepped point is accepted without another evaluation (its error is ~step^2 < 1e-12 rad) and
 // st follows it along dst; both are then well inside the reference's 1e-7 bisection tolerance.
 __device__ __forceinline__ void pi_newton(double x, double y, double z, double s0, double* B,
-                                          double* T, int* iters) {
+                                          double* T, int* iters, double* dz_out = nullptr,
+                                          bool* converged = nullptr) {
     const double PI = kRefPi;
     double bmax = z * 2 * PI, bmin = bmax - 2 * PI;
     const double r2 = x * x + y * y;
@@ -98,13 +99,56 @@ __device__ __forceinline__ void pi_newton(double x, double y, double z, double s
         if (newton && fabs(step) < 1e-6) {
             st += dst * step;
             sb = nx;
+            if (converged) *converged = true;
             break;
         }
         sb = nx;
     }
     *B = sb;
     *T = st;
+    if (dz_out) *dz_out = d;
     if (iters) *iters = it + 1;
+}
+
+// The reference's bisection (pi_bisect, KatsevichBkProj.cpp:291-309) replayed from a root.
+// Given tau, a root of zz(sb) = z accurate to ~1e-12 rad (Newton's), and dz = dzz/dsb near it,
+// every midpoint's decisions follow from sb - tau: zz(sb) < z iff sb < tau (zz increases with
+// sb), and the stop test |zz(sb) - z| <= 1e-7 is that of |dz (sb - tau)| (the linear model's
+// error there is ~1e-12, far below the bisection's 1e-7). The chord is evaluated exactly -- the
+// same pi_chord call as the bisection's -- only where either decision lies within 1e-10 of its
+// threshold, and once at the final midpoint for st. The midpoints are the bisection's own
+// arithmetic, so (sb, st) equal pi_bisect's bit for bit: the bisection remains the judge of the
+// endpoints, Newton only finds where it will end. Returns the chord evaluations made (~1).
+__device__ __forceinline__ int pi_bisect_replay(double x, double y, double z, double tau,
+                                                double dz, double* B, double* T) {
+    const double PI = kRefPi;
+    constexpr double kMargin = 1e-10;
+    double delta = 1, bmax = z * 2 * PI, bmin, r2 = x * x + y * y;
+    bmin = bmax - 2 * PI;
+    double sb = 0, st = 0;
+    bool have_st = false;
+    int ev = 0;
+    while (((bmax - bmin) > kPiTol) && (delta > kPiTol)) {
+        sb = (bmax + bmin) * 0.5;
+        const double dl = sb - tau;
+        double g = dz * dl;  // ~ zz(sb) - z
+        have_st = false;
+        if (fabs(dl) < kMargin || fabs(fabs(g) - kPiTol) < kMargin) {
+            g = pi_chord(x, y, r2, sb, &st) - z;
+            have_st = true;
+            ++ev;
+        }
+        if (g < 0) bmin = sb;
+        else bmax = sb;
+        delta = fabs(g);
+    }
+    if (!have_st) {
+        pi_chord(x, y, r2, sb, &st);
+        ++ev;
+    }
+    *B = sb;
+    *T = st;
+    return ev;
 }
 
 __device__ __forceinline__ void voxel_xyz(const BPParams& kp, long long idx, int* xi, int* yi,

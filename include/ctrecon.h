@@ -83,11 +83,15 @@ enum {
     CTRECON_HILBERT_TF32 = 2    /* tcgen05 Toeplitz GEMM in TF32 */
 };
 
-/* PI-line solver (CTRECON_OPT_PI_SOLVER). All are FP64 and converge to the same tau. */
+/* PI-line solver (CTRECON_OPT_PI_SOLVER). All are FP64 and give the same endpoints bit for bit:
+ * Newton finds the root, then the bisection is replayed from it (its midpoint decisions follow
+ * from the root; the chord is evaluated where a decision is close to its threshold and at the
+ * final midpoint), so the bisection decides every endpoint. */
 enum {
     CTRECON_PI_BISECT = 0,  /* bisection of KatsevichBkProj.cpp:283-312 (the arbiter) */
-    CTRECON_PI_NEWTON = 1,  /* safeguarded Newton from the bracket midpoint */
-    CTRECON_PI_LEARNED = 2  /* Newton seeded by the trained PI-line network */
+    CTRECON_PI_NEWTON = 1,  /* safeguarded Newton from the axis point's PI line, then the
+                               bisection replayed from its root */
+    CTRECON_PI_LEARNED = 2  /* the same, Newton seeded by the trained PI-line network */
 };
 
 /* Derivative of the filter (CTRECON_OPT_DERIVATIVE). */
@@ -101,7 +105,7 @@ enum {
 
 /* CTRECON_OPT_PINET_MODE. The network's inputs are (r, cos psi, sin psi) with
  * psi = phi - 2 pi z / pitch (the helix's screw symmetry), so its prediction is a function of
- * (r, psi) alone. Whatever the mode, the FP64 Newton solve decides every endpoint. */
+ * (r, psi) alone. Whatever the mode, the FP64 solve decides every endpoint. */
 enum {
     CTRECON_PINET_VOXEL_FP32 = 0, /* per voxel, FP32 SiLU (as ctrecon_pinet_predict) */
     CTRECON_PINET_VOXEL_BF16 = 1, /* per voxel, packed BF16 SiLU */
@@ -221,9 +225,9 @@ ctrecon_status ctrecon_filter_noalloc_dev_f32(void* stream, const ctrecon_filter
  * or CTRECON_ERR_TIMEOUT when a bounded wait inside a kernel gave up. */
 ctrecon_status ctrecon_sync(ctrecon_ctx* ctx, void* stream);
 
-/* PI-line solve as ctrecon_pi_dev, also counting the solver's iterations (device unsigned long
- * long, summed over solved voxels): bisection steps for CTRECON_PI_BISECT, Newton steps for
- * CTRECON_PI_NEWTON / CTRECON_PI_LEARNED. */
+/* PI-line solve as ctrecon_pi_dev, also counting the solver's chord evaluations (device
+ * unsigned long long, summed over solved voxels): bisection steps for CTRECON_PI_BISECT, Newton
+ * steps plus the replay's evaluations for CTRECON_PI_NEWTON / CTRECON_PI_LEARNED. */
 ctrecon_status ctrecon_pi_dev_stats(ctrecon_ctx* ctx, void* stream, const ctrecon_bp_geom* g,
                                     void* d_pitab, unsigned long long* d_updates,
                                     unsigned long long* d_iters);

@@ -57,3 +57,22 @@ def oracle_filter_params(O, s):
 
 def oracle_geom(O, s, honour_extras=True):
     return O.bp_geom(s.locus(), s.detector(), s.object(), honour_extras=honour_extras)
+
+
+def central_block(O, s, n=48):
+    """A central n^3 block of scan s at the scan's voxel pitch, posed the way the reference's
+    KatsevichBkProj accepts it (ObjR = n/2 voxels, so that its default pitch 2*ObjR/N is the
+    scan's), and restricted to the views [lo, hi) that the block's PI intervals need, with a
+    3-view margin so that loop bounds and endpoint weights are those of the full scan
+    (KatsevichBkProj.cpp:177-234). Returns (locus, detector, object, lo, hi)."""
+    dx = s.voxel_size[0]
+    obj = [dx * n / 2.0, float(n), float(n), float(n), dx, dx, dx]
+    g = O.bp_geom(s.locus(), s.detector(), obj, honour_extras=True)
+    pit = O.pi_table(g)
+    v = pit["valid"]
+    lo = max(0, int(np.floor(pit["B"][v].min())) - 3)
+    hi = min(s.P, int(np.ceil(pit["T"][v].max())) + 4)
+    locus = s.locus()
+    locus[4] = float(lo + 1)          # ProjBeginIndex (one-based)
+    locus[5] = float(hi)              # ProjEndIndex
+    return locus, s.detector(), obj, lo, hi
