@@ -1,23 +1,29 @@
-"""Benchmark: Katsevich helical cone-beam reconstruction of a 512x512x256 volume on B200.
+"""Benchmark: Katsevich helical cone-beam reconstruction of a 512^3 volume on B200.
 
-Workload (default, the plain FP32 B200 configuration): flat detector 64 rows x 736 columns
-at 0.8 mm, source radius 600 mm, source-detector 1200 mm, 1160 views/turn over 8 turns
-(9280 views), pitch 0.9x the Tam-Danielson window, 40 seeded random ellipsoids with Poisson
-noise at 1e5 photons/ray, 512x512x256 FP32 volume at 0.4 mm voxels. Synthetic data made on
-the device by the analytic FP64 projector (not timed).
+Workload (default, c3): flat detector 128 rows x 1024 columns at 0.8 mm, source radius 600 mm,
+source-detector 1200 mm, 2304 views/turn over 6 turns (13824 views), pitch 0.9x the
+Tam-Danielson window, 40 seeded random ellipsoids, 512^3 FP32 volume at 2*ObjR/512 = 0.469 mm.
+Synthetic data made on the device by the analytic FP64 projector (not timed). `--config c2`
+runs the 512x512x256 plain-FP32 scan (64 x 736 detector, 9280 views, Poisson noise) instead.
 
 One step = the whole hot path over one scan: filter (derivative, forward height rebin,
 Hilbert, backward rebin) -> PI-line solve -> voxel-driven backprojection.
 
 Metric: GUPS = voxel-view updates per second, the update count being the reference's own
-loop count sum(LoopEnd - LoopBegin + 1) over written voxels (KatsevichBkProj.cpp:237),
-taken from the bisection PI solve and used for every variant. `value` is updates / step
-time of the device-resident chain (all ranks' updates / max-over-ranks time); `e2e` is the
-same through the MEX-equivalent host calls (FP64 host buffers, copies in the timed region).
-With the plain options (the default), `mixed_learned` times the other side of the metric on
-the same resident inputs: BF16x3 Hilbert and the learned PI start (`vs_plain` = its speed-up).
+loop count sum(LoopEnd - LoopBegin + 1) over written voxels (KatsevichBkProj.cpp:237), taken
+from the bisection PI solve and used for every form. `value` is the plain FP32 form (FP32
+Hilbert, bisection PI solve) with inputs resident in HBM (all ranks' updates / max-over-ranks
+time). Beside it, on the same resident inputs: `forms.mixed_learned` (BF16x3 tensor-core
+Hilbert, the learned PI start) and `forms.mixed_learned_batched` (the same for two copies of the
+scan in one batch: one persistent backprojection launch over both, replayed as a CUDA graph),
+each with `vs_plain`; `accuracy` gives every form's relative RMSE and max-abs against the FP64
+oracle of the whole chain on a central 48^3 block. `e2e` is the plain form through the
+MEX-equivalent host calls (FP64 pinned host buffers, copies in the timed region) and
+`e2e_pageable` through the MEX modules themselves with pageable FP64 arrays, as MATLAB calls them.
+`roofline` is the backprojection kernel's (the dominant one) against its issue limit;
+`kernels` gives every kernel's time and roofline fraction, from CUDA events around each launch.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config c3|c2]
                     [--hilbert fp32|bf16x3|tf32] [--pi bisect|newton|learned]
 """
 from __future__ import annotations
@@ -53,7 +59,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c2")
+    ap.add_argument("--config", default="c3")
     ap.add_argument("--hilbert", default="fp32", choices=["fp32", "bf16x3", "tf32"])
     ap.add_argument("--pi", default="bisect", choices=["bisect", "newton", "learned"])
     ap.add_argument("--no-mixed", action="store_true",
@@ -69,37 +75,52 @@ def parse():
                          "copies, 100 first form")
     ap.add_argument("--batched", action="store_true",
                     help="16 uneven scans (c4): one-at-a-time vs one batched graph replay")
-    ap.add_argument("--report", choices=["c3", "c5", "extras"],
+    ap.add_argument("--report", choices=["c3", "c5", "extras", "refgpu"],
                     help="c3: error of each Hilbert variant vs the FP64 oracle and their times; "
                          "c5: the learned PI initialiser at 1024^3 (iterations saved, endpoint "
                          "agreement, time vs the plain form); extras: the panel rebin, "
-                         "DerMode 0, FilteringMode 1 and the file formats on the c2 scan")
+                         "DerMode 0, FilteringMode 1 and the file formats on the c2 scan; "
+                         "refgpu: the reference's own GPU MEX files recompiled for sm_100a "
+                         "(baseline/_ref) timed and checked beside this library on the c2 scan")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true",
+                    help="skip the FP64 oracle check of each form on the central block")
+    ap.add_argument("--no-batched", action="store_true",
+                    help="skip the mixed + learned + batched form (two scans, one graph)")
     return ap.parse_args()
 
 
 def load_peaks():
+    """Roofline denominators: MEASURED_PEAKS.json (copy bandwidth, cuBLAS BF16 burst and
+    sustained), else the pool's earlier measurement ("fallback")."""
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
             d = json.load(f)
-        return float(d["hbm_gbs"]), "measured"
+        return {"hbm_gbs": float(d["hbm_gbs"]), "bf16_tflops": float(d["bf16_tflops"]),
+                "bf16_tflops_sustained": float(d.get("bf16_tflops_sustained", d["bf16_tflops"])),
+                "source": "measured"}
     except Exception:
-        return 6650.0, "fallback"
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0,
+                "source": "fallback"}
+
+
+def load_profile_table(name):
+    """Rows `kernel workload value` of a committed ncu summary table under profiles/."""
+    out = {}
+    try:
+        for line in open(os.path.join(ROOT, "profiles", name)):
+            parts = line.split()
+            if len(parts) >= 3 and not line.startswith("#"):
+                out[(parts[0], parts[1])] = float(parts[2])
+    except OSError:
+        pass
+    return out
 
 
 def load_traffic(kernel, workload):
     """Per-launch DRAM bytes of `kernel` from the committed ncu summary, if any."""
-    path = os.path.join(ROOT, "profiles", "traffic.txt")
-    try:
-        for line in open(path):
-            parts = line.split()
-            if len(parts) >= 3 and not line.startswith("#") and parts[0] == kernel and \
-                    parts[1] == workload:
-                return float(parts[2])
-    except OSError:
-        pass
-    return None
+    return load_profile_table("traffic.txt").get((kernel, workload))
 
 
 class ClockSampler:
@@ -236,14 +257,14 @@ def cpu_filter_views(O, s, proj_sub):
     return O.katsevich_filter(fp, proj_sub)
 
 
-def cpu_bp_sample_port(O, s, fproj_views, lo, hi, nthreads, n=48):
-    locus, det, obj, lo2, hi2 = block_problem(O, s, n)
-    assert (lo2, hi2) == (lo, hi)
-    g = O.bp_geom(locus, det, obj, honour_extras=True)
-    img = np.zeros((n, n, n))
-    t = time.perf_counter()
-    _, nupd = O.bkproj(g, np.ascontiguousarray(fproj_views), img, nthreads=nthreads)
-    return time.perf_counter() - t, nupd
+def workload_config(s, ws):
+    """The `config` of both arms' lines: the workload, nothing of the implementation."""
+    gb = 4 * s.P * s.ZL * s.YL / 1e9
+    return {"workload": workload_name(s), "volume": list(s.vol_shape),
+            "voxel_mm": [round(v, 6) for v in s.voxel_size], "detector": [s.ZL, s.YL],
+            "views": s.P, "views_per_turn": s.views_per_turn, "parallelism": f"replicas{ws}",
+            "l2": (f"inputs larger than L2 (FP32 projections {gb:.2f} GB)" if gb > 0.126 else
+                   f"inputs smaller than L2 (FP32 projections {gb:.3f} GB): a test size")}
 
 
 def _ref_worker(args):
@@ -258,13 +279,51 @@ def _ref_worker(args):
     return time.perf_counter() - t
 
 
+class CpuChainSample:
+    """A bounded sample of the whole chain on the host cores, sized so that its own throughput
+    is the full scan's: the backprojection of a central n^3 block (one copy per process, or
+    OpenMP threads) and the filter of the same fraction of the scan's views as the block's
+    updates are of the scan's updates. Then GUPS = sample updates / sample time, with
+    full-scan time = full updates / GUPS."""
+
+    def __init__(self, O, s, d_proj_views, full_updates, n=32, copies=1):
+        self.O, self.s, self.n, self.copies = O, s, n, copies
+        self.locus, self.det, self.obj, lo, hi = block_problem(O, s, n)
+        self.gb = O.bp_geom(self.locus, self.det, self.obj, honour_extras=True)
+        proj_b = d_proj_views(max(0, lo - 1), min(s.P, hi + 1))
+        a = max(0, lo - 1)
+        self.fproj = np.ascontiguousarray(cpu_filter_views(O, s, proj_b)[lo - a:hi - a])
+        _, self.block_updates = O.bkproj(self.gb, self.fproj, np.zeros((n, n, n)))
+        self.updates = copies * self.block_updates
+        # filtered views in the same proportion to the scan's views as the updates
+        self.nview = max(1, int(round(s.P * self.updates / full_updates)))
+        self.filter_in = proj_b[:min(len(proj_b), self.nview + 2)]
+        while len(self.filter_in) < self.nview + 2:
+            self.filter_in = np.concatenate([self.filter_in, proj_b[:self.nview + 2 -
+                                                                     len(self.filter_in)]])
+        self.full_updates = full_updates
+
+    def filter_once(self):
+        t = time.perf_counter()
+        cpu_filter_views(self.O, self.s, self.filter_in)
+        return time.perf_counter() - t
+
+    def describe(self, who, workers):
+        return (f"per step: the filter of {self.nview} views ({who} filter restatement, "
+                f"OpenMP) and the backprojection of {self.copies} x a central {self.n}^3 block "
+                f"at the workload's voxel pitch ({self.updates} updates) by {workers}; "
+                f"views / {self.s.P} = updates / {self.full_updates}, so the sample's rate is "
+                f"the full chain's")
+
+
 # ---------------------------------------------------------------------------------------------
 def run_reference(args):
     """The reference's CPU path, timed on the host cores: KatsevichBkProj.cpp compiled
-    unchanged (oracle/_ref; single-threaded code, run as one process per core on the same
+    unchanged (oracle/_ref; single-threaded code, one process per core, each on the same
     central block) for the backprojection, and the FP64 restatement of KatsevichFiltering.m
     (MATLAB is unavailable; OpenMP over views) for the filter. Each step is a bounded sample
-    scaled to one full scan by the exact update count and the view count."""
+    whose views and updates are the same fraction of the scan's (CpuChainSample), so the
+    step's own rate is the chain's GUPS."""
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -277,53 +336,45 @@ def run_reference(args):
                           "oracle/_ref (KatsevichBkProj.cpp built from the CTRecon sources) "
                           "is missing"}))
         return
-    n = 48
-    locus, det, obj, lo, hi = block_problem(O, s, n)
-    # inputs: the same analytic phantom (FP64 oracle projector) on the views the block needs
-    gsub = O.bp_geom(locus, s.detector(), s.object())
-    proj = O.project_ellipsoids(gsub, s.ellipsoids())
-    fproj = cpu_filter_views(O, s, proj)
-    g = O.bp_geom(locus, det, obj, honour_extras=True)
-    _, block_updates = O.bkproj(g, fproj, np.zeros((n, n, n)))
     full_updates = _full_update_count(s)
+    gsub_cache = {}
+
+    def proj_views(a, b):
+        locus = s.locus()
+        locus[4], locus[5] = float(a + 1), float(b)
+        g = O.bp_geom(locus, s.detector(), s.object())
+        gsub_cache["g"] = g
+        return O.project_ellipsoids(g, s.ellipsoids())
+
+    smp = CpuChainSample(O, s, proj_views, full_updates, n=32, copies=cores)
     tmpdir = tempfile.mkdtemp()
     fpath = os.path.join(tmpdir, "fproj.npy")
-    np.save(fpath, fproj)
+    np.save(fpath, smp.fproj)
     import multiprocessing as mp
-    nproc = cores
     per_step = []
-    with mp.get_context("spawn").Pool(nproc) as pool:
+    with mp.get_context("spawn").Pool(cores) as pool:
+        pool.map(_ref_worker, [(smp.locus, smp.det, smp.obj, fpath)] * cores)  # load + page in
         for it in range(args.warmup + args.steps):
             t0 = time.perf_counter()
-            pool.map(_ref_worker, [(locus, det, obj, fpath)] * nproc)
-            wall_bp = time.perf_counter() - t0
-            bp_rate = nproc * block_updates / wall_bp  # updates/s on all cores
-            nv = 8
-            t1 = time.perf_counter()
-            cpu_filter_views(O, s, proj[:nv + 2])
-            t_view = (time.perf_counter() - t1) / nv
-            t_scan = full_updates / bp_rate + t_view * s.P
+            smp.filter_once()
+            pool.map(_ref_worker, [(smp.locus, smp.det, smp.obj, fpath)] * cores)
             if it >= args.warmup:
-                per_step.append(t_scan)
+                per_step.append(time.perf_counter() - t0)
     os.unlink(fpath)
     os.rmdir(tmpdir)
-    t_scan = statistics.median(per_step)
-    gups = full_updates / t_scan / 1e9
-    sample = (f"per step: KatsevichBkProj.cpp (oracle/_ref) on a central {n}^3 block at the "
-              f"workload's voxel pitch ({block_updates} updates) in {nproc} processes, plus "
-              f"the FP64 filter restatement on 8 views with {cores} threads; scaled to the "
-              f"full scan ({full_updates} updates, {s.P} views)")
+    t_step = statistics.mean(per_step)
+    gups = smp.updates / t_step / 1e9
+    sample = smp.describe("the FP64", f"KatsevichBkProj.cpp (oracle/_ref) in {cores} processes")
     line = {"impl": "reference", "metric": METRIC, "value": gups, "unit": "GUPS",
             "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": t_scan * 1e3, "higher_is_better": True, "scaling": "weak",
+            "ms_per_step": t_step * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": workload_name(s), "volume": list(s.vol_shape),
-                       "detector": [s.ZL, s.YL], "views": s.P},
+            "config": workload_config(s, ws),
             "cpu_baseline": {"value": gups, "unit": "GUPS", "cores": cores,
                              "kind": "reference", "sample": sample},
             "e2e": {"value": gups, "unit": "GUPS", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
-            "s_per_vol": t_scan}
+            "updates_per_step": smp.updates, "s_per_vol": full_updates / (gups * 1e9)}
     print(json.dumps(line))
 
 
@@ -341,6 +392,7 @@ def _full_update_count(s):
             torch.cuda.synchronize()
             n = int(d_cnt.item())
             c.close()
+            del d_tab
             return n
     except Exception:
         pass
@@ -555,6 +607,154 @@ def run_report_extras(args):
     ctx.close()
 
 
+def _refgpu_guard(s, AL, n_vox):
+    """Sizes the reference GPU MEX files handle, found by reading them: int32 element indices
+    (KatsevichFiltering_GPU.cu:294 (pIdx*AL + AIndex)*YL, :71, :820), a 3-D texture of depth
+    ProjNum (KatsevichBkProj_GPU.cu:262, at most 16384), the Hilbert batches of 1024 views
+    (:685: fewer views make its batch loop run past the data), and coordinate vectors sized
+    ProjNum that receive RecMX/RecMY/RecMZ entries (KatsevichBkProj_GPU.cu:300-309)."""
+    P = s.P
+    lim = 2 ** 31 - 1
+    if P * AL * s.YL > lim or P * s.ZL * s.YL > lim:
+        return "element indices exceed int32 in the reference GPU filter"
+    if P < 1024:
+        return "fewer than 1024 views: the reference's Hilbert batching needs at least one batch"
+    if P > 16384:
+        return "more than 16384 views: beyond a 3-D texture's depth"
+    if max(n_vox) > P:
+        return "a volume side larger than the view count overruns the reference's vectors"
+    return None
+
+
+def run_report_refgpu(args):
+    """The reference's own GPU MEX functions (KatsevichFiltering_GPU.cu, KatsevichBkProj_GPU.cu)
+    recompiled for sm_100a against the mex.h shim (baseline/Makefile), on the c2 scan: their
+    time through the MEX interface (FP64 host arrays, synchronous, as MATLAB calls them), the
+    device time of their kernels (CUDA events on the legacy stream they use), and their error
+    against the FP64 oracle on a central block -- beside this library's MEX modules on the same
+    arrays. Not a parity target: the reference GPU path has no endpoint weights, FP32 cuFFT and
+    9-bit texture interpolation weights."""
+    import torch
+    import ctrecon_b200 as ct
+    from ctrecon_b200.mexharness import MexModule
+    s = config(args.config if args.config not in ("c3",) else "c2")
+    AL = 2 * int(np.ceil(s.ZL * 1.3 * 0.5)) + 1
+    refdir = os.path.join(ROOT, "baseline", "_ref")
+    fpath = os.path.join(refdir, "KatsevichFiltering_GPU_ref.so")
+    bpath = os.path.join(refdir, "KatsevichBkProj_GPU_ref.so")
+    why = _refgpu_guard(s, AL, s.vol_shape)
+    if why is None and not (os.path.exists(fpath) and os.path.exists(bpath)):
+        why = "baseline/_ref (the reference GPU MEX files built by baseline/Makefile) is missing"
+    if why:
+        print(json.dumps({"report": "refgpu", "unavailable": why, "workload": workload_name(s)}))
+        return
+    O = _oracle()
+    ctx = ct.Context(0)
+    geom = s.geom_struct()
+    d_proj = torch.empty(s.proj_shape, dtype=torch.float32, device="cuda")
+    ctx.phantom_dev(geom, s.ellipsoids(), d_proj, photons=s.photons or 0.0, seed=s.seed)
+    proj64 = d_proj.cpu().numpy().astype(np.float64)   # pageable, as MATLAB's arrays
+    fargs = list(s.filter_args())
+    leg = torch.cuda.default_stream()  # the legacy stream the reference's thrust and kernels use
+
+    def timed(fn, reps=2):
+        fn()
+        torch.cuda.synchronize()
+        walls, devs = [], []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(leg)
+            t0 = time.perf_counter()
+            fn()
+            e1.record(leg)
+            torch.cuda.synchronize()
+            walls.append(time.perf_counter() - t0)
+            devs.append(e0.elapsed_time(e1) / 1e3)
+        return min(walls), min(devs)
+
+    out = {"report": "refgpu", "workload": workload_name(s), "updates": None,
+           "arrays": "FP64 pageable host arrays through the MEX interface (mex.h shim)"}
+    ref_f = MexModule(fpath)
+    ref_b = MexModule(bpath)
+    ours_f = MexModule(os.path.join(ROOT, "ctrecon_b200", "lib", "mex", "KatsevichFiltering_GPU.so"))
+    ours_b = MexModule(os.path.join(ROOT, "ctrecon_b200", "lib", "mex", "KatsevichBkProj_GPU.so"))
+    for m in (ref_f, ref_b, ours_f, ours_b):
+        m.set_print(False)
+    f_ref = np.empty_like(proj64)
+    f_ours = np.empty_like(proj64)
+    w, d = timed(lambda: ref_f.call([proj64] + fargs + [f_ref]))
+    out["filter_reference_gpu"] = {"wall_s": w, "device_span_s": d}
+    w, d = timed(lambda: ours_f.call([proj64] + fargs + [f_ours]))
+    out["filter_ours_mex"] = {"wall_s": w, "device_span_s": d}
+    img_ref = np.zeros(s.vol_shape)
+    img_ours = np.zeros(s.vol_shape)
+    w, d = timed(lambda: ref_b.call([geom, f_ref, img_ref]))
+    out["bkproj_reference_gpu"] = {"wall_s": w, "device_span_s": d}
+    w, d = timed(lambda: ours_b.call([geom, f_ours, img_ours]))
+    out["bkproj_ours_mex"] = {"wall_s": w, "device_span_s": d}
+    # device-resident kernels of this library on the same scan, for the kernel-only comparison
+    fpar = ct.scan_filter_params(s)
+    d_f = torch.empty_like(d_proj)
+    d_img = torch.zeros(s.vol_shape, dtype=torch.float32, device="cuda")
+    d_tab = torch.empty(ctx.pi_table_bytes(geom), dtype=torch.uint8, device="cuda")
+    d_cnt = torch.zeros(1, dtype=torch.int64, device="cuda")
+    ctx.pi_dev(geom, d_tab, d_cnt)
+    torch.cuda.synchronize()
+    updates = int(d_cnt.item())
+    out["updates"] = updates
+    cur = torch.cuda.current_stream()
+
+    def dev_ms(fn):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(cur)
+        fn()
+        e1.record(cur)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 1e3
+
+    out["filter_ours_device_s"] = dev_ms(lambda: ctx.filter_dev(fpar, d_proj, d_f))
+    out["pi_bkproj_ours_device_s"] = dev_ms(lambda: (ctx.pi_dev(geom, d_tab),
+                                                     ctx.bkproj_dev(geom, d_f, d_img,
+                                                                    d_pitab=d_tab)))
+    # accuracy on the central block: the reference GPU filter's views and its backprojection
+    # (of the oracle's filtered views) against the FP64 oracle
+    n = 48
+    locus, det, obj, lo, hi = block_problem(O, s, n)
+    a0, a1 = max(0, lo - 1), min(s.P, hi + 1)
+    orc_f = np.ascontiguousarray(cpu_filter_views(O, s, proj64[a0:a1])[lo - a0:hi - a0])
+    gb = O.bp_geom(locus, det, obj, honour_extras=True)
+    orc_img, _, touched = O.bkproj(gb, orc_f, np.zeros((n, n, n)), want_touched=True)
+    t = touched.astype(bool)
+
+    def err(x, r, m=None):
+        x, r = (x[m], r[m]) if m is not None else (x, r)
+        return {"rel_rmse": float(np.linalg.norm(x - r) / np.linalg.norm(r)),
+                "max_abs": float(np.abs(x - r).max())}
+
+    block = {"Locus": np.array(locus), "Detector": np.array(det), "Object": np.array(obj)}
+    bimg_ref = np.zeros((n, n, n))
+    ref_b.call([block, orc_f, bimg_ref])
+    bimg_ours = np.zeros((n, n, n))
+    ours_b.call([block, orc_f, bimg_ours])
+    out["accuracy_vs_fp64_oracle"] = {
+        "filter_reference_gpu": err(f_ref[lo:hi], orc_f),
+        "filter_ours": err(f_ours[lo:hi], orc_f),
+        "bkproj_reference_gpu": err(bimg_ref, orc_img, t),
+        "bkproj_ours": err(bimg_ours, orc_img, t),
+        "block": {"voxels": n ** 3, "written": int(t.sum()), "views": [lo, hi]}}
+    fr, fo = out["filter_reference_gpu"], out["filter_ours_mex"]
+    br, bo = out["bkproj_reference_gpu"], out["bkproj_ours_mex"]
+    out["speedup_mex"] = {"filter": fr["wall_s"] / fo["wall_s"],
+                          "bkproj": br["wall_s"] / bo["wall_s"],
+                          "chain": (fr["wall_s"] + br["wall_s"]) / (fo["wall_s"] + bo["wall_s"])}
+    out["gups_mex"] = {"reference_gpu": updates / (fr["wall_s"] + br["wall_s"]) / 1e9,
+                       "ours": updates / (fo["wall_s"] + bo["wall_s"]) / 1e9}
+    print(json.dumps(out))
+    ctx.close()
+
+
 def _train_pinet(ctx, s, out, stream, torch):
     """Trains the learned PI-line initialiser on the GPU (2^22 FP64 Newton pairs, 8 epochs)."""
     import ctypes
@@ -573,6 +773,9 @@ def run_report(args):
     """Reports of the c3 and c5 configurations (not the headline line)."""
     if args.report == "extras":
         run_report_extras(args)
+        return
+    if args.report == "refgpu":
+        run_report_refgpu(args)
         return
     import torch
     import ctrecon_b200 as ct
@@ -745,17 +948,63 @@ def run_report(args):
 
 
 # ---------------------------------------------------------------------------------------------
-def main():
-    args = parse()
-    if args.impl == "reference":
-        run_reference(args)
-        return
-    if args.batched:
-        run_batched(args)
-        return
-    if args.report:
-        run_report(args)
-        return
+FP32_LANES_PER_SM = 128  # FP32 FMA per SM and clock (sm_100)
+SMS = 148
+
+
+def kernel_rooflines(s, kt, steps, updates, peaks, sm_mhz, hil):
+    """Per-kernel time and roofline fraction from the CUDA-event kernel times `kt` ({kind:
+    (ms, launches)}) of `steps` steps. Algorithmic work per view / per update:
+      K1 deriv_rebin   HBM: 4*YL*ZL bytes read + 4*AL*YLp written (FP32, or BF16 hi + lo)
+      K2 hilbert_tc    tensor: 2*YL^2*AL flop per view (the dense Toeplitz product); the BF16x3
+                       split executes 3 products of YLp^2, reported as `executed`
+      K2 hilbert_simt  FP32 FMA pipe: AL*YL*YL/2 FMA per view (odd lags only) at
+                       128 FMA/SM/clock
+      cell_records     HBM: 4 bytes read + 16 written per detector cell and view
+      backproject      issue: warp instructions per update (ncu, profiles/inst_per_update.txt)
+                       over 148 SMs x 4 schedulers x the SM clock."""
+    YL, ZL, P = s.YL, s.ZL, s.P
+    AL = 2 * int(np.ceil(ZL * 1.3 * 0.5)) + 1
+    YLp = (YL + 63) // 64 * 64
+    clk = (sm_mhz or 1965.0) * 1e6
+    out = {}
+    for kind, (ms, n) in kt.items():
+        if n == 0:
+            continue
+        t = ms / 1e3 / steps  # seconds per step
+        r = {"ms_per_step": ms / steps, "launches_per_step": n / steps}
+        if kind == "deriv_rebin":
+            b = P * (4 * YL * ZL + 4 * AL * YLp)
+            r.update(bound="hbm", achieved_gbs=b / t / 1e9, peak_gbs=peaks["hbm_gbs"],
+                     frac=b / t / 1e9 / peaks["hbm_gbs"], algorithmic_bytes=b)
+        elif kind == "hilbert_tc":
+            f = 2.0 * YL * YL * AL * P
+            ex = (3 if hil == "bf16x3" else 1) * 2.0 * YLp * YLp * AL * P
+            pk = peaks["bf16_tflops"] * (1 if hil == "bf16x3" else 0.5)
+            r.update(bound="tensor", achieved_tflops=f / t / 1e12, peak_tflops=pk,
+                     frac=f / t / 1e12 / pk, executed_tflops=ex / t / 1e12,
+                     executed_frac=ex / t / 1e12 / pk, algorithmic_flop=f,
+                     peak_note="BF16 burst of measured" if hil == "bf16x3" else
+                     "half the BF16 burst of measured (TF32 rate)")
+        elif kind == "hilbert_simt":
+            fma = AL * YL * (YL / 2.0) * P
+            pk = SMS * FP32_LANES_PER_SM * clk
+            r.update(bound="fp32_fma", achieved_tflops=2 * fma / t / 1e12,
+                     peak_tflops=2 * pk / 1e12, frac=fma / t / pk, algorithmic_fma=fma)
+        elif kind == "cell_records":
+            b = P * (YL - 1) * (ZL - 1) * 20
+            r.update(bound="hbm", achieved_gbs=b / t / 1e9, peak_gbs=peaks["hbm_gbs"],
+                     frac=b / t / 1e9 / peaks["hbm_gbs"], algorithmic_bytes=b)
+        elif kind == "backproject":
+            r.update(gups=updates / t / 1e9,
+                     gather_equivalent_gbs=BYTES_PER_UPDATE * updates / t / 1e9)
+        elif kind == "pi_solve":
+            r.update(voxels_per_s=float(np.prod(s.vol_shape)) / t)
+        out[kind] = r
+    return out
+
+
+def run_headline(args):
     import torch
     import ctrecon_b200 as ct
     from ctrecon_b200 import _lib
@@ -763,26 +1012,17 @@ def main():
     ws, rank, local = dist_setup(args.gpus)
     dev = torch.device("cuda", local)
     s = config(args.config)
-    hil = {"fp32": _lib.HILBERT_FP32, "bf16x3": _lib.HILBERT_BF16X3,
-           "tf32": _lib.HILBERT_TF32}[args.hilbert]
-    pis = {"bisect": _lib.PI_BISECT, "newton": _lib.PI_NEWTON, "learned": _lib.PI_LEARNED}[args.pi]
-    ctx = ct.Context(local, hilbert=hil, pi_solver=_lib.PI_BISECT)
-    ctx.set_option(_lib.OPT_BP_VARIANT, args.bp_variant)
+    hil_of = {"fp32": _lib.HILBERT_FP32, "bf16x3": _lib.HILBERT_BF16X3,
+              "tf32": _lib.HILBERT_TF32}
+    pi_of = {"bisect": _lib.PI_BISECT, "newton": _lib.PI_NEWTON, "learned": _lib.PI_LEARNED}
+    ctx = ct.Context(local)
     ctx.set_option(_lib.OPT_PINET_MODE, {"voxel-fp32": _lib.PINET_VOXEL_FP32,
                                          "voxel-bf16": _lib.PINET_VOXEL_BF16,
                                          "grid": _lib.PINET_GRID}[args.pinet_mode])
     geom = s.geom_struct()
     fpar = ct.scan_filter_params(s)
-    pinet_info = None
-    if pis == _lib.PI_LEARNED:
-        import ctypes
-        loss = ctypes.c_float()
-        t0 = time.perf_counter()
-        _lib.check(_lib.lib().ctrecon_pinet_train(
-            ctx.handle, torch.cuda.current_stream().cuda_stream, 1 << 22, 8192, 8,
-            s.ObjR / s.ScanR * 1.05, 2024, ctypes.byref(loss)), ctx.handle)
-        pinet_info = {"train_pairs": 1 << 22, "epochs": 8, "train_s": time.perf_counter() - t0,
-                      "final_loss": loss.value}
+    stream = torch.cuda.current_stream()
+    peaks = load_peaks()
 
     # ---- inputs, resident in HBM before timing --------------------------------------------------
     d_proj = torch.empty(s.proj_shape, dtype=torch.float32, device=dev)
@@ -796,15 +1036,34 @@ def main():
     ctx.pi_dev(geom, d_tab, d_cnt)
     torch.cuda.synchronize()
     updates = int(d_cnt.item())
-    ctx.set_option(_lib.OPT_PI_SOLVER, pis)
-    stream = torch.cuda.current_stream()
+
+    pinet_info = None
+
+    def train_pinet():
+        nonlocal pinet_info
+        if pinet_info is not None:
+            return
+        import ctypes
+        loss = ctypes.c_float()
+        t0 = time.perf_counter()
+        _lib.check(_lib.lib().ctrecon_pinet_train(
+            ctx.handle, stream.cuda_stream, 1 << 22, 8192, 8, s.ObjR / s.ScanR * 1.05, 2024,
+            ctypes.byref(loss)), ctx.handle)
+        torch.cuda.synchronize()
+        pinet_info = {"train_pairs": 1 << 22, "epochs": 8,
+                      "train_s": time.perf_counter() - t0, "final_loss": loss.value}
+
+    # ---- the backprojector form: the autotuner's choice on this workload (untimed) ------------
     tune = None
     if args.bp_variant == -1:
-        # the autotuner picks the backprojector form on this workload (untimed setup)
+        ctx.set_option(_lib.OPT_HILBERT, _lib.HILBERT_FP32)
         ctx.filter_dev(fpar, d_proj, d_fproj)
         tune = ctx.tune_bkproj(geom, d_fproj, d_img, d_pitab=d_tab)
         ctx.set_option(_lib.OPT_BP_VARIANT, _lib.BP_AUTO)
-    bp_form = tune["best_variant"] if tune else args.bp_variant
+        bp_form = tune["best_variant"]
+    else:
+        ctx.set_option(_lib.OPT_BP_VARIANT, args.bp_variant)
+        bp_form = args.bp_variant
 
     ev = {k: [] for k in ("f0", "f1", "p1", "b1")}
 
@@ -824,83 +1083,137 @@ def main():
             for k, x in zip(("f0", "f1", "p1", "b1"), e):
                 ev[k].append(x)
 
-    for _ in range(max(3, args.warmup)):
-        step(False)
-    torch.cuda.synchronize()
-    barrier(ws)
-    sampler = ClockSampler(local)
-    sampler.start()
-    time.sleep(0.3)
-    torch.cuda.synchronize()
-    barrier(ws)
-    t_start = torch.cuda.Event(enable_timing=True)
-    t_end = torch.cuda.Event(enable_timing=True)
-    t_start.record(stream)
-    for _ in range(args.steps):
-        step(True)
-    t_end.record(stream)
-    torch.cuda.synchronize()
-    barrier(ws)
-    clocks = sampler.stop()
-    ms_total = t_start.elapsed_time(t_end)
-    ms_step = max_over_ranks(ms_total / args.steps, ws)
-    filt_ms = statistics.mean(a.elapsed_time(b) for a, b in zip(ev["f0"], ev["f1"]))
-    pi_ms = statistics.mean(a.elapsed_time(b) for a, b in zip(ev["f1"], ev["p1"]))
-    bp_ms = statistics.mean(a.elapsed_time(b) for a, b in zip(ev["p1"], ev["b1"]))
-    value = replica_gups(updates, ms_step, ws)
-    chunk = ctx.get_option(_lib.OPT_FILTER_CHUNK)
-    nchunks = (s.P + chunk - 1) // chunk
-    launches_per_step = 2 * nchunks + 1 + 1
-    if hil != _lib.HILBERT_FP32:
-        launches_per_step += nchunks
-    if pis == _lib.PI_LEARNED:
-        launches_per_step += 1  # the network's inference kernel before the Newton solve
-    if 10 <= bp_form < 100:
-        # the fifth form writes the cell records of each view window (up to 32 GiB) before its
-        # launch
-        plane = (s.ZL - 1) * (s.YL - 1) * 16
-        per = max(1, (32 << 30) // plane)
-        launches_per_step += 2 * ((s.P + per - 1) // per) - 1
-
-    # ---- the mixed-precision + learned form on the same resident inputs ----------------------
-    # (the metric compares plain FP32 against it): BF16x3 Hilbert, the learned PI start, the same
-    # backprojector form; reported beside the plain line, not as its value
-    mixed = None
-    if hil == _lib.HILBERT_FP32 and pis == _lib.PI_BISECT and not args.no_mixed:
-        import ctypes
-        if pinet_info is None:
-            loss = ctypes.c_float()
-            _lib.check(_lib.lib().ctrecon_pinet_train(
-                ctx.handle, stream.cuda_stream, 1 << 22, 8192, 8, s.ObjR / s.ScanR * 1.05,
-                2024, ctypes.byref(loss)), ctx.handle)
-        ctx.set_option(_lib.OPT_HILBERT, _lib.HILBERT_BF16X3)
-        ctx.set_option(_lib.OPT_PI_SOLVER, _lib.PI_LEARNED)
+    def time_form(hil, pis):
+        """K device-resident steps of one form; CUDA events on the launching stream, the
+        slowest rank's time, per-phase means and per-kernel times."""
+        ctx.set_option(_lib.OPT_HILBERT, hil_of[hil])
+        ctx.set_option(_lib.OPT_PI_SOLVER, pi_of[pis])
+        if pis == "learned":
+            train_pinet()
         for k in ev:
             ev[k].clear()
+        ctx.set_option(_lib.OPT_KERNEL_TIMING, 0)
         for _ in range(max(3, args.warmup)):
             step(False)
         torch.cuda.synchronize()
         barrier(ws)
-        m0, m1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        m0.record(stream)
+        ctx.kernel_times()  # drop anything recorded before
+        ctx.set_option(_lib.OPT_KERNEL_TIMING, 1)
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
         for _ in range(args.steps):
             step(True)
-        m1.record(stream)
+        t1.record(stream)
         torch.cuda.synchronize()
         barrier(ws)
-        mms = max_over_ranks(m0.elapsed_time(m1) / args.steps, ws)
-        mixed = {"value": replica_gups(updates, mms, ws), "unit": "GUPS", "ms_per_step": mms,
-                 "hilbert": "bf16x3", "pi_solver": "learned",
-                 "phase_ms": {
-                     "filter": statistics.mean(a.elapsed_time(b) for a, b in zip(ev["f0"], ev["f1"])),
-                     "pi": statistics.mean(a.elapsed_time(b) for a, b in zip(ev["f1"], ev["p1"])),
-                     "bkproj": statistics.mean(a.elapsed_time(b) for a, b in zip(ev["p1"], ev["b1"]))},
-                 "vs_plain": ms_step / mms}
-        ctx.set_option(_lib.OPT_HILBERT, hil)
-        ctx.set_option(_lib.OPT_PI_SOLVER, pis)
+        ctx.set_option(_lib.OPT_KERNEL_TIMING, 0)
+        kt = ctx.kernel_times()
+        ms = max_over_ranks(t0.elapsed_time(t1) / args.steps, ws)
+        ph = {"filter": statistics.mean(a.elapsed_time(b) for a, b in zip(ev["f0"], ev["f1"])),
+              "pi": statistics.mean(a.elapsed_time(b) for a, b in zip(ev["f1"], ev["p1"])),
+              "bkproj": statistics.mean(a.elapsed_time(b) for a, b in zip(ev["p1"], ev["b1"]))}
+        return {"value": replica_gups(updates, ms, ws), "unit": "GUPS", "ms_per_step": ms,
+                "s_per_vol": ms / 1e3, "hilbert": hil, "pi_solver": pis, "bp_variant": bp_form,
+                "phase_ms": ph, "kernel_times": kt}
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    plain = time_form(args.hilbert, args.pi)
+    plain_form = (args.hilbert, args.pi) == ("fp32", "bisect")
+    forms = {}
+    batched_equal = None
+    if plain_form and not args.no_mixed:
+        forms["mixed_learned"] = time_form("bf16x3", "learned")
+        forms["mixed_learned"]["vs_plain"] = plain["ms_per_step"] / forms["mixed_learned"]["ms_per_step"]
+        mixed_img = d_img.clone()
+        if not args.no_batched:
+            # two copies of the scan through the batch API: both filters and PI solves, then ONE
+            # persistent backprojection launch over the tiles of both volumes; captured into a
+            # CUDA graph on the second run and replayed
+            b = ct.Batch(ctx, [s, s])
+            b.set_variant(bp_form if 0 <= bp_form < 100 else 12)
+            d_fproj2, d_img2 = torch.empty_like(d_proj), torch.zeros_like(d_img)
+            bargs = ([d_proj, d_proj], [d_fproj, d_fproj2], [d_img, d_img2])
+            sb = torch.cuda.Stream()
+            with torch.cuda.stream(sb):
+                for _ in range(max(3, args.warmup)):
+                    b.run(*bargs, stream=sb, use_graph=True)
+                sb.synchronize()
+                barrier(ws)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(sb)
+                for _ in range(args.steps):
+                    b.run(*bargs, stream=sb, use_graph=True)
+                e1.record(sb)
+                sb.synchronize()
+                barrier(ws)
+            ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, ws)
+            # the batch's volumes against the single-scan mixed + learned volume (same options)
+            batched_equal = bool(torch.equal(d_img, mixed_img) and torch.equal(d_img2, mixed_img))
+            forms["mixed_learned_batched"] = {
+                "value": replica_gups(2 * updates, ms, ws), "unit": "GUPS", "ms_per_step": ms,
+                "scans_per_step": 2, "s_per_vol": ms / 2e3, "hilbert": "bf16x3",
+                "pi_solver": "learned", "bp_variant": b.variants()[0], "graph": True,
+                "vs_plain": plain["ms_per_step"] / (ms / 2),
+                "volumes_equal_single_scan_form": batched_equal}
+            b.close()
+            del d_fproj2, d_img2
+        del mixed_img
+    clocks = sampler.stop()
+    value = plain["value"]
+    ms_step = plain["ms_per_step"]
+
+    # ---- accuracy: every form's whole chain against the FP64 oracle on a central block --------
+    accuracy = None
+    if rank == 0 and not args.no_accuracy:
+        O = _oracle()
+        n = 48
+        locus, det, obj, lo, hi = block_problem(O, s, n)
+        a0, a1 = max(0, lo - 1), min(s.P, hi + 1)
+        t0 = time.perf_counter()
+        ref_f = np.ascontiguousarray(cpu_filter_views(
+            O, s, d_proj[a0:a1].cpu().numpy().astype(np.float64))[lo - a0:hi - a0])
+        gb = O.bp_geom(locus, det, obj, honour_extras=True)
+        sentinel = -5.5
+        ref_img, _, touched = O.bkproj(gb, ref_f, np.full((n, n, n), sentinel),
+                                       want_touched=True)
+        t_oracle = time.perf_counter() - t0
+        t = touched.astype(bool)
+        block = {"Locus": locus, "Detector": det, "Object": obj}
+        accuracy = {"block": {"voxels": n ** 3, "written": int(t.sum()), "views": [lo, hi],
+                              "oracle_s": t_oracle,
+                              "oracle": "FP64 filter restatement + orc_bkproj (= "
+                                        "KatsevichBkProj.cpp bit for bit)"}}
+        for name, (hil, pis) in (("plain", (args.hilbert, args.pi)),
+                                 ("mixed_learned", ("bf16x3", "learned"))):
+            if name != "plain" and name not in forms:
+                continue
+            ctx.set_option(_lib.OPT_HILBERT, hil_of[hil])
+            ctx.set_option(_lib.OPT_PI_SOLVER, pi_of[pis])
+            ctx.filter_dev(fpar, d_proj, d_fproj)
+            d_blk = torch.full((n, n, n), sentinel, dtype=torch.float32, device=dev)
+            ctx.bkproj_dev(block, d_fproj[lo:hi].contiguous(), d_blk)
+            torch.cuda.synchronize()
+            got = d_blk.cpu().numpy().astype(np.float64)
+            d = (got - ref_img)[t]
+            accuracy[name] = {
+                "rel_rmse": float(np.linalg.norm(d) / np.linalg.norm(ref_img[t])),
+                "max_abs": float(np.abs(d).max()),
+                "ref_max_abs": float(np.abs(ref_img[t]).max()),
+                "untouched_kept": bool(np.array_equal(got[~t], ref_img[~t]))}
+        if "mixed_learned_batched" in forms:
+            accuracy["mixed_learned_batched"] = dict(
+                accuracy["mixed_learned"],
+                note="its volumes are bit-identical to the single-scan mixed_learned form's "
+                     "(checked in this run)" if batched_equal else
+                     "its volumes DIFFER from the single-scan form's")
+    ctx.set_option(_lib.OPT_HILBERT, hil_of[args.hilbert])
+    ctx.set_option(_lib.OPT_PI_SOLVER, pi_of[args.pi])
 
     # ---- e2e through the MEX-equivalent host calls (FP64 pinned host buffers) -----------------
-    e2e = None
+    e2e = e2e_pageable = None
+    nproj, nvox = int(np.prod(s.proj_shape)), int(np.prod(s.vol_shape))
     if not args.no_e2e:
         h_proj = torch.empty(s.proj_shape, dtype=torch.float64, pin_memory=True)
         h_proj.copy_(d_proj.cpu().to(torch.float64))
@@ -917,23 +1230,78 @@ def main():
             ctx.bkproj_host(geom, np_fproj, np_img)        # KatsevichBkProj_GPU
         t_e2e = (time.perf_counter() - t0) / e2e_steps
         t_e2e = max_over_ranks(t_e2e, ws)
-        nproj, nvox = int(np.prod(s.proj_shape)), int(np.prod(s.vol_shape))
         e2e = {"value": ws * updates / t_e2e / 1e9, "unit": "GUPS",
                "h2d_bytes_per_step": 8 * (2 * nproj + nvox),
                "d2h_bytes_per_step": 8 * (nproj + nvox),
-               "s_per_vol": t_e2e,
-               "path": "ctrecon_filter_host_f64 + ctrecon_bkproj_host_f64 (MEX-equivalent)"}
+               "s_per_vol": t_e2e, "steps": e2e_steps,
+               "path": "ctrecon_filter_host_f64 + ctrecon_bkproj_host_f64 (MEX-equivalent), "
+                       "pinned FP64 host buffers"}
+        del h_fproj, h_img
+        # the MEX modules themselves, with pageable FP64 arrays as MATLAB passes them
+        # (FunctionKat_v6.m:85-113: FProj = Proj then KatsevichFiltering_GPU writes in place)
+        from ctrecon_b200.mexharness import MexModule
+        os.environ["CTRECON_DEVICE"] = str(local)  # the MEX modules' own contexts
+        libdir = os.path.join(ROOT, "ctrecon_b200", "lib", "mex")
+        mf = MexModule(os.path.join(libdir, "KatsevichFiltering_GPU.so"))
+        mb = MexModule(os.path.join(libdir, "KatsevichBkProj_GPU.so"))
+        p_proj = np.array(np_proj)          # pageable copies
+        del h_proj, np_proj
+        p_fproj = np.empty_like(p_proj)
+        p_img = np.zeros(s.vol_shape)
+        fargs = list(s.filter_args())
 
-    # ---- roofline of the dominant kernel (backprojection) -----------------------------------------
-    peak, peak_kind = load_peaks()
-    achieved = BYTES_PER_UPDATE * updates / (bp_ms / 1e3) / 1e9
+        def mex_step():
+            mf.call([p_proj] + fargs + [p_fproj])
+            mb.call([geom, p_fproj, p_img])
+
+        mex_step()
+        pg_steps = max(1, min(args.steps, 2))
+        barrier(ws)
+        t0 = time.perf_counter()
+        for _ in range(pg_steps):
+            mex_step()
+        t_pg = max_over_ranks((time.perf_counter() - t0) / pg_steps, ws)
+        e2e_pageable = {"value": ws * updates / t_pg / 1e9, "unit": "GUPS",
+                        "h2d_bytes_per_step": 8 * (2 * nproj + nvox),
+                        "d2h_bytes_per_step": 8 * (nproj + nvox), "s_per_vol": t_pg,
+                        "steps": pg_steps,
+                        "path": "KatsevichFiltering_GPU + KatsevichBkProj_GPU MEX modules "
+                                "(mex.h shim), pageable FP64 arrays"}
+        del p_proj, p_fproj, p_img
+
+    # ---- rooflines --------------------------------------------------------------------------------
+    kern = kernel_rooflines(s, plain["kernel_times"], args.steps, updates, peaks,
+                            clocks.get("sm_mhz"), args.hilbert)
+    if "mixed_learned" in forms:
+        forms["mixed_learned"]["kernels"] = kernel_rooflines(
+            s, forms["mixed_learned"]["kernel_times"], args.steps, updates, peaks,
+            clocks.get("sm_mhz"), "bf16x3")
     bp_kernel = ("k_bkproj" if bp_form >= 100 else "k_bkproj3" if bp_form in (0, 1)
                  else "k_bkproj2" if bp_form in (2, 3, 4) else "k_bkproj5" if bp_form >= 10
                  else "k_bkproj4")
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "peak_source": peak_kind,
-                "kernel": bp_kernel, "model": "16 B per voxel-view update",
-                "traffic": load_traffic(bp_kernel, workload_name(s))}
+    wl = workload_name(s)
+    ipu = load_profile_table("inst_per_update.txt").get((bp_kernel, wl))
+    roofline = None
+    bpk = kern.get("backproject")
+    if bpk:
+        t_bp = bpk["ms_per_step"] / 1e3
+        clk = (clocks.get("sm_mhz") or 1965.0) * 1e6
+        issue_peak = SMS * 4 * clk  # warp instructions per second
+        roofline = {"kernel": bp_kernel, "bound": "issue",
+                    "model": "warp instructions per update (ncu smsp__inst_executed.sum / "
+                             "updates, profiles/inst_per_update.txt) x updates / kernel time, "
+                             "over 148 SMs x 4 schedulers x the SM clock sampled in the run",
+                    "inst_per_update": ipu, "unit": "Ginst/s",
+                    "peak": issue_peak / 1e9, "peak_source": "148 x 4 x median SM clock",
+                    "achieved": ipu * updates / t_bp / 1e9 if ipu else None,
+                    "frac": ipu * updates / t_bp / issue_peak if ipu else None,
+                    "traffic": load_traffic(bp_kernel, wl),
+                    "hbm_gather_equivalent": {
+                        "model": "16 B per update (the four FP32 taps the reference reads, "
+                                 "KatsevichBkProj.cpp:253-256); the taps come from shared "
+                                 "memory, so this is not an HBM bound",
+                        "achieved_gbs": BYTES_PER_UPDATE * updates / t_bp / 1e9,
+                        "hbm_peak_gbs": peaks["hbm_gbs"]}}
 
     # ---- CPU baseline (rank 0, N = 1): the FP64 oracle restatement on a bounded sample -----------
     cpu = None
@@ -941,48 +1309,57 @@ def main():
         try:
             O = _oracle()
             cores = os.cpu_count() or 1
-            n = 48
-            locus, det, obj, lo, hi = block_problem(O, s, n)
-            proj_sub = d_proj[lo:hi].cpu().numpy().astype(np.float64)
-            t1 = time.perf_counter()
-            cpu_filter_views(O, s, proj_sub[:10])
-            t_view = (time.perf_counter() - t1) / 8
-            fproj_sub = d_fproj[lo:hi].cpu().numpy().astype(np.float64)
-            t_bp, n_bp = cpu_bp_sample_port(O, s, fproj_sub, lo, hi, cores, n=n)
-            t_scan = t_view * s.P + t_bp * updates / max(n_bp, 1)
-            cpu = {"value": updates / t_scan / 1e9, "unit": "GUPS", "cores": cores,
-                   "kind": "port", "s_per_vol": t_scan,
-                   "sample": (f"FP64 oracle with {cores} OpenMP threads: filter of 8 views and "
-                              f"backprojection of a central {n}^3 block ({n_bp} updates), "
-                              f"scaled to {s.P} views and {updates} updates")}
+            smp = CpuChainSample(O, s, lambda a, b: d_proj[a:b].cpu().numpy().astype(np.float64),
+                                 updates, n=32, copies=1)
+            t0 = time.perf_counter()
+            smp.filter_once()
+            O.bkproj(smp.gb, smp.fproj, np.zeros((smp.n,) * 3), nthreads=cores)
+            t_smp = time.perf_counter() - t0
+            g = smp.updates / t_smp / 1e9
+            cpu = {"value": g, "unit": "GUPS", "cores": cores, "kind": "port",
+                   "s_per_vol": updates / (g * 1e9), "sample_s": t_smp,
+                   "sample": smp.describe("the FP64 oracle's",
+                                          f"the FP64 oracle with {cores} OpenMP threads")}
         except Exception as exc:  # the baseline is reported, never required
             cpu = {"value": None, "unit": "GUPS", "cores": 0, "kind": "port",
                    "sample": f"failed: {exc}"}
 
     if rank == 0:
+        launches = sum(n for _, n in plain["kernel_times"].values())
         line = {"metric": METRIC, "value": value, "unit": "GUPS", "n_gpus": ws,
                 "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": ms_step,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "f32", "data": "synthetic",
-                "config": {"workload": workload_name(s), "volume": list(s.vol_shape),
-                           "voxel_mm": list(s.voxel_size), "detector": [s.ZL, s.YL],
-                           "views": s.P, "views_per_turn": s.views_per_turn,
-                           "hilbert": args.hilbert, "pi_solver": args.pi,
-                           "bp_variant": bp_form,
-                           "parallelism": f"replicas{ws}",
-                           "l2": "inputs larger than L2 (projections 1.75 GB)"},
+                "dtype": "f32", "data": "synthetic", "config": workload_config(s, ws),
+                "form": {k: plain[k] for k in ("hilbert", "pi_solver", "bp_variant")},
                 "updates_per_step": updates, "s_per_vol": ms_step / 1e3,
-                "phase_ms": {"filter": filt_ms, "pi": pi_ms, "bkproj": bp_ms},
-                "bkproj_gups": updates / (bp_ms / 1e3) / 1e9,
-                "pinet": pinet_info, "bp_tune": tune,
-                "gpu_launches": launches_per_step * args.steps,
-                "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
-                "mixed_learned": mixed}
+                "phase_ms": plain["phase_ms"],
+                "bkproj_gups": updates / (plain["phase_ms"]["bkproj"] / 1e3) / 1e9,
+                "gpu_launches": launches,
+                "e2e": e2e, "e2e_pageable": e2e_pageable, "roofline": roofline,
+                "kernels": kern, "cpu_baseline": cpu, "clocks": clocks,
+                "forms": {k: {kk: vv for kk, vv in v.items() if kk != "kernel_times"}
+                          for k, v in forms.items()},
+                "accuracy": accuracy, "pinet": pinet_info, "bp_tune": tune,
+                "peaks": peaks}
         print(json.dumps(line))
     ctx.close()
     if ws > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    if args.batched:
+        run_batched(args)
+        return
+    if args.report:
+        run_report(args)
+        return
+    run_headline(args)
 
 
 if __name__ == "__main__":

@@ -30,6 +30,11 @@ OPT_HILBERT, OPT_PI_SOLVER, OPT_FILTER_CHUNK, OPT_BP_VARIANT, OPT_VERBOSE = 1, 2
 OPT_DERIVATIVE = 6
 OPT_BP_WINDOW = 7
 OPT_PINET_MODE = 8
+OPT_KERNEL_TIMING = 9
+OPT_TC_FORM = 10
+TC_PARITY_SPLIT, TC_SINGLE_PASS = 0, 1
+KERNEL_KINDS = ("deriv_rebin", "hilbert_simt", "hilbert_tc", "pi_solve", "cell_records",
+                "backproject")
 PINET_VOXEL_FP32, PINET_VOXEL_BF16, PINET_GRID = 0, 1, 2
 DERIV_DIRECT, DERIV_CHAIN = 0, 1
 
@@ -97,6 +102,7 @@ SIGNATURES = [
     ("ctrecon_selftest_bounded_wait", _st, [_vp, _vp, ctypes.c_int]),
     ("ctrecon_sync", _st, [_vp, _vp]),
     ("ctrecon_pi_dev_stats", _st, [_vp, _vp, ctypes.POINTER(BPGeom), _vp, _vp, _vp]),
+    ("ctrecon_kernel_times", _st, [_vp, _dp, ctypes.POINTER(ctypes.c_ulonglong), ctypes.c_int]),
     ("ctrecon_batch_create", _st, [_vp, ctypes.c_int, ctypes.POINTER(FilterParams),
                                    ctypes.POINTER(BPGeom), ctypes.POINTER(_vp)]),
     ("ctrecon_batch_destroy", None, [_vp]),

@@ -174,6 +174,16 @@ class Context:
         check(lib().ctrecon_get_option(self._h, int(opt), ctypes.byref(v)), self._h)
         return v.value
 
+    def kernel_times(self) -> dict:
+        """{kind: (ms, launches)} of the launches timed since the last call (with
+        OPT_KERNEL_TIMING on); waits for them."""
+        from . import _lib
+        n = len(_lib.KERNEL_KINDS)
+        ms = (ctypes.c_double * n)()
+        cnt = (ctypes.c_ulonglong * n)()
+        check(lib().ctrecon_kernel_times(self._h, ms, cnt, n), self._h)
+        return {k: (ms[i], int(cnt[i])) for i, k in enumerate(_lib.KERNEL_KINDS)}
+
     # -- host FP64 (MEX-equivalent) --------------------------------------------------------
     def filter_host(self, p: FilterParams, proj: np.ndarray, fproj: Optional[np.ndarray] = None):
         n = p.yl * p.zl * p.proj_number

@@ -92,7 +92,7 @@ Status build_filter_plan(const ctrecon_filter_params& p, FilterPlan& plan) {
     plan.tc_mode = -1;
     CTR_TRY(build_filter_tables(p, plan.t));
     const FilterTables& t = plan.t;
-    plan.YLp = (t.YL + 63) / 64 * 64;
+    plan.YLp = (t.YL + 127) / 128 * 128;  // halves of 64 columns for the parity split
     const size_t ay = (size_t)t.AL * t.YL, zy = (size_t)t.ZL * t.YL;
     std::vector<FwEntry> fw(ay);
     for (size_t i = 0; i < ay; ++i) fw[i] = FwEntry{t.r0[i], t.r1[i], (float)t.wa[i], (float)t.wb[i]};
@@ -294,7 +294,79 @@ void ctrecon_ctx_destroy(ctrecon_ctx* ctx) {
         cudaStreamDestroy(st);
     }
     for (cudaEvent_t e : ctx->events) cudaEventDestroy(e);
+    for (const ctr::KernelSpan& k : ctx->kspans) {
+        cudaEventDestroy(k.a);
+        cudaEventDestroy(k.b);
+    }
+    for (cudaEvent_t e : ctx->kev_free) cudaEventDestroy(e);
     delete ctx;
+}
+
+namespace ctr {
+// A timing event from the context's pool (created on demand); nullptr on failure.
+static cudaEvent_t take_timing_event(ctrecon_ctx* ctx) {
+    if (!ctx->kev_free.empty()) {
+        cudaEvent_t e = ctx->kev_free.back();
+        ctx->kev_free.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    return cudaEventCreate(&e) == cudaSuccess ? e : nullptr;
+}
+
+// at most this many launches are kept between two queries; later ones go untimed
+constexpr size_t kMaxKernelSpans = 1 << 20;
+
+KernelTimer::KernelTimer(ctrecon_ctx* c, cudaStream_t st, int k) : ctx(c), s(st), kind(k) {
+    if (!ctx || !ctx->opt_kernel_timing || ctx->kspans.size() >= kMaxKernelSpans) {
+        ctx = nullptr;
+        return;
+    }
+    a = take_timing_event(ctx);
+    if (!a || cudaEventRecord(a, s) != cudaSuccess) {
+        if (a) ctx->kev_free.push_back(a);
+        a = nullptr;
+        ctx = nullptr;
+    }
+}
+
+void KernelTimer::stop() {
+    if (!ctx || !a) return;
+    cudaEvent_t b = take_timing_event(ctx);
+    if (b && cudaEventRecord(b, s) == cudaSuccess) {
+        ctx->kspans.push_back(KernelSpan{kind, a, b});
+    } else {
+        ctx->kev_free.push_back(a);
+        if (b) ctx->kev_free.push_back(b);
+    }
+    a = nullptr;
+    ctx = nullptr;
+}
+}  // namespace ctr
+
+ctrecon_status ctrecon_kernel_times(ctrecon_ctx* ctx, double* ms, unsigned long long* launches,
+                                    int n) {
+    if (!ctx || (n > 0 && (!ms || !launches)) || n < 0) return CTRECON_ERR_INVALID_ARGUMENT;
+    for (int i = 0; i < n; ++i) {
+        ms[i] = 0;
+        launches[i] = 0;
+    }
+    Status st;
+    cudaSetDevice(ctx->device);
+    for (const KernelSpan& k : ctx->kspans) {
+        float t = 0.f;
+        cudaError_t e = cudaEventSynchronize(k.b);
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&t, k.a, k.b);
+        if (e != cudaSuccess && st.ok()) st = cuda_status(e, "kernel timing events");
+        if (e == cudaSuccess && k.kind >= 0 && k.kind < n) {
+            ms[k.kind] += t;
+            launches[k.kind] += 1;
+        }
+        ctx->kev_free.push_back(k.a);
+        ctx->kev_free.push_back(k.b);
+    }
+    ctx->kspans.clear();
+    return finish(ctx, st);
 }
 
 ctrecon_status ctrecon_set_option(ctrecon_ctx* ctx, ctrecon_option opt, int value) {
@@ -337,6 +409,12 @@ ctrecon_status ctrecon_set_option(ctrecon_ctx* ctx, ctrecon_option opt, int valu
             return finish(ctx, make_status(CTRECON_ERR_INVALID_ARGUMENT, "bad network mode"));
         ctx->opt_pinet_mode = value;
         break;
+    case CTRECON_OPT_KERNEL_TIMING: ctx->opt_kernel_timing = value != 0; break;
+    case CTRECON_OPT_TC_FORM:
+        if (value != CTRECON_TC_PARITY_SPLIT && value != CTRECON_TC_SINGLE_PASS)
+            return finish(ctx, make_status(CTRECON_ERR_INVALID_ARGUMENT, "bad tensor-core form"));
+        ctx->opt_tc_form = value;
+        break;
     default: return finish(ctx, make_status(CTRECON_ERR_INVALID_ARGUMENT, "unknown option"));
     }
     return finish(ctx, Status::Ok());
@@ -353,6 +431,8 @@ ctrecon_status ctrecon_get_option(const ctrecon_ctx* ctx, ctrecon_option opt, in
     case CTRECON_OPT_DERIVATIVE: *value = ctx->opt_deriv; break;
     case CTRECON_OPT_BP_WINDOW: *value = ctx->opt_bp_window; break;
     case CTRECON_OPT_PINET_MODE: *value = ctx->opt_pinet_mode; break;
+    case CTRECON_OPT_KERNEL_TIMING: *value = ctx->opt_kernel_timing; break;
+    case CTRECON_OPT_TC_FORM: *value = ctx->opt_tc_form; break;
     default: return CTRECON_ERR_INVALID_ARGUMENT;
     }
     return CTRECON_OK;

@@ -231,7 +231,7 @@ ctrecon_status ctrecon_batch_create(ctrecon_ctx* ctx, int n_scans,
         b->n = n_scans;
         b->svar.assign(n_scans, (ctx->opt_bp_variant >= 0 && ctx->opt_bp_variant <= kMaxBPVariant)
                                     ? ctx->opt_bp_variant
-                                    : kDefaultBPVariant);
+                                    : kDefaultBatchVariant);
         b->fp.assign(fp, fp + n_scans);
         size_t nvox = 0;
         std::vector<double> work(n_scans);
@@ -366,7 +366,7 @@ ctrecon_status ctrecon_batch_tune(ctrecon_batch* b, void* stream, const float* c
         std::memset(out, 0, sizeof *out);
         const int saved_opt = ctx->opt_bp_variant;
         Status st;
-        std::vector<int> best(b->n, kDefaultBPVariant);
+        std::vector<int> best(b->n, kDefaultBatchVariant);
         double best_sum = 0;
         std::vector<double> cand_sum;
         for (int i = 0; st.ok() && i < b->n; ++i) {

@@ -257,12 +257,16 @@ Status launch_bkproj_v2(int variant, cudaStream_t s, BPPlan& plan, const float* 
 Status launch_bkproj_f32(ctrecon_ctx* ctx, cudaStream_t s, BPPlan& plan, const float* d_fproj,
                          const PiRecord* d_pitab, float* d_image) {
     const int variant = bp_variant_for(ctx, plan.g);
-    if (variant >= 100) return launch_bk<float>(s, plan, d_fproj, d_pitab, d_image);
+    if (variant >= 100) {
+        KernelTimer tm(ctx, s, kKBackproject);
+        return launch_bk<float>(s, plan, d_fproj, d_pitab, d_image);
+    }
     if (!ctx->ws_flag.ptr) return make_status(CTRECON_ERR_INTERNAL, "device error word not set up");
     if (variant >= 10)
         return launch_bkproj_v5<float>(variant, s, plan, d_fproj, d_pitab, d_image,
                                        ctx->ws_flag.as<int>(), ctx->ws_rec, ctx->ws_boxmaps,
-                                       ctx->boxmap_key, ctx->opt_bp_window);
+                                       ctx->boxmap_key, ctx->opt_bp_window, ctx);
+    KernelTimer tm(ctx, s, kKBackproject);
     return launch_bkproj_v2<float>(variant, s, plan, d_fproj, d_pitab, d_image,
                                    ctx->ws_flag.as<int>());
 }
@@ -270,12 +274,16 @@ Status launch_bkproj_f32(ctrecon_ctx* ctx, cudaStream_t s, BPPlan& plan, const f
 Status launch_bkproj_f64out(ctrecon_ctx* ctx, cudaStream_t s, BPPlan& plan,
                             const float* d_fproj, const PiRecord* d_pitab, double* d_image) {
     const int variant = bp_variant_for(ctx, plan.g);
-    if (variant >= 100) return launch_bk<double>(s, plan, d_fproj, d_pitab, d_image);
+    if (variant >= 100) {
+        KernelTimer tm(ctx, s, kKBackproject);
+        return launch_bk<double>(s, plan, d_fproj, d_pitab, d_image);
+    }
     if (!ctx->ws_flag.ptr) return make_status(CTRECON_ERR_INTERNAL, "device error word not set up");
     if (variant >= 10)
         return launch_bkproj_v5<double>(variant, s, plan, d_fproj, d_pitab, d_image,
                                         ctx->ws_flag.as<int>(), ctx->ws_rec, ctx->ws_boxmaps,
-                                        ctx->boxmap_key, ctx->opt_bp_window);
+                                        ctx->boxmap_key, ctx->opt_bp_window, ctx);
+    KernelTimer tm(ctx, s, kKBackproject);
     return launch_bkproj_v2<double>(variant, s, plan, d_fproj, d_pitab, d_image,
                                     ctx->ws_flag.as<int>());
 }

@@ -808,7 +808,7 @@ static Status upload_box_maps(cudaStream_t s, DevBuf& maps, BoxMapKey& key, cons
 template <typename OutT>
 Status launch_bkproj_v5(int variant, cudaStream_t s, BPPlan& plan, const float* d_fproj,
                         const PiRecord* d_pitab, OutT* d_image, int* err, DevBuf& recbuf,
-                        DevBuf& maps, BoxMapKey& mkey, int max_views) {
+                        DevBuf& maps, BoxMapKey& mkey, int max_views, ctrecon_ctx* tctx) {
     const BPParams& kp0 = plan.kp;
     const int RW = kp0.YL - 1, RH = kp0.ZL - 1;
     const size_t plane = (size_t)RW * RH * sizeof(float4);
@@ -842,9 +842,13 @@ Status launch_bkproj_v5(int variant, cudaStream_t s, BPPlan& plan, const float* 
     for (int w = 0; w < nwin; ++w) {
         const int a = w0 + w * per, b = std::min(w1, a + per - 1);
         const int nv = b - a + 1;
-        CTR_TRY(launch_cell_records(s, d_fproj, rec, a, nv, kp0.YL, kp0.ZL));
+        {
+            KernelTimer tm(tctx, s, kKCellRecords);
+            CTR_TRY(launch_cell_records(s, d_fproj, rec, a, nv, kp0.YL, kp0.ZL));
+        }
         kp.win0 = a;
         kp.win1 = b;
+        KernelTimer tm(tctx, s, kKBackproject);
         Status st;
         switch (variant) {
         case 11: st = launch_v5<4, 4, 2, OutT>(s, plan, kp, d_fproj, d_pitab, d_image, err, tmaps, a); break;
@@ -856,8 +860,8 @@ Status launch_bkproj_v5(int variant, cudaStream_t s, BPPlan& plan, const float* 
     return Status::Ok();
 }
 
-template Status launch_bkproj_v5<float>(int, cudaStream_t, BPPlan&, const float*, const PiRecord*, float*, int*, DevBuf&, DevBuf&, BoxMapKey&, int);
-template Status launch_bkproj_v5<double>(int, cudaStream_t, BPPlan&, const float*, const PiRecord*, double*, int*, DevBuf&, DevBuf&, BoxMapKey&, int);
+template Status launch_bkproj_v5<float>(int, cudaStream_t, BPPlan&, const float*, const PiRecord*, float*, int*, DevBuf&, DevBuf&, BoxMapKey&, int, ctrecon_ctx*);
+template Status launch_bkproj_v5<double>(int, cudaStream_t, BPPlan&, const float*, const PiRecord*, double*, int*, DevBuf&, DevBuf&, BoxMapKey&, int, ctrecon_ctx*);
 
 template Status launch_bkproj_v2<float>(int, cudaStream_t, BPPlan&, const float*, const PiRecord*, float*, int*);
 template Status launch_bkproj_v2<double>(int, cudaStream_t, BPPlan&, const float*, const PiRecord*, double*, int*);

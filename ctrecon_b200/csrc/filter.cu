@@ -111,14 +111,17 @@ __global__ void k_deriv_rebin(const float* __restrict__ proj, int proj_view0, in
     }
     __syncthreads();
     if (j >= YLp) return;
+    // the tensor-core forms read each kappa row de-interleaved: even columns, then odd ones
+    const size_t jx = mode == CTRECON_HILBERT_FP32 ? (size_t)j
+                                                   : (size_t)((j & 1) * (YLp >> 1) + (j >> 1));
     if (!real) {  // zero padding of the kappa rows (the GEMM form reads K = YLp)
-        for (int a = ry; a < AL; a += RG) store_kappa(X, xv + (size_t)a * YLp + j, plane, 0.f, mode);
+        for (int a = ry; a < AL; a += RG) store_kappa(X, xv + (size_t)a * YLp + jx, plane, 0.f, mode);
         return;
     }
 #pragma unroll 8
     for (int a = ry; a < AL; a += RG) {
         const FwEntry f = fw[(size_t)a * YL + j];
-        store_kappa(X, xv + (size_t)a * YLp + j, plane,
+        store_kappa(X, xv + (size_t)a * YLp + jx, plane,
                     fmaf(f.wa, gf[f.r0 * T + tx], f.wb * gf[f.r1 * T + tx]), mode);
     }
 }
@@ -323,19 +326,24 @@ Status launch_filter(ctrecon_ctx* ctx, cudaStream_t s, FilterPlan& plan, const f
         const int n = std::min(chunk, view_end - c0);
         dim3 g1((YLp + tj - 1) / tj, n);
         const size_t plane = (size_t)n * AL * YLp;
-        k_deriv_rebin<<<g1, b1, smem1, s>>>(d_proj, proj_view0, P, YL, ZL, AL, YLp, c0,
-                                            plan.fw.as<FwEntry>(), plan.cuy.as<float2>(),
-                                            plan.zcv.as<float>(), plan.inv2dl, dres,
-                                            (float)t.DeltaL, X, plane, mode);
-        CTR_CUDA(cudaGetLastError());
+        {
+            KernelTimer tm(ctx, s, kKDerivRebin);
+            k_deriv_rebin<<<g1, b1, smem1, s>>>(d_proj, proj_view0, P, YL, ZL, AL, YLp, c0,
+                                                plan.fw.as<FwEntry>(), plan.cuy.as<float2>(),
+                                                plan.zcv.as<float>(), plan.inv2dl, dres,
+                                                (float)t.DeltaL, X, plane, mode);
+            CTR_CUDA(cudaGetLastError());
+        }
         float* out = d_fproj + (size_t)(c0 - out_view0) * YL * ZL;
         if (mode == CTRECON_HILBERT_FP32) {
+            KernelTimer tm(ctx, s, kKHilbertSimt);
             dim3 g2((YL + kTileI - 1) / kTileI, n);
             k_hilbert_simt<<<g2, nthreads2, smem2, s>>>(static_cast<const float*>(X), AL, ALpad,
                                                         YL, YLp, ZL, plan.h.as<float>(), HOFF,
                                                         plan.bk.as<BkEntry>(), out);
             CTR_CUDA(cudaGetLastError());
         } else {
+            KernelTimer tm(ctx, s, kKHilbertTc);
             CTR_TRY(launch_hilbert_tc(ctx, s, plan, X, n, out, mode));
         }
     }

@@ -356,12 +356,15 @@ inline float tf32_rn(float f) {
 
 }  // namespace
 
-// Toeplitz operand(s) for a plan, built on the host (FP64 taps -> BF16 hi/lo or TF32).
+// Toeplitz operand(s) for a plan, built on the host (FP64 taps -> BF16 hi/lo or TF32), with
+// the columns in the kappa rows' de-interleaved order (the sum is over all j either way).
 static Status ensure_toeplitz(FilterPlan& plan, int mode, DevBuf& T0, DevBuf& T1, int& have_mode) {
     if (have_mode == mode) return Status::Ok();
     const int YL = plan.t.YL, YLp = plan.YLp;
     const size_t n = (size_t)YLp * YLp;
     if (mode == CTRECON_HILBERT_BF16X3) {
+        // columns in the kappa rows' de-interleaved order: input j sits at jd(j)
+        auto jd = [&](int j) { return (size_t)((j & 1) * (YLp / 2) + (j >> 1)); };
         std::vector<uint16_t> hi(n, 0), lo(n, 0);
         for (int i = 0; i < YL; ++i)
             for (int j = 0; j < YL; ++j) {
@@ -369,19 +372,20 @@ static Status ensure_toeplitz(FilterPlan& plan, int mode, DevBuf& T0, DevBuf& T1
                 if (!(m & 1)) continue;
                 float v = (float)plan.t.h[(size_t)(m + YL - 1)];
                 uint16_t h = bf16_bits_rn(v);
-                hi[(size_t)i * YLp + j] = h;
-                lo[(size_t)i * YLp + j] = bf16_bits_rn(v - bf16_to_float(h));
+                hi[(size_t)i * YLp + jd(j)] = h;
+                lo[(size_t)i * YLp + jd(j)] = bf16_bits_rn(v - bf16_to_float(h));
             }
         CTR_TRY(T0.ensure(n * 2, "Toeplitz hi"));
         CTR_TRY(T1.ensure(n * 2, "Toeplitz lo"));
         CTR_TRY(upload_now(T0.ptr, hi.data(), n * 2));
         CTR_TRY(upload_now(T1.ptr, lo.data(), n * 2));
     } else {
+        auto jd = [&](int j) { return (size_t)((j & 1) * (YLp / 2) + (j >> 1)); };
         std::vector<float> t(n, 0.f);
         for (int i = 0; i < YL; ++i)
             for (int j = 0; j < YL; ++j) {
                 int m = i - j;
-                if (m & 1) t[(size_t)i * YLp + j] = tf32_rn((float)plan.t.h[(size_t)(m + YL - 1)]);
+                if (m & 1) t[(size_t)i * YLp + jd(j)] = tf32_rn((float)plan.t.h[(size_t)(m + YL - 1)]);
             }
         CTR_TRY(T0.ensure(n * 4, "Toeplitz tf32"));
         CTR_TRY(upload_now(T0.ptr, t.data(), n * 4));
@@ -396,6 +400,8 @@ int hilbert_tc_views_per_tile(int AL) { return AL > 256 ? 1 : std::max(1, 256 / 
 
 Status launch_hilbert_tc(ctrecon_ctx* ctx, cudaStream_t s, FilterPlan& plan, const void* X,
                          int nviews, float* d_fproj_chunk, int mode) {
+    if (ctx->opt_tc_form == CTRECON_TC_PARITY_SPLIT && hilbert_tc2_fits(plan))
+        return launch_hilbert_tc2(ctx, s, plan, X, nviews, d_fproj_chunk, mode);
     const int AL = plan.t.AL, YL = plan.t.YL, ZL = plan.t.ZL, YLp = plan.YLp;
     if (AL > 512)
         return make_status(CTRECON_ERR_UNSUPPORTED,

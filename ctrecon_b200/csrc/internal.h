@@ -92,12 +92,18 @@ struct alignas(16) DresCol { int yd, yu; float alfa, dzc; };
 struct FilterPlan {
     ctrecon_filter_params p{};
     FilterTables t;
-    int YLp = 0;  // padded row length of the kappa-row buffers (multiple of 64)
+    int YLp = 0;  // padded row length of the kappa-row buffers (multiple of 128)
     DevBuf fw, bk, cuy, zcv, h;
     float inv2dl = 0;
-    // tensor-core Hilbert operands (Toeplitz hi/lo in BF16, or TF32), built on first use
+    // tensor-core Hilbert operands (Toeplitz hi/lo in BF16, or TF32), built on first use: the
+    // full Toeplitz with its columns in the kappa rows' de-interleaved order (single-pass form,
+    // hilbert_tc.cu), and the two parity halves with the backward-rebin table by parity
+    // (parity-split form, hilbert_tc2.cu)
     DevBuf tcT0, tcT1;
     int tc_mode = -1;
+    DevBuf tc2T0, tc2T1, bkp;
+    int tc2_mode = -1;
+    bool bkp_ready = false;
     // DerMode 0 resampling (DresCol per column and side, [column][side]), built on first use
     DevBuf dres;
     bool dres_ready = false;
@@ -160,12 +166,38 @@ std::string tune_key(const BPGeom& g);
 int bp_variant_for(const ctrecon_ctx* ctx, const BPGeom& g);
 extern const int kTuneCandidates[];
 extern const int kNumTuneCandidates;
-constexpr int kDefaultBPVariant = 2;
+// The form used when CTRECON_OPT_BP_VARIANT is CTRECON_BP_AUTO (the default) and the tuning
+// table has no entry for the geometry: the fifth form with blocks of 8 views (the tuner's choice
+// on every benchmark scan). Its cell records are written in view windows sized to the free
+// memory, so it runs at any scan length.
+constexpr int kDefaultBPVariant = 12;
+// A batch's default form: the second form, since a batch holds the cell records of all of its
+// fifth-form scans at once.
+constexpr int kDefaultBatchVariant = 2;
 // Times every candidate form: prepare(v) (untimed, may be empty) then run_one(v) three times,
 // the last two timed with CUDA events on s; candidates that cannot launch are marked -1.
 Status tune_candidates(ctrecon_tune_result* res, cudaStream_t s,
                        const std::function<Status(int)>& prepare,
                        const std::function<Status(int)>& run_one, int max_variant = 1000);
+
+// Per-kernel device timing (CTRECON_OPT_KERNEL_TIMING): a KernelTimer records a pair of CUDA
+// events around the launches of one kernel kind on the launching stream; ctrecon_kernel_times
+// sums the pairs per kind (api.cpp). With the option off (or no context) it does nothing.
+struct KernelSpan {
+    int kind;
+    cudaEvent_t a, b;
+};
+struct KernelTimer {
+    KernelTimer(ctrecon_ctx* ctx, cudaStream_t s, int kind);
+    ~KernelTimer() { stop(); }
+    void stop();
+    KernelTimer(const KernelTimer&) = delete;
+    KernelTimer& operator=(const KernelTimer&) = delete;
+    ctrecon_ctx* ctx;
+    cudaStream_t s;
+    int kind;
+    cudaEvent_t a = nullptr;
+};
 
 // One scan of a batched backprojection (batch.cpp, bkproj2.cu)
 struct BatchScanDev {
@@ -202,11 +234,15 @@ struct ctrecon_ctx {
     int opt_hilbert = CTRECON_HILBERT_FP32;
     int opt_pi = CTRECON_PI_BISECT;
     int opt_filter_chunk = 2048;  // larger chunks fill the GPU better (c2: 512 -> 2048, -4 %)
-    int opt_bp_variant = 2;  // second form, 8 slices x 8 views
+    int opt_bp_variant = CTRECON_BP_AUTO;  // the tuning table's form, else kDefaultBPVariant
     int opt_verbose = 0;
     int opt_deriv = CTRECON_DERIV_CHAIN;
     int opt_bp_window = 0;
     int opt_pinet_mode = CTRECON_PINET_GRID;  // CTRECON_OPT_PINET_MODE
+    int opt_kernel_timing = 0;                // CTRECON_OPT_KERNEL_TIMING
+    int opt_tc_form = CTRECON_TC_PARITY_SPLIT;  // CTRECON_OPT_TC_FORM
+    std::vector<ctr::KernelSpan> kspans;      // timed launches since the last query
+    std::vector<cudaEvent_t> kev_free;        // timing events for reuse
     cudaStream_t host_stream = nullptr;  // stream for the synchronous host calls
     cudaStream_t up_stream = nullptr;    // host -> device copies of the host calls
     cudaStream_t down_stream = nullptr;  // device -> host copies of the host calls
@@ -243,6 +279,13 @@ Status build_bp_plan(const BPGeom& g, BPPlan& plan);
 Status reset_device_flag(ctrecon_ctx* ctx, cudaStream_t s);
 
 // kernel launchers (filter.cu, pi.cu, bkproj.cu, phantom.cu)
+// tensor-core Hilbert (hilbert_tc.cu: single pass; hilbert_tc2.cu: parity split, persistent).
+// In the tensor-core modes the kappa rows are stored de-interleaved: column j of a row at
+// (j & 1) * YLp / 2 + (j >> 1).
+int hilbert_tc_views_per_tile(int AL);
+bool hilbert_tc2_fits(const FilterPlan& plan);
+Status launch_hilbert_tc2(ctrecon_ctx* ctx, cudaStream_t s, FilterPlan& plan, const void* X,
+                          int nviews, float* d_fproj_chunk, int mode);
 Status launch_filter(ctrecon_ctx* ctx, cudaStream_t s, FilterPlan& plan, const float* d_proj,
                      int proj_view0, int proj_nviews, float* d_fproj, int out_view0,
                      int view_begin, int view_end);
@@ -274,7 +317,18 @@ Status launch_cell_records(cudaStream_t s, const float* d_fproj, void* rec, int 
 template <typename OutT>
 Status launch_bkproj_v5(int variant, cudaStream_t s, BPPlan& plan, const float* d_fproj,
                         const PiRecord* d_pitab, OutT* d_image, int* err, DevBuf& recbuf,
-                        DevBuf& maps, BoxMapKey& mkey, int max_views);
+                        DevBuf& maps, BoxMapKey& mkey, int max_views,
+                        ctrecon_ctx* tctx = nullptr);
+// kinds of KernelTimer (the index into ctrecon_kernel_times' arrays)
+enum KernelKind {
+    kKDerivRebin = 0,   // K1 k_deriv_rebin
+    kKHilbertSimt = 1,  // K2 k_hilbert_simt (FP32)
+    kKHilbertTc = 2,    // K2 k_hilbert_tc (tensor cores)
+    kKPiSolve = 3,      // K3 PI solve (with the learned start's network)
+    kKCellRecords = 4,  // k_cell_records of the fifth form
+    kKBackproject = 5,  // K4, any form
+    kNumKernelKinds = 6
+};
 Status launch_convert_f32_to_f64(cudaStream_t s, const float* in, double* out, size_t n);
 Status launch_average_into(cudaStream_t s, float* a, const float* b, size_t n);
 Status launch_phantom(cudaStream_t s, const BPGeom& g, const double* d_ell, int n_ell,

@@ -130,6 +130,7 @@ Status launch_pi_guess(ctrecon_ctx* ctx, cudaStream_t s, BPPlan& plan, PiRecord*
 
 Status launch_pi_stats(ctrecon_ctx* ctx, cudaStream_t s, BPPlan& plan, PiRecord* d_pitab,
                        unsigned long long* d_updates, unsigned long long* d_iters) {
+    KernelTimer tm(ctx, s, kKPiSolve);
     if (ctx->opt_pi == CTRECON_PI_LEARNED)
         return launch_pi_learned(ctx, s, plan, d_pitab, d_updates, d_iters);
     return launch_solve(s, plan, ctx->opt_pi, nullptr, d_pitab, d_updates, d_iters);

@@ -178,6 +178,12 @@ def config(name: str) -> HelicalScan:
     if name == "c3":
         return HelicalScan("c3", 600.0, 1200.0, 1024, 128, 0.8, 0.8, 2304, 6, 0.9,
                            512, 512, 512, voxel=None, n_ellipsoids=40, seed=1003)
+    if name == "c3s":
+        # a slab of c3 for profiling captures: same detector, pitch and voxels, 1.25 turns,
+        # 32 slices (FP32 projections 1.5 GB, above L2)
+        return HelicalScan("c3s", 600.0, 1200.0, 1024, 128, 0.8, 0.8, 2304, 1.25, 0.9,
+                           512, 512, 32, voxel=(0.46875, 0.46875, 0.46875), n_ellipsoids=40,
+                           seed=1013)
     if name == "c5":
         return HelicalScan("c5", 600.0, 1200.0, 1536, 256, 0.5, 0.5, 2000, 10, 0.9,
                            1024, 1024, 1024, voxel=None, n_ellipsoids=40, seed=1005)

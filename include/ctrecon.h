@@ -117,7 +117,8 @@ typedef enum ctrecon_option {
     CTRECON_OPT_HILBERT = 1,          /* CTRECON_HILBERT_*; default FP32 */
     CTRECON_OPT_PI_SOLVER = 2,        /* CTRECON_PI_*; default BISECT */
     CTRECON_OPT_FILTER_CHUNK = 3,     /* views per filter work chunk; default 2048 */
-    CTRECON_OPT_BP_VARIANT = 4,       /* backprojector variant, default 2: 0, 1 = per-cell
+    CTRECON_OPT_BP_VARIANT = 4,       /* backprojector variant, default CTRECON_BP_AUTO (the
+                                         tuning table's form for the geometry, else 12): 0, 1 = per-cell
                                          records, blocks of 4 / 8 views; 2, 3, 4 = second
                                          form (slices x views) 8x8, 4x8, 8x4; 5, 6, 7 = per-cell
                                          records staged by producer warps (views per block x
@@ -133,9 +134,23 @@ typedef enum ctrecon_option {
     CTRECON_OPT_BP_WINDOW = 7,        /* views per cell-record window of variants 10..12;
                                          0 (default) = as many as 32 GiB of records hold,
                                          and at most half of the free device memory */
-    CTRECON_OPT_PINET_MODE = 8        /* how the learned PI solve evaluates the network:
+    CTRECON_OPT_PINET_MODE = 8,       /* how the learned PI solve evaluates the network:
                                          CTRECON_PINET_* below */
+    CTRECON_OPT_KERNEL_TIMING = 9,    /* 1: time every kernel launch of the single-scan entry
+                                         points with CUDA events on its stream (read with
+                                         ctrecon_kernel_times); default 0 */
+    CTRECON_OPT_TC_FORM = 10          /* form of the tensor-core Hilbert: CTRECON_TC_* below */
 } ctrecon_option;
+
+/* CTRECON_OPT_TC_FORM. Both forms compute the same sums to FP32 rounding. */
+enum {
+    CTRECON_TC_PARITY_SPLIT = 0, /* default: odd and even output columns as two half-size
+                                    Toeplitz products (the taps vanish at even lags), one
+                                    persistent CTA per SM overlapping each tile's backward rebin
+                                    with the next tile's MMAs; views of up to 256 kappa rows */
+    CTRECON_TC_SINGLE_PASS = 1   /* one full-size product per tile, then its backward rebin; also
+                                    the form used for views of more than 256 kappa rows */
+};
 
 /* ---- context ---------------------------------------------------------------------- */
 ctrecon_status ctrecon_ctx_create(int device, ctrecon_ctx** out);
@@ -221,6 +236,17 @@ ctrecon_status ctrecon_bkproj_dev_f32(ctrecon_ctx* ctx, void* stream,
 ctrecon_status ctrecon_filter_noalloc_dev_f32(void* stream, const ctrecon_filter_params* p,
                                               const float* d_proj, float* d_fproj);
 
+/* Device time per kernel kind of the launches made since the last call while
+ * CTRECON_OPT_KERNEL_TIMING was on, in milliseconds, with the launch counts; the kinds are
+ * 0 derivative + forward rebin (k_deriv_rebin), 1 FP32 Hilbert + backward rebin
+ * (k_hilbert_simt), 2 tensor-core Hilbert + backward rebin (k_hilbert_tc), 3 PI-line solve
+ * (with the learned start's network), 4 cell records of the fifth backprojector form,
+ * 5 backprojection (any form). Arrays of n entries; waits for the timed work. No counterpart in
+ * the reference (a profiling aid). */
+#define CTRECON_KERNEL_KINDS 6
+ctrecon_status ctrecon_kernel_times(ctrecon_ctx* ctx, double* ms, unsigned long long* launches,
+                                    int n);
+
 /* Waits for the work enqueued on `stream` and reports device-side failures: a CUDA error,
  * or CTRECON_ERR_TIMEOUT when a bounded wait inside a kernel gave up. */
 ctrecon_status ctrecon_sync(ctrecon_ctx* ctx, void* stream);
@@ -246,7 +272,8 @@ ctrecon_status ctrecon_batch_create(ctrecon_ctx* ctx, int n_scans,
                                     const ctrecon_bp_geom* geoms, ctrecon_batch** out);
 void ctrecon_batch_destroy(ctrecon_batch* batch);
 /* backprojector form of every scan of the batch: 0 .. 12 as CTRECON_OPT_BP_VARIANT (default:
- * the context's); scans that share a form share one persistent launch. The fifth form
+ * the context's when it names a form 0 .. 12, else 2); scans that share a form share one
+ * persistent launch. The fifth form
  * (10 .. 12) holds the cell records of all its scans at once (16 bytes per detector cell and
  * view) and writes them right before the launch. */
 ctrecon_status ctrecon_batch_set_variant(ctrecon_batch* batch, int variant);

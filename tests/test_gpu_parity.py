@@ -118,6 +118,38 @@ def test_filter_tensor_core_two_halves(torch_mod, oracle_mod, zl, yl, mode, boun
     assert err < bound
 
 
+@pytest.mark.parametrize("mode,bound", [("bf16x3", 5e-5), ("tf32", 5e-3)])
+@pytest.mark.parametrize("yl,zl,chunk", [(300, 16, 2048), (130, 40, 7), (736, 64, 100)])
+def test_filter_tensor_core_forms_agree(torch_mod, oracle_mod, yl, zl, chunk, mode, bound):
+    """The parity-split persistent form (default) and the single-pass form of the tensor-core
+    Hilbert, each against the FP64 oracle and against each other, on ragged shapes: 300 columns
+    (each parity's 192 outputs padded to two 128-row blocks), 130 columns with 53 kappa rows per
+    view (four views per tile) in chunks of 7 views (partial view groups), and the c2 detector
+    in chunks of 100 views."""
+    import ctrecon_b200 as ct
+    from ctrecon_b200 import _lib
+    from ctrecon_b200.geometry import small_config
+    s = small_config(name="ragged", YL=yl, ZL=zl, views_per_turn=90, turns=1.3, NX=24, NY=24,
+                     NZ=8)
+    O = oracle_mod
+    proj = O.project_ellipsoids(oracle_geom(O, s), s.ellipsoids())
+    ref = O.katsevich_filter(oracle_filter_params(O, s), proj)
+    m = ct.HILBERT_BF16X3 if mode == "bf16x3" else ct.HILBERT_TF32
+    out = {}
+    for form in (_lib.TC_PARITY_SPLIT, _lib.TC_SINGLE_PASS):
+        with ct.Context(0, hilbert=m) as cx:
+            cx.set_option(_lib.OPT_TC_FORM, form)
+            cx.set_option(_lib.OPT_FILTER_CHUNK, chunk)
+            out[form] = cx.filter_host(ct.scan_filter_params(s), proj)
+        err = rel_rmse(out[form], ref)
+        print(f"filter {zl}x{yl} {mode} form {form}: rel RMSE {err:.3e}")
+        assert err < bound
+        assert np.all(np.isfinite(out[form]))
+    d = rel_rmse(out[_lib.TC_PARITY_SPLIT], out[_lib.TC_SINGLE_PASS])
+    print(f"  forms differ by {d:.2e}")
+    assert d < bound
+
+
 def test_chain_c1_bf16x3_matches_oracle(torch_mod, c1_case):
     import ctrecon_b200 as ct
     s = c1_case["s"]
