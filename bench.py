@@ -608,53 +608,60 @@ def run_report_extras(args):
 
 
 def _refgpu_guard(s, AL, n_vox):
-    """Sizes the reference GPU MEX files handle, found by reading them: int32 element indices
-    (KatsevichFiltering_GPU.cu:294 (pIdx*AL + AIndex)*YL, :71, :820), a 3-D texture of depth
-    ProjNum (KatsevichBkProj_GPU.cu:262, at most 16384), the Hilbert batches of 1024 views
-    (:685: fewer views make its batch loop run past the data), and coordinate vectors sized
-    ProjNum that receive RecMX/RecMY/RecMZ entries (KatsevichBkProj_GPU.cu:300-309)."""
+    """(filter, backprojection) reasons the reference GPU MEX files cannot run scan s (None when
+    they can), found by reading them. Filter: int32 element indices
+    (KatsevichFiltering_GPU.cu:294 (pIdx*AL + AIndex)*YL, :71, :820); the complex buffer of a
+    Hilbert batch, YL*nn2*ProjNumber elements computed in int (:637, batches of 1024 views, the
+    last of up to 2047); at least one batch of 1024 views (:685: fewer make its batch loop run
+    past the data). Backprojection: a 3-D texture of depth ProjNum (KatsevichBkProj_GPU.cu:262,
+    at most 16384) and coordinate vectors sized ProjNum that receive RecMX/RecMY/RecMZ entries
+    (KatsevichBkProj_GPU.cu:300-309)."""
     P = s.P
     lim = 2 ** 31 - 1
-    if P * AL * s.YL > lim or P * s.ZL * s.YL > lim:
-        return "element indices exceed int32 in the reference GPU filter"
+    nn2 = 2 * 2 ** (int(np.ceil(np.log2(s.YL))) + 1)
+    last = P - (P // 1024 - 1) * 1024 if P >= 1024 else P
+    f = None
     if P < 1024:
-        return "fewer than 1024 views: the reference's Hilbert batching needs at least one batch"
+        f = "fewer than 1024 views: the reference's Hilbert batching needs one whole batch"
+    elif P * AL * s.YL > lim or P * s.ZL * s.YL > lim:
+        f = "element indices exceed int32 in the reference GPU filter"
+    elif s.YL * nn2 * last > lim:
+        f = (f"its Hilbert buffer of YL*nn2*views = {s.YL}*{nn2}*{last} elements overflows the "
+             f"int it is sized with (KatsevichFiltering_GPU.cu:637)")
+    b = None
     if P > 16384:
-        return "more than 16384 views: beyond a 3-D texture's depth"
-    if max(n_vox) > P:
-        return "a volume side larger than the view count overruns the reference's vectors"
-    return None
+        b = "more than 16384 views: beyond a 3-D texture's depth"
+    elif max(n_vox) > P:
+        b = "a volume side larger than the view count overruns the reference's vectors"
+    elif int(np.prod(n_vox)) > lim:
+        b = "image indices exceed int32"
+    return f, b
 
 
 def run_report_refgpu(args):
     """The reference's own GPU MEX functions (KatsevichFiltering_GPU.cu, KatsevichBkProj_GPU.cu)
-    recompiled for sm_100a against the mex.h shim (baseline/Makefile), on the c2 scan: their
-    time through the MEX interface (FP64 host arrays, synchronous, as MATLAB calls them), the
-    device time of their kernels (CUDA events on the legacy stream they use), and their error
-    against the FP64 oracle on a central block -- beside this library's MEX modules on the same
-    arrays. Not a parity target: the reference GPU path has no endpoint weights, FP32 cuFFT and
-    9-bit texture interpolation weights."""
+    recompiled for sm_100a against the mex.h shim (baseline/Makefile), beside this library's MEX
+    modules on the same FP64 host arrays (synchronous calls, as MATLAB makes them): their time
+    through the MEX interface, the device span of their work (CUDA events on the legacy stream
+    they use), and their error against the FP64 oracle on a central block. The reference GPU
+    filter runs where its int-sized buffers allow (c1; at c2 and above its Hilbert buffer size
+    overflows), its backprojector on c1 and c2. Not a parity target: the reference GPU path has
+    no endpoint weights, FP32 cuFFT and 9-bit texture interpolation weights."""
     import torch
     import ctrecon_b200 as ct
     from ctrecon_b200.mexharness import MexModule
-    s = config(args.config if args.config not in ("c3",) else "c2")
-    AL = 2 * int(np.ceil(s.ZL * 1.3 * 0.5)) + 1
     refdir = os.path.join(ROOT, "baseline", "_ref")
     fpath = os.path.join(refdir, "KatsevichFiltering_GPU_ref.so")
     bpath = os.path.join(refdir, "KatsevichBkProj_GPU_ref.so")
-    why = _refgpu_guard(s, AL, s.vol_shape)
-    if why is None and not (os.path.exists(fpath) and os.path.exists(bpath)):
-        why = "baseline/_ref (the reference GPU MEX files built by baseline/Makefile) is missing"
-    if why:
-        print(json.dumps({"report": "refgpu", "unavailable": why, "workload": workload_name(s)}))
+    if not (os.path.exists(fpath) and os.path.exists(bpath)):
+        print(json.dumps({"report": "refgpu", "unavailable": "baseline/_ref (the reference GPU "
+                          "MEX files built by baseline/Makefile) is missing"}))
         return
     O = _oracle()
-    ctx = ct.Context(0)
-    geom = s.geom_struct()
-    d_proj = torch.empty(s.proj_shape, dtype=torch.float32, device="cuda")
-    ctx.phantom_dev(geom, s.ellipsoids(), d_proj, photons=s.photons or 0.0, seed=s.seed)
-    proj64 = d_proj.cpu().numpy().astype(np.float64)   # pageable, as MATLAB's arrays
-    fargs = list(s.filter_args())
+    names = [args.config] if args.config not in ("c3",) else ["c1", "c2"]
+    result = {"report": "refgpu",
+              "arrays": "FP64 pageable host arrays through the MEX interface (mex.h shim)",
+              "scans": {}}
     leg = torch.cuda.default_stream()  # the legacy stream the reference's thrust and kernels use
 
     def timed(fn, reps=2):
@@ -670,89 +677,88 @@ def run_report_refgpu(args):
             torch.cuda.synchronize()
             walls.append(time.perf_counter() - t0)
             devs.append(e0.elapsed_time(e1) / 1e3)
-        return min(walls), min(devs)
-
-    out = {"report": "refgpu", "workload": workload_name(s), "updates": None,
-           "arrays": "FP64 pageable host arrays through the MEX interface (mex.h shim)"}
-    ref_f = MexModule(fpath)
-    ref_b = MexModule(bpath)
-    ours_f = MexModule(os.path.join(ROOT, "ctrecon_b200", "lib", "mex", "KatsevichFiltering_GPU.so"))
-    ours_b = MexModule(os.path.join(ROOT, "ctrecon_b200", "lib", "mex", "KatsevichBkProj_GPU.so"))
-    for m in (ref_f, ref_b, ours_f, ours_b):
-        m.set_print(False)
-    f_ref = np.empty_like(proj64)
-    f_ours = np.empty_like(proj64)
-    w, d = timed(lambda: ref_f.call([proj64] + fargs + [f_ref]))
-    out["filter_reference_gpu"] = {"wall_s": w, "device_span_s": d}
-    w, d = timed(lambda: ours_f.call([proj64] + fargs + [f_ours]))
-    out["filter_ours_mex"] = {"wall_s": w, "device_span_s": d}
-    img_ref = np.zeros(s.vol_shape)
-    img_ours = np.zeros(s.vol_shape)
-    w, d = timed(lambda: ref_b.call([geom, f_ref, img_ref]))
-    out["bkproj_reference_gpu"] = {"wall_s": w, "device_span_s": d}
-    w, d = timed(lambda: ours_b.call([geom, f_ours, img_ours]))
-    out["bkproj_ours_mex"] = {"wall_s": w, "device_span_s": d}
-    # device-resident kernels of this library on the same scan, for the kernel-only comparison
-    fpar = ct.scan_filter_params(s)
-    d_f = torch.empty_like(d_proj)
-    d_img = torch.zeros(s.vol_shape, dtype=torch.float32, device="cuda")
-    d_tab = torch.empty(ctx.pi_table_bytes(geom), dtype=torch.uint8, device="cuda")
-    d_cnt = torch.zeros(1, dtype=torch.int64, device="cuda")
-    ctx.pi_dev(geom, d_tab, d_cnt)
-    torch.cuda.synchronize()
-    updates = int(d_cnt.item())
-    out["updates"] = updates
-    cur = torch.cuda.current_stream()
-
-    def dev_ms(fn):
-        fn()
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(cur)
-        fn()
-        e1.record(cur)
-        torch.cuda.synchronize()
-        return e0.elapsed_time(e1) / 1e3
-
-    out["filter_ours_device_s"] = dev_ms(lambda: ctx.filter_dev(fpar, d_proj, d_f))
-    out["pi_bkproj_ours_device_s"] = dev_ms(lambda: (ctx.pi_dev(geom, d_tab),
-                                                     ctx.bkproj_dev(geom, d_f, d_img,
-                                                                    d_pitab=d_tab)))
-    # accuracy on the central block: the reference GPU filter's views and its backprojection
-    # (of the oracle's filtered views) against the FP64 oracle
-    n = 48
-    locus, det, obj, lo, hi = block_problem(O, s, n)
-    a0, a1 = max(0, lo - 1), min(s.P, hi + 1)
-    orc_f = np.ascontiguousarray(cpu_filter_views(O, s, proj64[a0:a1])[lo - a0:hi - a0])
-    gb = O.bp_geom(locus, det, obj, honour_extras=True)
-    orc_img, _, touched = O.bkproj(gb, orc_f, np.zeros((n, n, n)), want_touched=True)
-    t = touched.astype(bool)
+        return {"wall_s": min(walls), "device_span_s": min(devs)}
 
     def err(x, r, m=None):
         x, r = (x[m], r[m]) if m is not None else (x, r)
         return {"rel_rmse": float(np.linalg.norm(x - r) / np.linalg.norm(r)),
                 "max_abs": float(np.abs(x - r).max())}
 
-    block = {"Locus": np.array(locus), "Detector": np.array(det), "Object": np.array(obj)}
-    bimg_ref = np.zeros((n, n, n))
-    ref_b.call([block, orc_f, bimg_ref])
-    bimg_ours = np.zeros((n, n, n))
-    ours_b.call([block, orc_f, bimg_ours])
-    out["accuracy_vs_fp64_oracle"] = {
-        "filter_reference_gpu": err(f_ref[lo:hi], orc_f),
-        "filter_ours": err(f_ours[lo:hi], orc_f),
-        "bkproj_reference_gpu": err(bimg_ref, orc_img, t),
-        "bkproj_ours": err(bimg_ours, orc_img, t),
-        "block": {"voxels": n ** 3, "written": int(t.sum()), "views": [lo, hi]}}
-    fr, fo = out["filter_reference_gpu"], out["filter_ours_mex"]
-    br, bo = out["bkproj_reference_gpu"], out["bkproj_ours_mex"]
-    out["speedup_mex"] = {"filter": fr["wall_s"] / fo["wall_s"],
-                          "bkproj": br["wall_s"] / bo["wall_s"],
-                          "chain": (fr["wall_s"] + br["wall_s"]) / (fo["wall_s"] + bo["wall_s"])}
-    out["gups_mex"] = {"reference_gpu": updates / (fr["wall_s"] + br["wall_s"]) / 1e9,
-                       "ours": updates / (fo["wall_s"] + bo["wall_s"]) / 1e9}
-    print(json.dumps(out))
-    ctx.close()
+    ref_f, ref_b = MexModule(fpath), MexModule(bpath)
+    ours_f = MexModule(os.path.join(ROOT, "ctrecon_b200", "lib", "mex", "KatsevichFiltering_GPU.so"))
+    ours_b = MexModule(os.path.join(ROOT, "ctrecon_b200", "lib", "mex", "KatsevichBkProj_GPU.so"))
+    for m in (ref_f, ref_b, ours_f, ours_b):
+        m.set_print(False)
+    for name in names:
+        s = config(name)
+        AL = 2 * int(np.ceil(s.ZL * 1.3 * 0.5)) + 1
+        why_f, why_b = _refgpu_guard(s, AL, s.vol_shape)
+        out = {"workload": workload_name(s)}
+        ctx = ct.Context(0)
+        geom = s.geom_struct()
+        d_proj = torch.empty(s.proj_shape, dtype=torch.float32, device="cuda")
+        ctx.phantom_dev(geom, s.ellipsoids(), d_proj, photons=s.photons or 0.0, seed=s.seed)
+        d_tab = torch.empty(ctx.pi_table_bytes(geom), dtype=torch.uint8, device="cuda")
+        d_cnt = torch.zeros(1, dtype=torch.int64, device="cuda")
+        ctx.pi_dev(geom, d_tab, d_cnt)
+        torch.cuda.synchronize()
+        updates = int(d_cnt.item())
+        out["updates"] = updates
+        proj64 = d_proj.cpu().numpy().astype(np.float64)   # pageable, as MATLAB's arrays
+        del d_proj, d_tab
+        ctx.close()
+        torch.cuda.empty_cache()
+        fargs = list(s.filter_args())
+        f_ours = np.empty_like(proj64)
+        out["filter_ours_mex"] = timed(lambda: ours_f.call([proj64] + fargs + [f_ours]))
+        if why_f is None:
+            f_ref = np.empty_like(proj64)
+            out["filter_reference_gpu"] = timed(lambda: ref_f.call([proj64] + fargs + [f_ref]))
+        else:
+            out["filter_reference_gpu"] = {"unavailable": why_f}
+        img_ours = np.zeros(s.vol_shape)
+        out["bkproj_ours_mex"] = timed(lambda: ours_b.call([geom, f_ours, img_ours]))
+        if why_b is None:
+            img_ref = np.zeros(s.vol_shape)
+            out["bkproj_reference_gpu"] = timed(lambda: ref_b.call([geom, f_ours, img_ref]))
+        else:
+            out["bkproj_reference_gpu"] = {"unavailable": why_b}
+        # accuracy on the central block: the reference GPU filter's views and its
+        # backprojection (of the oracle's filtered views) against the FP64 oracle
+        n = 48
+        locus, det, obj, lo, hi = block_problem(O, s, n)
+        a0, a1 = max(0, lo - 1), min(s.P, hi + 1)
+        orc_f = np.ascontiguousarray(cpu_filter_views(O, s, proj64[a0:a1])[lo - a0:hi - a0])
+        gb = O.bp_geom(locus, det, obj, honour_extras=True)
+        orc_img, _, touched = O.bkproj(gb, orc_f, np.zeros((n, n, n)), want_touched=True)
+        t = touched.astype(bool)
+        block = {"Locus": np.array(locus), "Detector": np.array(det), "Object": np.array(obj)}
+        acc = {"block": {"voxels": n ** 3, "written": int(t.sum()), "views": [lo, hi]},
+               "filter_ours": err(f_ours[lo:hi], orc_f)}
+        bimg_ours = np.zeros((n, n, n))
+        ours_b.call([block, orc_f, bimg_ours])
+        acc["bkproj_ours"] = err(bimg_ours, orc_img, t)
+        if why_f is None:
+            acc["filter_reference_gpu"] = err(f_ref[lo:hi], orc_f)
+        if why_b is None:
+            bimg_ref = np.zeros((n, n, n))
+            ref_b.call([block, orc_f, bimg_ref])
+            acc["bkproj_reference_gpu"] = err(bimg_ref, orc_img, t)
+        out["accuracy_vs_fp64_oracle"] = acc
+        sp = {}
+        if why_f is None:
+            sp["filter"] = out["filter_reference_gpu"]["wall_s"] / out["filter_ours_mex"]["wall_s"]
+        if why_b is None:
+            sp["bkproj"] = out["bkproj_reference_gpu"]["wall_s"] / out["bkproj_ours_mex"]["wall_s"]
+        if why_f is None and why_b is None:
+            rt = out["filter_reference_gpu"]["wall_s"] + out["bkproj_reference_gpu"]["wall_s"]
+            ot = out["filter_ours_mex"]["wall_s"] + out["bkproj_ours_mex"]["wall_s"]
+            sp["chain"] = rt / ot
+            out["gups_mex"] = {"reference_gpu": updates / rt / 1e9, "ours": updates / ot / 1e9}
+        out["speedup_mex"] = sp
+        result["scans"][name] = out
+        del proj64, f_ours, img_ours
+    print(json.dumps(result))
 
 
 def _train_pinet(ctx, s, out, stream, torch):
@@ -956,8 +962,9 @@ def kernel_rooflines(s, kt, steps, updates, peaks, sm_mhz, hil):
     """Per-kernel time and roofline fraction from the CUDA-event kernel times `kt` ({kind:
     (ms, launches)}) of `steps` steps. Algorithmic work per view / per update:
       K1 deriv_rebin   HBM: 4*YL*ZL bytes read + 4*AL*YLp written (FP32, or BF16 hi + lo)
-      K2 hilbert_tc    tensor: 2*YL^2*AL flop per view (the dense Toeplitz product); the BF16x3
-                       split executes 3 products of YLp^2, reported as `executed`
+      K2 hilbert_tc    tensor: 2*YL^2*AL flop per view (the dense Toeplitz product); the kernel
+                       executes two half-size products per view group (odd lags only, padded
+                       rows and kappa rows), three of them for BF16x3: `executed`
       K2 hilbert_simt  FP32 FMA pipe: AL*YL*YL/2 FMA per view (odd lags only) at
                        128 FMA/SM/clock
       cell_records     HBM: 4 bytes read + 16 written per detector cell and view
@@ -965,7 +972,7 @@ def kernel_rooflines(s, kt, steps, updates, peaks, sm_mhz, hil):
                        over 148 SMs x 4 schedulers x the SM clock."""
     YL, ZL, P = s.YL, s.ZL, s.P
     AL = 2 * int(np.ceil(ZL * 1.3 * 0.5)) + 1
-    YLp = (YL + 63) // 64 * 64
+    YLp = (YL + 127) // 128 * 128
     clk = (sm_mhz or 1965.0) * 1e6
     out = {}
     for kind, (ms, n) in kt.items():
@@ -979,7 +986,16 @@ def kernel_rooflines(s, kt, steps, updates, peaks, sm_mhz, hil):
                      frac=b / t / 1e9 / peaks["hbm_gbs"], algorithmic_bytes=b)
         elif kind == "hilbert_tc":
             f = 2.0 * YL * YL * AL * P
-            ex = (3 if hil == "bf16x3" else 1) * 2.0 * YLp * YLp * AL * P
+            # the parity-split form: two products of (YLp/2 rows padded to 128) x YLp/2 per
+            # parity on each view group's kappa rows padded to 16
+            vpt = max(1, 256 // AL)
+            ntile = (vpt * AL + 15) // 16 * 16
+            YLh = YLp // 2
+            YLhA = (YLh + 127) // 128 * 128
+            ex = ((3 if hil == "bf16x3" else 1) * 2.0 * (2 * YLhA) * YLh * ntile *
+                  np.ceil(P / vpt))
+            if AL > 256:  # the single-pass form: one full product per view
+                ex = (3 if hil == "bf16x3" else 1) * 2.0 * YLp * YLp * AL * P
             pk = peaks["bf16_tflops"] * (1 if hil == "bf16x3" else 0.5)
             r.update(bound="tensor", achieved_tflops=f / t / 1e12, peak_tflops=pk,
                      frac=f / t / 1e12 / pk, executed_tflops=ex / t / 1e12,

@@ -102,10 +102,8 @@ Status build_filter_plan(const ctrecon_filter_params& p, FilterPlan& plan) {
     for (int j = 0; j < t.YL; ++j) cuy[j] = make_float2((float)t.cu[j], (float)t.y[j]);
     std::vector<float> zcv(t.ZL);
     for (int k = 0; k < t.ZL; ++k) zcv[k] = (float)(t.z[k] * t.cv);
-    const int HOFF = plan.YLp + 64;
-    std::vector<float> hpad(2 * (size_t)HOFF, 0.f);
-    for (int m = -(t.YL - 1); m <= t.YL - 1; ++m)
-        if (m & 1) hpad[(size_t)(HOFF + m)] = (float)t.h[(size_t)(m + t.YL - 1)];
+    std::vector<float> hpad;
+    build_simt_taps(t, plan.YLp, hpad);
     CTR_TRY(upload(plan.fw, fw, "forward-rebin table"));
     CTR_TRY(upload(plan.bk, bk, "backward-rebin table"));
     CTR_TRY(upload(plan.cuy, cuy, "derivative coefficients"));

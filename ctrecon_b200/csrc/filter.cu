@@ -45,155 +45,229 @@ __device__ __forceinline__ void store_kappa(void* X, size_t idx, size_t plane, f
     }
 }
 
-// Block (T columns) x (RG row groups): thread (tx, ry) owns column j = blockIdx.x * T + tx and
-// computes the derivative rows k = ry, ry + RG, ... then the kappa rows a = ry, ry + RG, ...;
-// the RG groups keep RG independent row walks in flight per column.
+// Block (T = 32 columns) x (RG row groups); it walks views vbeg + blockIdx.y * VB .. + VB - 1 of
+// the chunk (at most vend): the forward-rebin entries of its columns are loaded into shared
+// memory once and serve all VB views (otherwise the 16-byte entries, read for every kappa
+// sample of every view, are the largest stream the kernel moves). Per view, thread (tx, ry)
+// computes the derivative rows k = ry, ry + RG, ... of column j = blockIdx.x * T + tx into
+// shared memory, then the kappa rows a = ry, ry + RG, ...; the RG groups keep RG independent
+// row walks in flight per column.
 // dres != NULL selects the direct half-view derivative of KatsevichFiltering_T.m:50-101
 // (entries [column][side], side 0 applied to the next view, side 1 to this one; dl = DeltaL):
 // the resampled row position (k + 1 - HalfZ) * Dzc + HalfZ is formed here in FP32, the column
 // position comes from the FP64 host table; indices clamped as CheckData.m.
-__global__ void k_deriv_rebin(const float* __restrict__ proj, int proj_view0, int P, int YL,
-                              int ZL, int AL, int YLp, int vbeg,
-                              const FwEntry* __restrict__ fw, const float2* __restrict__ cuy,
-                              const float* __restrict__ zcv, float inv2dl,
-                              const DresCol* __restrict__ dres, float dl,
-                              void* __restrict__ X, size_t plane, int mode) {
-    extern __shared__ float gf[];  // ZL x blockDim.x: the derivative of the block's columns
-    const int T = blockDim.x, tx = threadIdx.x, ry = threadIdx.y, RG = blockDim.y;
-    const int j = blockIdx.x * T + tx;
-    const int p = vbeg + blockIdx.y;
-    const size_t xv = (size_t)blockIdx.y * AL * YLp;
+constexpr int kK1Cols = 32;
+constexpr int kK1Views = 16;
+__global__ void __launch_bounds__(kK1Cols * kRowGroups * 2)
+k_deriv_rebin(const float* __restrict__ proj, int proj_view0, int P, int YL, int ZL, int AL,
+              int YLp, int vbeg, int vend, const FwEntry* __restrict__ fw,
+              const float2* __restrict__ cuy, const float* __restrict__ zcv, float inv2dl,
+              const DresCol* __restrict__ dres, float dl, void* __restrict__ X, size_t plane,
+              int mode) {
+    extern __shared__ __align__(16) unsigned char k1_smem[];
+    constexpr int T = kK1Cols;
+    const int tx = threadIdx.x, ry = threadIdx.y, RG = blockDim.y;
+    FwEntry* fws = reinterpret_cast<FwEntry*>(k1_smem);                   // AL x T
+    float* gf = reinterpret_cast<float*>(k1_smem + (size_t)AL * T * sizeof(FwEntry));  // ZL x T
+    const int j = blockIdx.x * T + tx;  // < YLp: the grid covers YLp, a multiple of T
     const bool real = j < YL;
-    if (real && dres) {
-        const size_t S = (size_t)YL * ZL;
-        const int pc = p > P - 2 ? P - 2 : p;  // the last view repeats its neighbour (:101)
-        const float* Pn = proj + (size_t)(pc + 1 - proj_view0) * S;
-        const float* Pc = proj + (size_t)(pc - proj_view0) * S;
-        const DresCol c1 = dres[(size_t)j * 2], c2 = dres[(size_t)j * 2 + 1];
-        const float hz = 0.5f * (float)(ZL + 1);
-        auto sample = [&](const float* Pv, const DresCol& c, int k) {
-            const float zc = fmaf(c.dzc, (float)(k + 1) - hz, hz);
-            const float fz = floorf(zc);
-            const float b = zc - fz, a = c.alfa;
-            const int iz = (int)fz;
-            const int ZD = min(max(iz, 1), ZL) - 1, ZU = min(max(iz + 1, 1), ZL) - 1;
-            const float* rd = Pv + (size_t)ZD * YL;
-            const float* ru = Pv + (size_t)ZU * YL;
-            return rd[c.yd] * (1.f - a) * (1.f - b) + ru[c.yd] * (1.f - a) * b +
-                   rd[c.yu] * a * (1.f - b) + ru[c.yu] * a * b;
-        };
-        for (int k = ry; k < ZL; k += RG)
-            gf[k * T + tx] = (sample(Pn, c1, k) - sample(Pc, c2, k)) / dl;
-    } else if (real) {
-        const size_t S = (size_t)YL * ZL;
-        // view derivative: views 0 and P-1 reuse the derivative of views 1 and P-2 (:58-59)
-        const int pc = p < 1 ? 1 : (p > P - 2 ? P - 2 : p);
-        const float* Pm = proj + (size_t)(pc - 1 - proj_view0) * S;
-        const float* Pp = proj + (size_t)(pc + 1 - proj_view0) * S;
-        const float* Pv = proj + (size_t)(p - proj_view0) * S;
-        // u stencil with the reference's edge rule (:63-78)
-        int jl = j - 1, jr = j + 1;
-        if (j < 2) { jl = 0; jr = 2; }
-        else if (j > YL - 3) { jl = YL - 3; jr = YL - 1; }
-        const float2 cy = cuy[j];  // (u coefficient, y coordinate)
-        // sixteen rows' loads in flight per thread (the kernel is load-latency bound)
-#pragma unroll 16
-        for (int k = ry; k < ZL; k += RG) {
-            int kl = k - 1, kr = k + 1;  // v stencil, same edge rule (:85-95)
-            if (k < 2) { kl = 0; kr = 2; }
-            else if (k > ZL - 3) { kl = ZL - 3; kr = ZL - 1; }
-            const float* row = Pv + (size_t)k * YL;
-            float g = (Pp[(size_t)k * YL + j] - Pm[(size_t)k * YL + j]) * inv2dl;
-            g = fmaf(row[jr] - row[jl], cy.x, g);
-            g = fmaf(zcv[k] * cy.y, Pv[(size_t)kr * YL + j] - Pv[(size_t)kl * YL + j], g);
-            gf[k * T + tx] = g;
+    if (real)
+        for (int a = ry; a < AL; a += RG) fws[a * T + tx] = fw[(size_t)a * YL + j];
+    // every Hilbert form reads the kappa rows de-interleaved: even columns, then odd ones
+    const size_t jx = (size_t)((j & 1) * (YLp >> 1) + (j >> 1));
+    const size_t S = (size_t)YL * ZL;
+    const int p0 = vbeg + blockIdx.y * kK1Views;
+    for (int pv = 0; pv < kK1Views; ++pv) {
+        const int p = p0 + pv;
+        if (p >= vend) break;  // block-uniform
+        const size_t xv = (size_t)(p - vbeg) * AL * YLp;
+        __syncthreads();  // the previous view's gf is read; fws is loaded (every thread)
+        if (!real) {
+            // nothing to differentiate
+        } else if (dres) {
+            const int pc = p > P - 2 ? P - 2 : p;  // the last view repeats its neighbour (:101)
+            const float* Pn = proj + (size_t)(pc + 1 - proj_view0) * S;
+            const float* Pc = proj + (size_t)(pc - proj_view0) * S;
+            const DresCol c1 = dres[(size_t)j * 2], c2 = dres[(size_t)j * 2 + 1];
+            const float hz = 0.5f * (float)(ZL + 1);
+            auto sample = [&](const float* Pv, const DresCol& c, int k) {
+                const float zc = fmaf(c.dzc, (float)(k + 1) - hz, hz);
+                const float fz = floorf(zc);
+                const float b = zc - fz, a = c.alfa;
+                const int iz = (int)fz;
+                const int ZD = min(max(iz, 1), ZL) - 1, ZU = min(max(iz + 1, 1), ZL) - 1;
+                const float* rd = Pv + (size_t)ZD * YL;
+                const float* ru = Pv + (size_t)ZU * YL;
+                return rd[c.yd] * (1.f - a) * (1.f - b) + ru[c.yd] * (1.f - a) * b +
+                       rd[c.yu] * a * (1.f - b) + ru[c.yu] * a * b;
+            };
+            for (int k = ry; k < ZL; k += RG)
+                gf[k * T + tx] = (sample(Pn, c1, k) - sample(Pc, c2, k)) / dl;
+        } else {
+            // view derivative: views 0 and P-1 reuse the derivative of views 1 and P-2 (:58-59)
+            const int pc = p < 1 ? 1 : (p > P - 2 ? P - 2 : p);
+            const float* Pm = proj + (size_t)(pc - 1 - proj_view0) * S;
+            const float* Pp = proj + (size_t)(pc + 1 - proj_view0) * S;
+            const float* Pv = proj + (size_t)(p - proj_view0) * S;
+            // u stencil with the reference's edge rule (:63-78)
+            int jl = j - 1, jr = j + 1;
+            if (j < 2) { jl = 0; jr = 2; }
+            else if (j > YL - 3) { jl = YL - 3; jr = YL - 1; }
+            const float2 cy = cuy[j];  // (u coefficient, y coordinate)
+#pragma unroll 8
+            for (int k = ry; k < ZL; k += RG) {
+                int kl = k - 1, kr = k + 1;  // v stencil, same edge rule (:85-95)
+                if (k < 2) { kl = 0; kr = 2; }
+                else if (k > ZL - 3) { kl = ZL - 3; kr = ZL - 1; }
+                const float* row = Pv + (size_t)k * YL;
+                float g = (Pp[(size_t)k * YL + j] - Pm[(size_t)k * YL + j]) * inv2dl;
+                g = fmaf(row[jr] - row[jl], cy.x, g);
+                g = fmaf(zcv[k] * cy.y, Pv[(size_t)kr * YL + j] - Pv[(size_t)kl * YL + j], g);
+                gf[k * T + tx] = g;
+            }
+        }
+        __syncthreads();
+        if (!real) {  // zero padding of the kappa rows (the Hilbert forms read K = YLp)
+            for (int a = ry; a < AL; a += RG) store_kappa(X, xv + (size_t)a * YLp + jx, plane, 0.f, mode);
+            continue;
+        }
+#pragma unroll 8
+        for (int a = ry; a < AL; a += RG) {
+            const FwEntry f = fws[a * T + tx];
+            store_kappa(X, xv + (size_t)a * YLp + jx, plane,
+                        fmaf(f.wa, gf[f.r0 * T + tx], f.wb * gf[f.r1 * T + tx]), mode);
         }
     }
-    __syncthreads();
-    if (j >= YLp) return;
-    // the tensor-core forms read each kappa row de-interleaved: even columns, then odd ones
-    const size_t jx = mode == CTRECON_HILBERT_FP32 ? (size_t)j
-                                                   : (size_t)((j & 1) * (YLp >> 1) + (j >> 1));
-    if (!real) {  // zero padding of the kappa rows (the GEMM form reads K = YLp)
-        for (int a = ry; a < AL; a += RG) store_kappa(X, xv + (size_t)a * YLp + jx, plane, 0.f, mode);
-        return;
-    }
-#pragma unroll 8
-    for (int a = ry; a < AL; a += RG) {
-        const FwEntry f = fw[(size_t)a * YL + j];
-        store_kappa(X, xv + (size_t)a * YLp + jx, plane,
-                    fmaf(f.wa, gf[f.r0 * T + tx], f.wb * gf[f.r1 * T + tx]), mode);
-    }
+}
+
+// K1 launch: grid (YLp / 32, views / 16), shared memory for the entries and one view's rows
+static Status k1_shape(int AL, int ZL, size_t* smem) {
+    *smem = (size_t)AL * kK1Cols * sizeof(FwEntry) + (size_t)ZL * kK1Cols * sizeof(float);
+    if (*smem > 227 * 1024)
+        return make_status(CTRECON_ERR_UNSUPPORTED, "too many detector rows for K1");
+    return Status::Ok();
+}
+
+static Status launch_k1(cudaStream_t s, const float* d_proj, int proj_view0, int P, int YL,
+                        int ZL, int AL, int YLp, int c0, int n, const FwEntry* fw,
+                        const float2* cuy, const float* zcv, float inv2dl, const DresCol* dres,
+                        float dl, void* X, size_t plane, int mode) {
+    size_t smem;
+    CTR_TRY(k1_shape(AL, ZL, &smem));
+    CTR_CUDA(cudaFuncSetAttribute(k_deriv_rebin, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)smem));
+    const dim3 g((YLp + kK1Cols - 1) / kK1Cols, (n + kK1Views - 1) / kK1Views);
+    const dim3 b(kK1Cols, kRowGroups * 2);
+    k_deriv_rebin<<<g, b, smem, s>>>(d_proj, proj_view0, P, YL, ZL, AL, YLp, c0, c0 + n, fw, cuy,
+                                     zcv, inv2dl, dres, dl, X, plane, mode);
+    CTR_CUDA(cudaGetLastError());
+    return Status::Ok();
 }
 
 // ---------------------------------------------------------------------------------------------
 // K2 (FP32 SIMT)
 // ---------------------------------------------------------------------------------------------
-constexpr int kTileI = 64;   // output columns per CTA
-constexpr int kXS = 65;      // padded shared-memory row stride
-constexpr int kRA = 4;       // kappa rows per thread
+constexpr int kTileI = 64;   // output columns per CTA (32 of each parity)
+constexpr int kXS = 65;      // padded row stride of the output tile in shared memory
+constexpr int kXP = 36;      // row stride (floats) of one parity's 32 staged inputs
+// kappa rows per thread: 4, or 8 for views of more than 256 kappa rows (512 threads at most)
+inline int simt_rows_per_thread(int AL) { return AL > 256 ? 8 : 4; }
 
-// thread (ig, ag): ig in 0..7 selects parity q = ig>>2 and column group s = ig&3; the thread
-// owns columns i_m = i0 + q + 2(8s + m), m = 0..7, and kappa rows a0..a0+kRA-1. Only inputs
-// j of the opposite parity contribute (odd lags), so the lag window advances by one tap
-// per step of j and rotates through registers.
-__global__ void k_hilbert_simt(const float* __restrict__ X, int AL, int ALpad, int YL, int YLp,
-                               int ZL, const float* __restrict__ hpad, int HOFF,
-                               const BkEntry* __restrict__ bk, float* __restrict__ fproj) {
-    extern __shared__ float sm[];
-    float* hs = sm;               // 2*HOFF taps, hs[HOFF + L] = h[L]
-    float* xs = hs + 2 * HOFF;    // ALpad x kXS: kappa-row chunk, later the output tile
+__device__ __forceinline__ void cp_async16(float* dst, const float* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
+                     (uint32_t)__cvta_generic_to_shared(dst)),
+                 "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Thread (ig, ag): ig in 0..7 selects output parity q = ig>>2 and column group s = ig&3; the
+// thread owns columns i_m = i0 + q + 2(8s + m), m = 0..7, and kappa rows a0..a0+RA-1. Only
+// inputs of the other parity contribute (odd lags): with j_n = jc + (1-q) + 2n the lag is
+// 2K + 1, K = (i0 - jc)/2 + q - 1 + 8s + m - n, and hso[KOFF + K] = h(2K + 1) (odd-lag taps,
+// contiguous). Eight input steps n use the 15 taps K = c - 7 .. c + 7 of a register window
+// indexed statically (T[m - n + 7]), so the inner loop is FMAs and its loads only. The
+// kappa rows are de-interleaved (even columns, then odd ones, as the derivative kernel writes
+// them), so each parity's 32 inputs of a chunk are 128 contiguous bytes: they are staged with
+// cp.async into a double-buffered ring, one chunk ahead of the arithmetic.
+template <int RA>
+__global__ void __launch_bounds__(512, RA == 4 ? 2 : 1)
+k_hilbert_simt(const float* __restrict__ X, int AL, int ALpad, int YL, int YLp, int ZL,
+               const float* __restrict__ hso, const BkEntry* __restrict__ bk,
+               float* __restrict__ fproj) {
+    extern __shared__ __align__(16) float sm[];
+    const int KOFF = simt_koff(YLp);
+    float* hs = sm;               // 2*KOFF odd-lag taps
+    float* xs = hs + 2 * KOFF;    // two stages of ALpad x 2 parities x kXP; later the output tile
+    const int stage_f = ALpad * 2 * kXP;
     const int tid = threadIdx.x, nt = blockDim.x;
     const int ig = tid & 7, ag = tid >> 3;
     const int q = ig >> 2, s = ig & 3;
     const int i0 = blockIdx.x * kTileI;
     const int v = blockIdx.y;
+    const int YLh = YLp >> 1;
     const float* Xv = X + (size_t)v * AL * YLp;
-    for (int t = tid; t < 2 * HOFF; t += nt) hs[t] = hpad[t];
-    const int a0 = ag * kRA;
-    float acc[kRA][8];
+    const int nchunk = YLp / kTileI;
+    auto stage_in = [&](int c, int st) {
+        // row a, parity p, 16-byte piece k: X[a][p*YLh + 32c + 4k .. +3]
+        float* dst = xs + st * stage_f;
+        for (int t = tid; t < AL * 16; t += nt) {
+            const int a = t >> 4, p = (t >> 3) & 1, k = t & 7;
+            cp_async16(dst + (a * 2 + p) * kXP + 4 * k,
+                       Xv + (size_t)a * YLp + p * YLh + 32 * c + 4 * k);
+        }
+        cp_async_commit();
+    };
+    stage_in(0, 0);
+    for (int t = tid; t < 2 * KOFF; t += nt) hs[t] = hso[t];
+    for (int t = tid; t < (ALpad - AL) * 2 * kXP; t += nt) {  // padded rows stay zero
+        xs[AL * 2 * kXP + t] = 0.f;
+        xs[stage_f + AL * 2 * kXP + t] = 0.f;
+    }
+    const int a0 = ag * RA;
+    float acc[RA][8];
 #pragma unroll
-    for (int r = 0; r < kRA; ++r)
+    for (int r = 0; r < RA; ++r)
 #pragma unroll
         for (int m = 0; m < 8; ++m) acc[r][m] = 0.f;
 
-    for (int jc = 0; jc < YLp; jc += kTileI) {
-        __syncthreads();
-        for (int t = tid; t < ALpad * kTileI; t += nt) {
-            const int a = t >> 6, jj = t & 63;
-            xs[a * kXS + jj] = (a < AL) ? Xv[(size_t)a * YLp + jc + jj] : 0.f;
+    for (int c = 0; c < nchunk; ++c) {
+        if (c + 1 < nchunk) {
+            stage_in(c + 1, (c + 1) & 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
         }
         __syncthreads();
-        if (a0 < ALpad) {
-            // lag(m, n) = i_m - j_n with j_n = jc + (1-q) + 2n
-            const int base = HOFF + i0 - jc + 2 * q - 1 + 16 * s;
-            float w[8];
+        const float* xr = xs + (c & 1) * stage_f + (a0 * 2 + (1 - q)) * kXP;
+        const int c0 = KOFF + ((i0 - c * kTileI) >> 1) + q - 1 + 8 * s;
 #pragma unroll
-            for (int m = 0; m < 8; ++m) w[m] = hs[base + 2 * m];
-            const float* xr = xs + a0 * kXS + (1 - q);
+        for (int t = 0; t < 4; ++t) {
+            float T[15];
 #pragma unroll
-            for (int n = 0; n < 32; ++n) {
-                if (n > 0) {
+            for (int u = 0; u < 15; ++u) T[u] = hs[c0 - 8 * t - 7 + u];
 #pragma unroll
-                    for (int m = 7; m > 0; --m) w[m] = w[m - 1];
-                    w[0] = hs[base - 2 * n];
-                }
+            for (int r = 0; r < RA; ++r) {
+                const float4 x0 = *reinterpret_cast<const float4*>(xr + r * 2 * kXP + 8 * t);
+                const float4 x1 = *reinterpret_cast<const float4*>(xr + r * 2 * kXP + 8 * t + 4);
+                const float xv[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
 #pragma unroll
-                for (int r = 0; r < kRA; ++r) {
-                    const float xv = xr[r * kXS + 2 * n];
+                for (int n = 0; n < 8; ++n)
 #pragma unroll
-                    for (int m = 0; m < 8; ++m) acc[r][m] = fmaf(w[m], xv, acc[r][m]);
-                }
+                    for (int m = 0; m < 8; ++m) acc[r][m] = fmaf(T[m - n + 7], xv[n], acc[r][m]);
             }
         }
+        __syncthreads();  // the stage is refilled two chunks on
     }
-    __syncthreads();
-    if (a0 < ALpad) {
+    float* ot = xs;  // [ALpad][kXS] output tile in natural column order
 #pragma unroll
-        for (int r = 0; r < kRA; ++r)
+    for (int r = 0; r < RA; ++r)
 #pragma unroll
-            for (int m = 0; m < 8; ++m) xs[(a0 + r) * kXS + q + 2 * (8 * s + m)] = acc[r][m];
-    }
+        for (int m = 0; m < 8; ++m) ot[(a0 + r) * kXS + q + 2 * (8 * s + m)] = acc[r][m];
     __syncthreads();
     // post-weight + backward rebin (:181-284): a gather across the kappa rows of the tile; the
     // table entries of four outputs are loaded (read-only path) before their stores, so their
@@ -212,10 +286,50 @@ __global__ void k_hilbert_simt(const float* __restrict__ X, int AL, int ALpad, i
             const int idx = idx0 + r * nt, k = idx >> 6, t = idx & 63, i = i0 + t;
             if (idx >= ZL * kTileI || i >= YL) continue;
             fproj[((size_t)v * ZL + k) * YL + i] =
-                fmaf(__int_as_float(e[r].z), xs[e[r].x * kXS + t],
-                     __int_as_float(e[r].w) * xs[e[r].y * kXS + t]);
+                fmaf(__int_as_float(e[r].z), ot[e[r].x * kXS + t],
+                     __int_as_float(e[r].w) * ot[e[r].y * kXS + t]);
         }
     }
+}
+
+// shared memory of k_hilbert_simt: the taps, two input stages, or the output tile
+size_t simt_smem_bytes(int ALpad, int YLp) {
+    const size_t stages = (size_t)2 * ALpad * 2 * kXP;
+    return (2 * (size_t)simt_koff(YLp) + std::max(stages, (size_t)ALpad * kXS)) * sizeof(float);
+}
+
+// Launches k_hilbert_simt over `n` views of kappa rows X into `out` (shape checked first).
+static Status simt_shape(int AL, int YLp, int* RA, int* ALpad, int* nthreads, size_t* smem) {
+    *RA = simt_rows_per_thread(AL);
+    *ALpad = (AL + *RA - 1) / *RA * *RA;
+    *nthreads = (*ALpad / *RA) * 8;
+    if (*nthreads > 512)
+        return make_status(CTRECON_ERR_UNSUPPORTED, "too many kappa lines for the FP32 filter");
+    *smem = simt_smem_bytes(*ALpad, YLp);
+    if (*smem > 227 * 1024)
+        return make_status(CTRECON_ERR_UNSUPPORTED, "detector too wide for the FP32 filter");
+    if (YLp % 64)
+        return make_status(CTRECON_ERR_INTERNAL, "kappa rows must be padded to 64 columns");
+    return Status::Ok();
+}
+
+static Status launch_simt(cudaStream_t s, const float* X, int AL, int YL, int YLp, int ZL,
+                          const float* hso, const BkEntry* bk, float* out, int n) {
+    int RA, ALpad, nthreads;
+    size_t smem;
+    CTR_TRY(simt_shape(AL, YLp, &RA, &ALpad, &nthreads, &smem));
+    const dim3 g((YL + kTileI - 1) / kTileI, n);
+    if (RA == 4) {
+        CTR_CUDA(cudaFuncSetAttribute(k_hilbert_simt<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem));
+        k_hilbert_simt<4><<<g, nthreads, smem, s>>>(X, AL, ALpad, YL, YLp, ZL, hso, bk, out);
+    } else {
+        CTR_CUDA(cudaFuncSetAttribute(k_hilbert_simt<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem));
+        k_hilbert_simt<8><<<g, nthreads, smem, s>>>(X, AL, ALpad, YL, YLp, ZL, hso, bk, out);
+    }
+    CTR_CUDA(cudaGetLastError());
+    return Status::Ok();
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -301,47 +415,30 @@ Status launch_filter(ctrecon_ctx* ctx, cudaStream_t s, FilterPlan& plan, const f
         dres = plan.dres.as<DresCol>();
     }
 
-    // K1 launch shape: one thread per column, ZL floats of shared memory per thread
-    int tj = 128;
-    while (tj > 32 && (size_t)ZL * tj * sizeof(float) > 96 * 1024) tj /= 2;
-    const size_t smem1 = (size_t)ZL * tj * sizeof(float);
-    const dim3 b1(tj, kRowGroups);
-    if (smem1 > 200 * 1024)
-        return make_status(CTRECON_ERR_UNSUPPORTED, "too many detector rows for K1");
-    CTR_CUDA(cudaFuncSetAttribute(k_deriv_rebin, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)smem1));
-    // K2 launch shape
-    const int ALpad = (AL + kRA - 1) / kRA * kRA;
-    const int nthreads2 = std::max(32, (ALpad / kRA) * 8);
-    if (nthreads2 > 1024)
-        return make_status(CTRECON_ERR_UNSUPPORTED, "too many kappa lines for the FP32 filter");
-    const int HOFF = YLp + 64;
-    const size_t smem2 = (2 * (size_t)HOFF + (size_t)ALpad * kXS) * sizeof(float);
-    if (smem2 > 227 * 1024)
-        return make_status(CTRECON_ERR_UNSUPPORTED, "detector too wide for the FP32 filter");
-    CTR_CUDA(cudaFuncSetAttribute(k_hilbert_simt, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)smem2));
+    {  // K1 launch shape, checked before any launch
+        size_t smem1;
+        CTR_TRY(k1_shape(AL, ZL, &smem1));
+    }
+    if (mode == CTRECON_HILBERT_FP32) {  // K2 launch shape, checked before any launch
+        int RA, ALpad, nthreads2;
+        size_t smem2;
+        CTR_TRY(simt_shape(AL, YLp, &RA, &ALpad, &nthreads2, &smem2));
+    }
 
     for (int c0 = view_begin; c0 < view_end; c0 += chunk) {
         const int n = std::min(chunk, view_end - c0);
-        dim3 g1((YLp + tj - 1) / tj, n);
         const size_t plane = (size_t)n * AL * YLp;
         {
             KernelTimer tm(ctx, s, kKDerivRebin);
-            k_deriv_rebin<<<g1, b1, smem1, s>>>(d_proj, proj_view0, P, YL, ZL, AL, YLp, c0,
-                                                plan.fw.as<FwEntry>(), plan.cuy.as<float2>(),
-                                                plan.zcv.as<float>(), plan.inv2dl, dres,
-                                                (float)t.DeltaL, X, plane, mode);
-            CTR_CUDA(cudaGetLastError());
+            CTR_TRY(launch_k1(s, d_proj, proj_view0, P, YL, ZL, AL, YLp, c0, n,
+                              plan.fw.as<FwEntry>(), plan.cuy.as<float2>(), plan.zcv.as<float>(),
+                              plan.inv2dl, dres, (float)t.DeltaL, X, plane, mode));
         }
         float* out = d_fproj + (size_t)(c0 - out_view0) * YL * ZL;
         if (mode == CTRECON_HILBERT_FP32) {
             KernelTimer tm(ctx, s, kKHilbertSimt);
-            dim3 g2((YL + kTileI - 1) / kTileI, n);
-            k_hilbert_simt<<<g2, nthreads2, smem2, s>>>(static_cast<const float*>(X), AL, ALpad,
-                                                        YL, YLp, ZL, plan.h.as<float>(), HOFF,
-                                                        plan.bk.as<BkEntry>(), out);
-            CTR_CUDA(cudaGetLastError());
+            CTR_TRY(launch_simt(s, static_cast<const float*>(X), AL, YL, YLp, ZL,
+                                plan.h.as<float>(), plan.bk.as<BkEntry>(), out, n));
         } else {
             KernelTimer tm(ctx, s, kKHilbertTc);
             CTR_TRY(launch_hilbert_tc(ctx, s, plan, X, n, out, mode));
@@ -354,39 +451,24 @@ Status launch_filter(ctrecon_ctx* ctx, cudaStream_t s, FilterPlan& plan, const f
 // (`chunk` views of AL*YLp floats), for the entry point that allocates nothing (noalloc.cu).
 Status launch_filter_fp32_preplaced(cudaStream_t s, const FilterTables& t, int YLp,
                                     const FwEntry* fw, const BkEntry* bk, const float2* cuy,
-                                    const float* zcv, const float* hpad, float inv2dl,
+                                    const float* zcv, const float* hso, float inv2dl,
                                     float* kappa, int chunk, const float* d_proj,
                                     float* d_fproj) {
     const int YL = t.YL, ZL = t.ZL, AL = t.AL, P = t.P;
-    int tj = 128;
-    while (tj > 32 && (size_t)ZL * tj * sizeof(float) > 96 * 1024) tj /= 2;
-    const size_t smem1 = (size_t)ZL * tj * sizeof(float);
-    const dim3 b1(tj, kRowGroups);
-    if (smem1 > 200 * 1024)
-        return make_status(CTRECON_ERR_UNSUPPORTED, "too many detector rows for K1");
-    CTR_CUDA(cudaFuncSetAttribute(k_deriv_rebin, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)smem1));
-    const int ALpad = (AL + kRA - 1) / kRA * kRA;
-    const int nthreads2 = std::max(32, (ALpad / kRA) * 8);
-    if (nthreads2 > 1024)
-        return make_status(CTRECON_ERR_UNSUPPORTED, "too many kappa lines for the FP32 filter");
-    const int HOFF = YLp + 64;
-    const size_t smem2 = (2 * (size_t)HOFF + (size_t)ALpad * kXS) * sizeof(float);
-    if (smem2 > 227 * 1024)
-        return make_status(CTRECON_ERR_UNSUPPORTED, "detector too wide for the FP32 filter");
-    CTR_CUDA(cudaFuncSetAttribute(k_hilbert_simt, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)smem2));
+    {
+        size_t smem1;
+        CTR_TRY(k1_shape(AL, ZL, &smem1));
+    }
+    {
+        int RA, ALpad, nthreads2;
+        size_t smem2;
+        CTR_TRY(simt_shape(AL, YLp, &RA, &ALpad, &nthreads2, &smem2));
+    }
     for (int c0 = 0; c0 < P; c0 += chunk) {
         const int n = std::min(chunk, P - c0);
-        dim3 g1((YLp + tj - 1) / tj, n);
-        k_deriv_rebin<<<g1, b1, smem1, s>>>(d_proj, 0, P, YL, ZL, AL, YLp, c0, fw, cuy, zcv,
-                                            inv2dl, nullptr, 0.f, kappa, 0,
-                                            CTRECON_HILBERT_FP32);
-        CTR_CUDA(cudaGetLastError());
-        dim3 g2((YL + kTileI - 1) / kTileI, n);
-        k_hilbert_simt<<<g2, nthreads2, smem2, s>>>(kappa, AL, ALpad, YL, YLp, ZL, hpad, HOFF, bk,
-                                                    d_fproj + (size_t)c0 * YL * ZL);
-        CTR_CUDA(cudaGetLastError());
+        CTR_TRY(launch_k1(s, d_proj, 0, P, YL, ZL, AL, YLp, c0, n, fw, cuy, zcv, inv2dl, nullptr,
+                          0.f, kappa, 0, CTRECON_HILBERT_FP32));
+        CTR_TRY(launch_simt(s, kappa, AL, YL, YLp, ZL, hso, bk, d_fproj + (size_t)c0 * YL * ZL, n));
     }
     return Status::Ok();
 }

@@ -295,4 +295,13 @@ BPParams make_bp_params(const BPGeom& g) {
     return k;
 }
 
+void build_simt_taps(const FilterTables& t, int YLp, std::vector<float>& hso) {
+    const int KOFF = simt_koff(YLp);
+    hso.assign(2 * (size_t)KOFF, 0.f);
+    for (int K = -KOFF; K < KOFF; ++K) {
+        const int L = 2 * K + 1;  // odd lag
+        if (L >= -(t.YL - 1) && L <= t.YL - 1) hso[(size_t)(K + KOFF)] = (float)t.h[(size_t)(L + t.YL - 1)];
+    }
+}
+
 }  // namespace ctr

@@ -279,6 +279,10 @@ Status build_bp_plan(const BPGeom& g, BPPlan& plan);
 Status reset_device_flag(ctrecon_ctx* ctx, cudaStream_t s);
 
 // kernel launchers (filter.cu, pi.cu, bkproj.cu, phantom.cu)
+// Odd-lag Hilbert taps of the FP32 filter: hso[simt_koff(YLp) + K] = h(2K + 1) for
+// |2K + 1| <= YL - 1, zero beyond; 2 * simt_koff(YLp) entries (geometry.cpp).
+__host__ __device__ inline int simt_koff(int YLp) { return YLp / 2 + 32; }
+void build_simt_taps(const FilterTables& t, int YLp, std::vector<float>& hso);
 // tensor-core Hilbert (hilbert_tc.cu: single pass; hilbert_tc2.cu: parity split, persistent).
 // In the tensor-core modes the kappa rows are stored de-interleaved: column j of a row at
 // (j & 1) * YLp / 2 + (j >> 1).

@@ -11,6 +11,7 @@
 // allocating library routine; only the caller's projection buffers and this array are used.
 #include "internal.h"
 
+#include <cstring>
 #include <mutex>
 #include <vector>
 
@@ -18,7 +19,7 @@ namespace ctr {
 
 Status launch_filter_fp32_preplaced(cudaStream_t s, const FilterTables& t, int YLp,
                                     const FwEntry* fw, const BkEntry* bk, const float2* cuy,
-                                    const float* zcv, const float* hpad, float inv2dl,
+                                    const float* zcv, const float* hso, float inv2dl,
                                     float* kappa, int chunk, const float* d_proj,
                                     float* d_fproj);
 void set_noctx_error(const std::string& m);
@@ -59,7 +60,8 @@ static Status filter_noalloc(cudaStream_t s, const ctrecon_filter_params& p, con
     CTR_TRY(build_filter_tables(p, t));
     const int YL = t.YL, ZL = t.ZL, AL = t.AL;
     const int YLp = (YL + 63) / 64 * 64;
-    const int HOFF = YLp + 64;
+    std::vector<float> hso;
+    build_simt_taps(t, YLp, hso);
     const size_t ay = (size_t)AL * YL, zy = (size_t)ZL * YL;
     // layout of the array: tables, then the kappa-row scratch
     const size_t o_fw = 0;
@@ -67,7 +69,7 @@ static Status filter_noalloc(cudaStream_t s, const ctrecon_filter_params& p, con
     const size_t o_cuy = align256(o_bk + zy * sizeof(BkEntry));
     const size_t o_zcv = align256(o_cuy + (size_t)YL * sizeof(float2));
     const size_t o_h = align256(o_zcv + (size_t)ZL * sizeof(float));
-    const size_t o_kappa = align256(o_h + 2 * (size_t)HOFF * sizeof(float));
+    const size_t o_kappa = align256(o_h + hso.size() * sizeof(float));
     const size_t per_view = (size_t)AL * YLp * sizeof(float);
     if (o_kappa + per_view > kNoAllocBytes)
         return make_status(CTRECON_ERR_UNSUPPORTED,
@@ -87,9 +89,7 @@ static Status filter_noalloc(cudaStream_t s, const ctrecon_filter_params& p, con
     for (int j = 0; j < YL; ++j) cuy[j] = make_float2((float)t.cu[j], (float)t.y[j]);
     float* zcv = reinterpret_cast<float*>(blob.data() + o_zcv);
     for (int k = 0; k < ZL; ++k) zcv[k] = (float)(t.z[k] * t.cv);
-    float* hp = reinterpret_cast<float*>(blob.data() + o_h);
-    for (int m = -(YL - 1); m <= YL - 1; ++m)
-        if (m & 1) hp[HOFF + m] = (float)t.h[(size_t)(m + YL - 1)];
+    std::memcpy(blob.data() + o_h, hso.data(), hso.size() * sizeof(float));
 
     void* base = nullptr;
     CTR_TRY(scratch_address(&base));
