@@ -73,6 +73,9 @@ def parse():
                          "form tile shapes, 5-9 per-cell records staged by producer warps, "
                          "10-12 cell records written to HBM first and brought in by tensor "
                          "copies, 100 first form")
+    ap.add_argument("--bp-window", type=int, default=0,
+                    help="views per cell-record window of the fifth backprojector form (0: as "
+                         "many as fit); smaller windows hold less device memory")
     ap.add_argument("--batched", action="store_true",
                     help="16 uneven scans (c4): one-at-a-time vs one batched graph replay")
     ap.add_argument("--report", choices=["c3", "c5", "extras", "refgpu"],
@@ -1032,6 +1035,8 @@ def run_headline(args):
               "tf32": _lib.HILBERT_TF32}
     pi_of = {"bisect": _lib.PI_BISECT, "newton": _lib.PI_NEWTON, "learned": _lib.PI_LEARNED}
     ctx = ct.Context(local)
+    if args.bp_window:
+        ctx.set_option(_lib.OPT_BP_WINDOW, args.bp_window)
     ctx.set_option(_lib.OPT_PINET_MODE, {"voxel-fp32": _lib.PINET_VOXEL_FP32,
                                          "voxel-bf16": _lib.PINET_VOXEL_BF16,
                                          "grid": _lib.PINET_GRID}[args.pinet_mode])
@@ -1327,15 +1332,20 @@ def run_headline(args):
             cores = os.cpu_count() or 1
             smp = CpuChainSample(O, s, lambda a, b: d_proj[a:b].cpu().numpy().astype(np.float64),
                                  updates, n=32, copies=1)
+            # the sample repeated until 10 s of CPU time have passed
+            reps = 0
             t0 = time.perf_counter()
-            smp.filter_once()
-            O.bkproj(smp.gb, smp.fproj, np.zeros((smp.n,) * 3), nthreads=cores)
+            while reps == 0 or time.perf_counter() - t0 < 10.0:
+                smp.filter_once()
+                O.bkproj(smp.gb, smp.fproj, np.zeros((smp.n,) * 3), nthreads=cores)
+                reps += 1
             t_smp = time.perf_counter() - t0
-            g = smp.updates / t_smp / 1e9
+            g = reps * smp.updates / t_smp / 1e9
             cpu = {"value": g, "unit": "GUPS", "cores": cores, "kind": "port",
-                   "s_per_vol": updates / (g * 1e9), "sample_s": t_smp,
+                   "s_per_vol": updates / (g * 1e9), "sample_s": t_smp, "repeats": reps,
                    "sample": smp.describe("the FP64 oracle's",
-                                          f"the FP64 oracle with {cores} OpenMP threads")}
+                                          f"the FP64 oracle with {cores} OpenMP threads") +
+                   f"; repeated {reps} times ({t_smp:.1f} s)"}
         except Exception as exc:  # the baseline is reported, never required
             cpu = {"value": None, "unit": "GUPS", "cores": 0, "kind": "port",
                    "sample": f"failed: {exc}"}

@@ -45,105 +45,94 @@ __device__ __forceinline__ void store_kappa(void* X, size_t idx, size_t plane, f
     }
 }
 
-// Block (T = 32 columns) x (RG row groups); it walks views vbeg + blockIdx.y * VB .. + VB - 1 of
-// the chunk (at most vend): the forward-rebin entries of its columns are loaded into shared
-// memory once and serve all VB views (otherwise the 16-byte entries, read for every kappa
-// sample of every view, are the largest stream the kernel moves). Per view, thread (tx, ry)
-// computes the derivative rows k = ry, ry + RG, ... of column j = blockIdx.x * T + tx into
-// shared memory, then the kappa rows a = ry, ry + RG, ...; the RG groups keep RG independent
-// row walks in flight per column.
+// Block (T columns) x (RG row groups): thread (tx, ry) owns column j = blockIdx.x * T + tx and
+// computes the derivative rows k = ry, ry + RG, ... then the kappa rows a = ry, ry + RG, ...;
+// the RG groups keep RG independent row walks in flight per column.
 // dres != NULL selects the direct half-view derivative of KatsevichFiltering_T.m:50-101
 // (entries [column][side], side 0 applied to the next view, side 1 to this one; dl = DeltaL):
 // the resampled row position (k + 1 - HalfZ) * Dzc + HalfZ is formed here in FP32, the column
 // position comes from the FP64 host table; indices clamped as CheckData.m.
-constexpr int kK1Cols = 32;
-constexpr int kK1Views = 16;
-__global__ void __launch_bounds__(kK1Cols * kRowGroups * 2)
-k_deriv_rebin(const float* __restrict__ proj, int proj_view0, int P, int YL, int ZL, int AL,
-              int YLp, int vbeg, int vend, const FwEntry* __restrict__ fw,
-              const float2* __restrict__ cuy, const float* __restrict__ zcv, float inv2dl,
-              const DresCol* __restrict__ dres, float dl, void* __restrict__ X, size_t plane,
-              int mode) {
-    extern __shared__ __align__(16) unsigned char k1_smem[];
-    constexpr int T = kK1Cols;
-    const int tx = threadIdx.x, ry = threadIdx.y, RG = blockDim.y;
-    FwEntry* fws = reinterpret_cast<FwEntry*>(k1_smem);                   // AL x T
-    float* gf = reinterpret_cast<float*>(k1_smem + (size_t)AL * T * sizeof(FwEntry));  // ZL x T
-    const int j = blockIdx.x * T + tx;  // < YLp: the grid covers YLp, a multiple of T
+__global__ void k_deriv_rebin(const float* __restrict__ proj, int proj_view0, int P, int YL,
+                              int ZL, int AL, int YLp, int vbeg,
+                              const FwEntry* __restrict__ fw, const float2* __restrict__ cuy,
+                              const float* __restrict__ zcv, float inv2dl,
+                              const DresCol* __restrict__ dres, float dl,
+                              void* __restrict__ X, size_t plane, int mode) {
+    extern __shared__ float gf[];  // ZL x blockDim.x: the derivative of the block's columns
+    const int T = blockDim.x, tx = threadIdx.x, ry = threadIdx.y, RG = blockDim.y;
+    const int j = blockIdx.x * T + tx;
+    const int p = vbeg + blockIdx.y;
+    const size_t xv = (size_t)blockIdx.y * AL * YLp;
     const bool real = j < YL;
-    if (real)
-        for (int a = ry; a < AL; a += RG) fws[a * T + tx] = fw[(size_t)a * YL + j];
+    if (real && dres) {
+        const size_t S = (size_t)YL * ZL;
+        const int pc = p > P - 2 ? P - 2 : p;  // the last view repeats its neighbour (:101)
+        const float* Pn = proj + (size_t)(pc + 1 - proj_view0) * S;
+        const float* Pc = proj + (size_t)(pc - proj_view0) * S;
+        const DresCol c1 = dres[(size_t)j * 2], c2 = dres[(size_t)j * 2 + 1];
+        const float hz = 0.5f * (float)(ZL + 1);
+        auto sample = [&](const float* Pv, const DresCol& c, int k) {
+            const float zc = fmaf(c.dzc, (float)(k + 1) - hz, hz);
+            const float fz = floorf(zc);
+            const float b = zc - fz, a = c.alfa;
+            const int iz = (int)fz;
+            const int ZD = min(max(iz, 1), ZL) - 1, ZU = min(max(iz + 1, 1), ZL) - 1;
+            const float* rd = Pv + (size_t)ZD * YL;
+            const float* ru = Pv + (size_t)ZU * YL;
+            return rd[c.yd] * (1.f - a) * (1.f - b) + ru[c.yd] * (1.f - a) * b +
+                   rd[c.yu] * a * (1.f - b) + ru[c.yu] * a * b;
+        };
+        for (int k = ry; k < ZL; k += RG)
+            gf[k * T + tx] = (sample(Pn, c1, k) - sample(Pc, c2, k)) / dl;
+    } else if (real) {
+        const size_t S = (size_t)YL * ZL;
+        // view derivative: views 0 and P-1 reuse the derivative of views 1 and P-2 (:58-59)
+        const int pc = p < 1 ? 1 : (p > P - 2 ? P - 2 : p);
+        const float* Pm = proj + (size_t)(pc - 1 - proj_view0) * S;
+        const float* Pp = proj + (size_t)(pc + 1 - proj_view0) * S;
+        const float* Pv = proj + (size_t)(p - proj_view0) * S;
+        // u stencil with the reference's edge rule (:63-78)
+        int jl = j - 1, jr = j + 1;
+        if (j < 2) { jl = 0; jr = 2; }
+        else if (j > YL - 3) { jl = YL - 3; jr = YL - 1; }
+        const float2 cy = cuy[j];  // (u coefficient, y coordinate)
+        // sixteen rows' loads in flight per thread (the kernel is load-latency bound)
+#pragma unroll 16
+        for (int k = ry; k < ZL; k += RG) {
+            int kl = k - 1, kr = k + 1;  // v stencil, same edge rule (:85-95)
+            if (k < 2) { kl = 0; kr = 2; }
+            else if (k > ZL - 3) { kl = ZL - 3; kr = ZL - 1; }
+            const float* row = Pv + (size_t)k * YL;
+            float g = (Pp[(size_t)k * YL + j] - Pm[(size_t)k * YL + j]) * inv2dl;
+            g = fmaf(row[jr] - row[jl], cy.x, g);
+            g = fmaf(zcv[k] * cy.y, Pv[(size_t)kr * YL + j] - Pv[(size_t)kl * YL + j], g);
+            gf[k * T + tx] = g;
+        }
+    }
+    __syncthreads();
+    if (j >= YLp) return;
     // every Hilbert form reads the kappa rows de-interleaved: even columns, then odd ones
     const size_t jx = (size_t)((j & 1) * (YLp >> 1) + (j >> 1));
-    const size_t S = (size_t)YL * ZL;
-    const int p0 = vbeg + blockIdx.y * kK1Views;
-    for (int pv = 0; pv < kK1Views; ++pv) {
-        const int p = p0 + pv;
-        if (p >= vend) break;  // block-uniform
-        const size_t xv = (size_t)(p - vbeg) * AL * YLp;
-        __syncthreads();  // the previous view's gf is read; fws is loaded (every thread)
-        if (!real) {
-            // nothing to differentiate
-        } else if (dres) {
-            const int pc = p > P - 2 ? P - 2 : p;  // the last view repeats its neighbour (:101)
-            const float* Pn = proj + (size_t)(pc + 1 - proj_view0) * S;
-            const float* Pc = proj + (size_t)(pc - proj_view0) * S;
-            const DresCol c1 = dres[(size_t)j * 2], c2 = dres[(size_t)j * 2 + 1];
-            const float hz = 0.5f * (float)(ZL + 1);
-            auto sample = [&](const float* Pv, const DresCol& c, int k) {
-                const float zc = fmaf(c.dzc, (float)(k + 1) - hz, hz);
-                const float fz = floorf(zc);
-                const float b = zc - fz, a = c.alfa;
-                const int iz = (int)fz;
-                const int ZD = min(max(iz, 1), ZL) - 1, ZU = min(max(iz + 1, 1), ZL) - 1;
-                const float* rd = Pv + (size_t)ZD * YL;
-                const float* ru = Pv + (size_t)ZU * YL;
-                return rd[c.yd] * (1.f - a) * (1.f - b) + ru[c.yd] * (1.f - a) * b +
-                       rd[c.yu] * a * (1.f - b) + ru[c.yu] * a * b;
-            };
-            for (int k = ry; k < ZL; k += RG)
-                gf[k * T + tx] = (sample(Pn, c1, k) - sample(Pc, c2, k)) / dl;
-        } else {
-            // view derivative: views 0 and P-1 reuse the derivative of views 1 and P-2 (:58-59)
-            const int pc = p < 1 ? 1 : (p > P - 2 ? P - 2 : p);
-            const float* Pm = proj + (size_t)(pc - 1 - proj_view0) * S;
-            const float* Pp = proj + (size_t)(pc + 1 - proj_view0) * S;
-            const float* Pv = proj + (size_t)(p - proj_view0) * S;
-            // u stencil with the reference's edge rule (:63-78)
-            int jl = j - 1, jr = j + 1;
-            if (j < 2) { jl = 0; jr = 2; }
-            else if (j > YL - 3) { jl = YL - 3; jr = YL - 1; }
-            const float2 cy = cuy[j];  // (u coefficient, y coordinate)
+    if (!real) {  // zero padding of the kappa rows (the GEMM form reads K = YLp)
+        for (int a = ry; a < AL; a += RG) store_kappa(X, xv + (size_t)a * YLp + jx, plane, 0.f, mode);
+        return;
+    }
 #pragma unroll 8
-            for (int k = ry; k < ZL; k += RG) {
-                int kl = k - 1, kr = k + 1;  // v stencil, same edge rule (:85-95)
-                if (k < 2) { kl = 0; kr = 2; }
-                else if (k > ZL - 3) { kl = ZL - 3; kr = ZL - 1; }
-                const float* row = Pv + (size_t)k * YL;
-                float g = (Pp[(size_t)k * YL + j] - Pm[(size_t)k * YL + j]) * inv2dl;
-                g = fmaf(row[jr] - row[jl], cy.x, g);
-                g = fmaf(zcv[k] * cy.y, Pv[(size_t)kr * YL + j] - Pv[(size_t)kl * YL + j], g);
-                gf[k * T + tx] = g;
-            }
-        }
-        __syncthreads();
-        if (!real) {  // zero padding of the kappa rows (the Hilbert forms read K = YLp)
-            for (int a = ry; a < AL; a += RG) store_kappa(X, xv + (size_t)a * YLp + jx, plane, 0.f, mode);
-            continue;
-        }
-#pragma unroll 8
-        for (int a = ry; a < AL; a += RG) {
-            const FwEntry f = fws[a * T + tx];
-            store_kappa(X, xv + (size_t)a * YLp + jx, plane,
-                        fmaf(f.wa, gf[f.r0 * T + tx], f.wb * gf[f.r1 * T + tx]), mode);
-        }
+    for (int a = ry; a < AL; a += RG) {
+        const FwEntry f = fw[(size_t)a * YL + j];
+        store_kappa(X, xv + (size_t)a * YLp + jx, plane,
+                    fmaf(f.wa, gf[f.r0 * T + tx], f.wb * gf[f.r1 * T + tx]), mode);
     }
 }
 
-// K1 launch: grid (YLp / 32, views / 16), shared memory for the entries and one view's rows
-static Status k1_shape(int AL, int ZL, size_t* smem) {
-    *smem = (size_t)AL * kK1Cols * sizeof(FwEntry) + (size_t)ZL * kK1Cols * sizeof(float);
-    if (*smem > 227 * 1024)
+
+// K1 launch: one thread per column (blocks of up to 128 columns x kRowGroups row groups), ZL
+// floats of shared memory per thread
+static Status k1_shape(int ZL, int* tj, size_t* smem) {
+    *tj = 128;
+    while (*tj > 32 && (size_t)ZL * *tj * sizeof(float) > 96 * 1024) *tj /= 2;
+    *smem = (size_t)ZL * *tj * sizeof(float);
+    if (*smem > 200 * 1024)
         return make_status(CTRECON_ERR_UNSUPPORTED, "too many detector rows for K1");
     return Status::Ok();
 }
@@ -152,14 +141,15 @@ static Status launch_k1(cudaStream_t s, const float* d_proj, int proj_view0, int
                         int ZL, int AL, int YLp, int c0, int n, const FwEntry* fw,
                         const float2* cuy, const float* zcv, float inv2dl, const DresCol* dres,
                         float dl, void* X, size_t plane, int mode) {
+    int tj;
     size_t smem;
-    CTR_TRY(k1_shape(AL, ZL, &smem));
+    CTR_TRY(k1_shape(ZL, &tj, &smem));
     CTR_CUDA(cudaFuncSetAttribute(k_deriv_rebin, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)smem));
-    const dim3 g((YLp + kK1Cols - 1) / kK1Cols, (n + kK1Views - 1) / kK1Views);
-    const dim3 b(kK1Cols, kRowGroups * 2);
-    k_deriv_rebin<<<g, b, smem, s>>>(d_proj, proj_view0, P, YL, ZL, AL, YLp, c0, c0 + n, fw, cuy,
-                                     zcv, inv2dl, dres, dl, X, plane, mode);
+    const dim3 g((YLp + tj - 1) / tj, n);
+    const dim3 b(tj, kRowGroups);
+    k_deriv_rebin<<<g, b, smem, s>>>(d_proj, proj_view0, P, YL, ZL, AL, YLp, c0, fw, cuy, zcv,
+                                     inv2dl, dres, dl, X, plane, mode);
     CTR_CUDA(cudaGetLastError());
     return Status::Ok();
 }
@@ -416,8 +406,9 @@ Status launch_filter(ctrecon_ctx* ctx, cudaStream_t s, FilterPlan& plan, const f
     }
 
     {  // K1 launch shape, checked before any launch
+        int tj;
         size_t smem1;
-        CTR_TRY(k1_shape(AL, ZL, &smem1));
+        CTR_TRY(k1_shape(ZL, &tj, &smem1));
     }
     if (mode == CTRECON_HILBERT_FP32) {  // K2 launch shape, checked before any launch
         int RA, ALpad, nthreads2;
@@ -456,8 +447,9 @@ Status launch_filter_fp32_preplaced(cudaStream_t s, const FilterTables& t, int Y
                                     float* d_fproj) {
     const int YL = t.YL, ZL = t.ZL, AL = t.AL, P = t.P;
     {
+        int tj;
         size_t smem1;
-        CTR_TRY(k1_shape(AL, ZL, &smem1));
+        CTR_TRY(k1_shape(ZL, &tj, &smem1));
     }
     {
         int RA, ALpad, nthreads2;
