@@ -160,8 +160,9 @@ static Status launch_k1(cudaStream_t s, const float* d_proj, int proj_view0, int
 constexpr int kTileI = 64;   // output columns per CTA (32 of each parity)
 constexpr int kXS = 65;      // padded row stride of the output tile in shared memory
 constexpr int kXP = 36;      // row stride (floats) of one parity's 32 staged inputs
-// kappa rows per thread: 4, or 8 for views of more than 256 kappa rows (512 threads at most)
-inline int simt_rows_per_thread(int AL) { return AL > 256 ? 8 : 4; }
+// kappa rows per thread: 4 (at most 384 threads, two CTAs per SM), or 8 for views of more than
+// 192 kappa rows (at most 512 threads)
+inline int simt_rows_per_thread(int AL) { return AL > 192 ? 8 : 4; }
 
 __device__ __forceinline__ void cp_async16(float* dst, const float* src) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
@@ -185,14 +186,18 @@ __device__ __forceinline__ void cp_async_wait() {
 // them), so each parity's 32 inputs of a chunk are 128 contiguous bytes: they are staged with
 // cp.async into a double-buffered ring, one chunk ahead of the arithmetic.
 template <int RA>
-__global__ void __launch_bounds__(512, RA == 4 ? 2 : 1)
+__global__ void __launch_bounds__(RA == 4 ? 384 : 512, RA == 4 ? 2 : 1)
 k_hilbert_simt(const float* __restrict__ X, int AL, int ALpad, int YL, int YLp, int ZL,
                const float* __restrict__ hso, const BkEntry* __restrict__ bk,
                float* __restrict__ fproj) {
     extern __shared__ __align__(16) float sm[];
     const int KOFF = simt_koff(YLp);
-    float* hs = sm;               // 2*KOFF odd-lag taps
-    float* xs = hs + 2 * KOFF;    // two stages of ALpad x 2 parities x kXP; later the output tile
+    // the odd-lag taps twice: hs0 = hso, and hs1 shifted by one element so that both output
+    // parities' 15-tap windows start on a 16-byte boundary (four LDS.128); hs1 sits 4 words past
+    // a bank-aligned offset so the two parities' windows fall in different banks
+    float* hs0 = sm;
+    float* hs1 = sm + 2 * KOFF + 4;
+    float* xs = sm + 4 * KOFF + 8;  // two stages of ALpad x 2 parities x kXP; later the output tile
     const int stage_f = ALpad * 2 * kXP;
     const int tid = threadIdx.x, nt = blockDim.x;
     const int ig = tid & 7, ag = tid >> 3;
@@ -202,18 +207,28 @@ k_hilbert_simt(const float* __restrict__ X, int AL, int ALpad, int YL, int YLp, 
     const int YLh = YLp >> 1;
     const float* Xv = X + (size_t)v * AL * YLp;
     const int nchunk = YLp / kTileI;
+    // staging: 8 threads per staged row (2 AL rows: kappa row a, parity p at r = 2a + p), 16
+    // bytes each; a thread keeps one parity and steps RS rows (RS even), so its addresses advance
+    // by constants
+    const int RS = (nt >> 3) & ~1;
+    const int r0 = tid >> 3, piece = tid & 7;
+    const bool stager = r0 < RS;
+    const float* src0 = Xv + (size_t)(r0 >> 1) * YLp + (r0 & 1) * YLh + 4 * piece;
+    const size_t src_step = (size_t)(RS >> 1) * YLp;
     auto stage_in = [&](int c, int st) {
-        // row a, parity p, 16-byte piece k: X[a][p*YLh + 32c + 4k .. +3]
-        float* dst = xs + st * stage_f;
-        for (int t = tid; t < AL * 16; t += nt) {
-            const int a = t >> 4, p = (t >> 3) & 1, k = t & 7;
-            cp_async16(dst + (a * 2 + p) * kXP + 4 * k,
-                       Xv + (size_t)a * YLp + p * YLh + 32 * c + 4 * k);
+        if (stager) {
+            float* dst = xs + st * stage_f + r0 * kXP + 4 * piece;
+            const float* src = src0 + 32 * c;
+            for (int r = r0; r < 2 * AL; r += RS, dst += RS * kXP, src += src_step)
+                cp_async16(dst, src);
         }
         cp_async_commit();
     };
     stage_in(0, 0);
-    for (int t = tid; t < 2 * KOFF; t += nt) hs[t] = hso[t];
+    for (int t = tid; t < 2 * KOFF; t += nt) {
+        hs0[t] = hso[t];
+        hs1[t] = t + 1 < 2 * KOFF ? hso[t + 1] : 0.f;
+    }
     for (int t = tid; t < (ALpad - AL) * 2 * kXP; t += nt) {  // padded rows stay zero
         xs[AL * 2 * kXP + t] = 0.f;
         xs[stage_f + AL * 2 * kXP + t] = 0.f;
@@ -235,11 +250,16 @@ k_hilbert_simt(const float* __restrict__ X, int AL, int ALpad, int YL, int YLp, 
         __syncthreads();
         const float* xr = xs + (c & 1) * stage_f + (a0 * 2 + (1 - q)) * kXP;
         const int c0 = KOFF + ((i0 - c * kTileI) >> 1) + q - 1 + 8 * s;
+        // window start c0 - 8t - 7 is q (mod 4): hs0 from it, or hs1 from one element before
+        const float* hq = q ? hs1 + (c0 - 8) : hs0 + (c0 - 7);
 #pragma unroll
         for (int t = 0; t < 4; ++t) {
-            float T[15];
+            float T[16];
 #pragma unroll
-            for (int u = 0; u < 15; ++u) T[u] = hs[c0 - 8 * t - 7 + u];
+            for (int w = 0; w < 4; ++w) {
+                const float4 h4 = *reinterpret_cast<const float4*>(hq - 8 * t + 4 * w);
+                T[4 * w] = h4.x; T[4 * w + 1] = h4.y; T[4 * w + 2] = h4.z; T[4 * w + 3] = h4.w;
+            }
 #pragma unroll
             for (int r = 0; r < RA; ++r) {
                 const float4 x0 = *reinterpret_cast<const float4*>(xr + r * 2 * kXP + 8 * t);
@@ -285,7 +305,7 @@ k_hilbert_simt(const float* __restrict__ X, int AL, int ALpad, int YL, int YLp, 
 // shared memory of k_hilbert_simt: the taps, two input stages, or the output tile
 size_t simt_smem_bytes(int ALpad, int YLp) {
     const size_t stages = (size_t)2 * ALpad * 2 * kXP;
-    return (2 * (size_t)simt_koff(YLp) + std::max(stages, (size_t)ALpad * kXS)) * sizeof(float);
+    return (4 * (size_t)simt_koff(YLp) + 8 + std::max(stages, (size_t)ALpad * kXS)) * sizeof(float);
 }
 
 // Launches k_hilbert_simt over `n` views of kappa rows X into `out` (shape checked first).

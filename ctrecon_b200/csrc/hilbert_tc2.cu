@@ -14,7 +14,8 @@
 // the same columns and walk the column blocks of a view group before the next group, so the
 // CTAs working at one time share the group's kappa rows in L2 and write whole sectors of FProj
 // between them. M = 128 outputs (TMEM lanes), N = the group's vpt*AL kappa rows (<= 256),
-// K = YLp/2 in blocks of 128 bytes (128-byte swizzle, no multicast).
+// K = YLp/2 in blocks of 64 bytes for BF16x3 (64-byte swizzle; five stages of the four operand
+// tiles fit shared memory) or 128 bytes for TF32 (128-byte swizzle), no multicast.
 //
 // Persistent and warp-specialised: one CTA per SM walks tiles blockIdx.x, + gridDim.x, ...;
 // warp 0 issues the tensor copies into an S-stage ring, warp 1 the MMAs into one of two TMEM
@@ -53,6 +54,7 @@ constexpr int kRowsAhead = 8;               // backward-rebin entries loaded ahe
 
 struct Tc2Params {
     int AL, YL, ZL, nviews, vpt, ntile, YLh, YLhA, nk, ncb, ntiles, S;
+    int kin;  // K elements per block (the 64- or 128-byte swizzle row)
     int stage_bytes, a_bytes, b_bytes, bar_off;
     const BkEntry* bkp;  // [ZL][2][YLhA], entry (z, p, i') of output column 2 i' + p
     float* out;
@@ -104,6 +106,22 @@ __device__ __forceinline__ void tmem_ld4(uint32_t taddr, float& v0, float& v1, f
     v3 = __uint_as_float(r3);
 }
 
+// K-major operand with 64-byte rows and the 64-byte swizzle: SBO = 8 rows * 64 B = 512 B,
+// version 1 (sm_100), layout type 4 (SWIZZLE_64B)
+__device__ __forceinline__ uint64_t sw64_desc(uint32_t saddr) {
+    uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
+    d |= (uint64_t)(512u >> 4) << 32;
+    d |= (uint64_t)1 << 46;
+    d |= (uint64_t)4 << 61;
+    return d;
+}
+
+template <int RB>
+__device__ __forceinline__ uint64_t swz_desc(uint32_t saddr) {
+    if constexpr (RB == 128) return tcu::sw128_desc(saddr);
+    else return sw64_desc(saddr);
+}
+
 __device__ __forceinline__ float pick4(int d, float v0, float v1, float v2, float v3) {
     return d == 0 ? v0 : d == 1 ? v1 : d == 2 ? v2 : v3;
 }
@@ -119,7 +137,7 @@ __device__ __forceinline__ void tile_coords(const Tc2Params& p, int t, int& vg, 
     vg = r / p.ncb;
 }
 
-template <int MODE>
+template <int MODE, int RB>
 __global__ void __launch_bounds__(kThreads2, 1)
 k_hilbert_tc2(const __grid_constant__ CUtensorMap tA0, const __grid_constant__ CUtensorMap tA1,
               const __grid_constant__ CUtensorMap tB0, const __grid_constant__ CUtensorMap tB1,
@@ -151,7 +169,7 @@ k_hilbert_tc2(const __grid_constant__ CUtensorMap tA0, const __grid_constant__ C
     __syncthreads();
     tcu::fence_after();
     const uint32_t tmem = *tslot;
-    const uint32_t kin = MODE == CTRECON_HILBERT_BF16X3 ? 64 : 32;  // K elements per 128 bytes
+    const uint32_t kin = (uint32_t)p.kin;  // K elements per block of RB bytes
 
     if (warp == 0) {
         // ---- tensor copies -------------------------------------------------------------------
@@ -210,16 +228,13 @@ k_hilbert_tc2(const __grid_constant__ CUtensorMap tA0, const __grid_constant__ C
                     const uint32_t b0 = a0 + PL * p.a_bytes;
                     const uint32_t b1 = b0 + p.b_bytes;
 #pragma unroll
-                    for (int ks = 0; ks < 4; ++ks) {  // 32 bytes of K per MMA
+                    for (int ks = 0; ks < RB / 32; ++ks) {  // 32 bytes of K per MMA
                         const uint32_t off = 32u * ks;
                         const uint32_t acc = (kb > 0 || ks > 0) ? 1u : 0u;
-                        mma2<MODE>(td, tcu::sw128_desc(a0 + off), tcu::sw128_desc(b0 + off), idesc,
-                                   acc);
+                        mma2<MODE>(td, swz_desc<RB>(a0 + off), swz_desc<RB>(b0 + off), idesc, acc);
                         if (MODE == CTRECON_HILBERT_BF16X3) {
-                            mma2<MODE>(td, tcu::sw128_desc(a0 + off), tcu::sw128_desc(b1 + off),
-                                       idesc, 1u);
-                            mma2<MODE>(td, tcu::sw128_desc(a1 + off), tcu::sw128_desc(b0 + off),
-                                       idesc, 1u);
+                            mma2<MODE>(td, swz_desc<RB>(a0 + off), swz_desc<RB>(b1 + off), idesc, 1u);
+                            mma2<MODE>(td, swz_desc<RB>(a1 + off), swz_desc<RB>(b0 + off), idesc, 1u);
                         }
                     }
                     tcu::mma_commit(&empty[s]);
@@ -292,7 +307,7 @@ k_hilbert_tc2(const __grid_constant__ CUtensorMap tA0, const __grid_constant__ C
 }
 
 Status make_map2(CUtensorMap* m, const void* base, bool bf16, uint64_t inner, uint64_t rows,
-                 uint64_t row_stride_elems, uint32_t box_inner, uint32_t box_rows) {
+                 uint64_t row_stride_elems, uint32_t box_inner, uint32_t box_rows, int row_bytes) {
     auto enc = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(tensor_map_encoder());
     if (!enc) return make_status(CTRECON_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
     const uint64_t esz = bf16 ? 2 : 4;
@@ -302,7 +317,8 @@ Status make_map2(CUtensorMap* m, const void* base, bool bf16, uint64_t inner, ui
     cuuint32_t estr[2] = {1, 1};
     CUresult r = enc(m, bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
                      2, const_cast<void*>(base), dims, strides, box, estr,
-                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     row_bytes == 128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS)
         return make_status(CTRECON_ERR_CUDA,
@@ -420,26 +436,30 @@ Status launch_hilbert_tc2(ctrecon_ctx* ctx, cudaStream_t s, FilterPlan& plan, co
     const int vpt = hilbert_tc_views_per_tile(AL);
     const int ntile = (vpt * AL + 15) / 16 * 16;
     const int YLh = YLp / 2, YLhA = (YLh + kM2 - 1) / kM2 * kM2;
-    const uint32_t kin = bf ? 64 : 32;
+    // BF16x3 stages hold four operand tiles: 64-byte rows (32 elements of K) let five stages fit
+    // where 128-byte rows let two; TF32 keeps 128-byte rows (32 elements, one plane)
+    const int RB = bf ? 64 : 128;
+    const uint32_t kin = (uint32_t)RB / (bf ? 2 : 4);
     const uint64_t rows = (uint64_t)nviews * AL;
     const size_t plane = (size_t)rows * YLp * (bf ? 2 : 4);
     CUtensorMap tA0, tA1, tB0, tB1;
-    CTR_TRY(make_map2(&tA0, plan.tc2T0.ptr, bf, YLh, (uint64_t)2 * YLhA, YLh, kin, kM2));
+    CTR_TRY(make_map2(&tA0, plan.tc2T0.ptr, bf, YLh, (uint64_t)2 * YLhA, YLh, kin, kM2, RB));
     CTR_TRY(make_map2(&tA1, bf ? plan.tc2T1.ptr : plan.tc2T0.ptr, bf, YLh, (uint64_t)2 * YLhA, YLh,
-                      kin, kM2));
-    CTR_TRY(make_map2(&tB0, X, bf, YLp, rows, YLp, kin, ntile));
+                      kin, kM2, RB));
+    CTR_TRY(make_map2(&tB0, X, bf, YLp, rows, YLp, kin, ntile, RB));
     CTR_TRY(make_map2(&tB1, bf ? (const void*)((const char*)X + plane) : X, bf, YLp, rows, YLp,
-                      kin, ntile));
+                      kin, ntile, RB));
     Tc2Params p;
     p.AL = AL; p.YL = YL; p.ZL = ZL; p.nviews = nviews; p.vpt = vpt; p.ntile = ntile;
     p.YLh = YLh; p.YLhA = YLhA;
     p.nk = YLh / (int)kin;
+    p.kin = (int)kin;
     p.ncb = YLhA / kM2;
     const int nvg = (nviews + vpt - 1) / vpt;
     p.ntiles = nvg * p.ncb * 2;
     const int PL = bf ? 2 : 1;
-    p.a_bytes = kM2 * 128;
-    p.b_bytes = ntile * 128;
+    p.a_bytes = kM2 * RB;
+    p.b_bytes = ntile * RB;
     p.stage_bytes = PL * (p.a_bytes + p.b_bytes);
     const size_t budget = 227 * 1024 - 1024 - 256;  // alignment slack and barriers
     p.S = (int)std::min<size_t>(6, budget / (size_t)p.stage_bytes);
@@ -452,13 +472,13 @@ Status launch_hilbert_tc2(ctrecon_ctx* ctx, cudaStream_t s, FilterPlan& plan, co
     const size_t smem = (size_t)p.bar_off + 256 + 1024;
     const int grid = std::min(p.ntiles, sm_count());
     if (bf) {
-        CTR_CUDA(cudaFuncSetAttribute(k_hilbert_tc2<CTRECON_HILBERT_BF16X3>,
+        CTR_CUDA(cudaFuncSetAttribute(k_hilbert_tc2<CTRECON_HILBERT_BF16X3, 64>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_hilbert_tc2<CTRECON_HILBERT_BF16X3><<<grid, kThreads2, smem, s>>>(tA0, tA1, tB0, tB1, p);
+        k_hilbert_tc2<CTRECON_HILBERT_BF16X3, 64><<<grid, kThreads2, smem, s>>>(tA0, tA1, tB0, tB1, p);
     } else {
-        CTR_CUDA(cudaFuncSetAttribute(k_hilbert_tc2<CTRECON_HILBERT_TF32>,
+        CTR_CUDA(cudaFuncSetAttribute(k_hilbert_tc2<CTRECON_HILBERT_TF32, 128>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_hilbert_tc2<CTRECON_HILBERT_TF32><<<grid, kThreads2, smem, s>>>(tA0, tA1, tB0, tB1, p);
+        k_hilbert_tc2<CTRECON_HILBERT_TF32, 128><<<grid, kThreads2, smem, s>>>(tA0, tA1, tB0, tB1, p);
     }
     CTR_CUDA(cudaGetLastError());
     return Status::Ok();
