@@ -50,7 +50,7 @@ constexpr int kM2 = 128;
 constexpr int kEpiWarps = 16;               // four per TMEM lane quarter
 constexpr int kThreads2 = 32 * (2 + kEpiWarps);
 constexpr int kAccCols = 256;               // one accumulator buffer
-constexpr int kRowsAhead = 8;               // backward-rebin entries loaded ahead per warp
+constexpr int kRowsAhead = 4;               // backward-rebin entries loaded ahead per warp
 
 struct Tc2Params {
     int AL, YL, ZL, nviews, vpt, ntile, YLh, YLhA, nk, ncb, ntiles, S;
@@ -120,6 +120,22 @@ template <int RB>
 __device__ __forceinline__ uint64_t swz_desc(uint32_t saddr) {
     if constexpr (RB == 128) return tcu::sw128_desc(saddr);
     else return sw64_desc(saddr);
+}
+
+// four rows' 4-column windows in flight behind one wait (the loaded registers pass through the
+// wait, so no use of them can be scheduled before it)
+__device__ __forceinline__ void tmem_ld4_nowait(uint32_t taddr, uint32_t* r) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld16(uint32_t* r) {
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]),
+                   "+r"(r[6]), "+r"(r[7]), "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]),
+                   "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15])
+                 :
+                 : "memory");
 }
 
 __device__ __forceinline__ float pick4(int d, float v0, float v1, float v2, float v3) {
@@ -270,29 +286,51 @@ k_hilbert_tc2(const __grid_constant__ CUtensorMap tA0, const __grid_constant__ C
                     const int k = k0 + 4 * r;
                     e[r] = k < p.ZL ? __ldg(bkrow + (size_t)k * zstride) : make_int4(0, 0, 0, 0);
                 }
+                // rows past ZL (warp-uniform) read a harmless window and store nothing
+                int lo[kRowsAhead], hi[kRowsAhead];
 #pragma unroll
                 for (int r = 0; r < kRowsAhead; ++r) {
-                    const int k = k0 + 4 * r;
-                    if (k >= p.ZL) break;  // warp-uniform
-                    const int rb = e[r].x, re = e[r].y;
-                    const float gb = __int_as_float(e[r].z), ge = __int_as_float(e[r].w);
-                    const int lo = __reduce_min_sync(0xffffffffu, (unsigned)min(rb, re));
-                    const int hi = __reduce_max_sync(0xffffffffu, (unsigned)max(rb, re));
-                    for (int vl = 0; vl < nv; ++vl) {
-                        const int cbase = vl * p.AL;  // this view's first accumulator column
-                        float vb = 0.f, ve = 0.f;
-                        for (int w = lo; w <= hi; w += 4) {
-                            // window of 4 columns, kept inside the 256-column buffer
-                            const int c0 = min(cbase + w, kAccCols - 4);
-                            float v0, v1, v2, v3;
-                            tmem_ld4(acc_base + (uint32_t)c0, v0, v1, v2, v3);
-                            const int db = cbase + rb - c0, de = cbase + re - c0;
-                            if (db >= 0 && db < 4) vb = pick4(db, v0, v1, v2, v3);
-                            if (de >= 0 && de < 4) ve = pick4(de, v0, v1, v2, v3);
+                    lo[r] = (int)__reduce_min_sync(0xffffffffu, (unsigned)min(e[r].x, e[r].y));
+                    hi[r] = (int)__reduce_max_sync(0xffffffffu, (unsigned)max(e[r].x, e[r].y));
+                }
+                for (int vl = 0; vl < nv; ++vl) {
+                    const int cbase = vl * p.AL;  // this view's first accumulator column
+#pragma unroll
+                    for (int r4 = 0; r4 < kRowsAhead; r4 += 4) {
+                        // the first 4-column window of four rows (kept inside the 256-column
+                        // buffer), one wait for all four
+                        uint32_t w[16];
+                        int c0[4];
+#pragma unroll
+                        for (int r = 0; r < 4; ++r) {
+                            c0[r] = min(cbase + lo[r4 + r], kAccCols - 4);
+                            tmem_ld4_nowait(acc_base + (uint32_t)c0[r], w + 4 * r);
                         }
-                        if (valid)
-                            p.out[(size_t)(vg * p.vpt + vl) * vstride + (size_t)k * p.YL + i] =
-                                fmaf(gb, vb, ge * ve);
+                        tmem_wait_ld16(w);
+#pragma unroll
+                        for (int r = 0; r < 4; ++r) {
+                            const int k = k0 + 4 * (r4 + r);
+                            const int4 er = e[r4 + r];
+                            const int db = cbase + er.x - c0[r], de = cbase + er.y - c0[r];
+                            const float v0 = __uint_as_float(w[4 * r]);
+                            const float v1 = __uint_as_float(w[4 * r + 1]);
+                            const float v2 = __uint_as_float(w[4 * r + 2]);
+                            const float v3 = __uint_as_float(w[4 * r + 3]);
+                            float vb = (db >= 0 && db < 4) ? pick4(db, v0, v1, v2, v3) : 0.f;
+                            float ve = (de >= 0 && de < 4) ? pick4(de, v0, v1, v2, v3) : 0.f;
+                            // rows spanning more than four kappa rows (warp-uniform): more windows
+                            for (int ww = lo[r4 + r] + 4; ww <= hi[r4 + r]; ww += 4) {
+                                const int cw = min(cbase + ww, kAccCols - 4);
+                                float u0, u1, u2, u3;
+                                tmem_ld4(acc_base + (uint32_t)cw, u0, u1, u2, u3);
+                                const int db2 = cbase + er.x - cw, de2 = cbase + er.y - cw;
+                                if (db2 >= 0 && db2 < 4) vb = pick4(db2, u0, u1, u2, u3);
+                                if (de2 >= 0 && de2 < 4) ve = pick4(de2, u0, u1, u2, u3);
+                            }
+                            if (valid && k < p.ZL)
+                                p.out[(size_t)(vg * p.vpt + vl) * vstride + (size_t)k * p.YL + i] =
+                                    fmaf(__int_as_float(er.z), vb, __int_as_float(er.w) * ve);
+                        }
                     }
                 }
             }
