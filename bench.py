@@ -17,9 +17,11 @@ time). Beside it, on the same resident inputs: `forms.mixed_learned` (BF16x3 ten
 Hilbert, the learned PI start) and `forms.mixed_learned_batched` (the same for two copies of the
 scan in one batch: one persistent backprojection launch over both, replayed as a CUDA graph),
 each with `vs_plain`; `accuracy` gives every form's relative RMSE and max-abs against the FP64
-oracle of the whole chain on a central 48^3 block. `e2e` is the plain form through the
-MEX-equivalent host calls (FP64 pinned host buffers, copies in the timed region) and
-`e2e_pageable` through the MEX modules themselves with pageable FP64 arrays, as MATLAB calls them.
+oracle of the whole chain on a central 48^3 block. `e2e` is the plain form end to end through
+the C ABI's whole-chain call `ctrecon_recon_host_f64` (FP64 pinned host buffers, copies in the
+timed region); `e2e_mex_pinned` through the two MEX-equivalent calls (FProj comes down and goes
+back up in between) and `e2e_pageable` through the MEX modules themselves with pageable FP64
+arrays, as MATLAB calls them.
 `roofline` is the backprojection kernel's (the dominant one) against its issue limit;
 `kernels` gives every kernel's time and roofline fraction, from CUDA events around each launch.
 
@@ -1233,7 +1235,7 @@ def run_headline(args):
     ctx.set_option(_lib.OPT_PI_SOLVER, pi_of[args.pi])
 
     # ---- e2e through the MEX-equivalent host calls (FP64 pinned host buffers) -----------------
-    e2e = e2e_pageable = None
+    e2e = e2e_mex = e2e_pageable = None
     nproj, nvox = int(np.prod(s.proj_shape)), int(np.prod(s.vol_shape))
     if not args.no_e2e:
         h_proj = torch.empty(s.proj_shape, dtype=torch.float64, pin_memory=True)
@@ -1241,22 +1243,36 @@ def run_headline(args):
         h_fproj = torch.empty_like(h_proj).pin_memory()
         h_img = torch.zeros(s.vol_shape, dtype=torch.float64).pin_memory()
         np_proj, np_fproj, np_img = h_proj.numpy(), h_fproj.numpy(), h_img.numpy()
+        e2e_steps = max(1, min(args.steps, 3))
+        # the whole chain in one call: FP64 projections up (pipelined with the filter), FProj
+        # kept on the device, the FP64 image up (untouched voxels keep their values) and down
+        ctx.recon_host(fpar, geom, np_proj, np_img)
+        barrier(ws)
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            ctx.recon_host(fpar, geom, np_proj, np_img)
+        t_e2e = max_over_ranks((time.perf_counter() - t0) / e2e_steps, ws)
+        e2e = {"value": ws * updates / t_e2e / 1e9, "unit": "GUPS",
+               "h2d_bytes_per_step": 8 * (nproj + nvox), "d2h_bytes_per_step": 8 * nvox,
+               "s_per_vol": t_e2e, "steps": e2e_steps,
+               "path": "ctrecon_recon_host_f64 (filter + backprojection in one call, "
+                       "FunctionKat_v6.m:85-113 without the FProj round trip), pinned FP64 host "
+                       "buffers"}
+        # the two MEX-equivalent calls, FProj through the host in between
         ctx.filter_host(fpar, np_proj, np_fproj)
         ctx.bkproj_host(geom, np_fproj, np_img)
-        e2e_steps = max(1, min(args.steps, 3))
         barrier(ws)
         t0 = time.perf_counter()
         for _ in range(e2e_steps):
             ctx.filter_host(fpar, np_proj, np_fproj)       # KatsevichFiltering_GPU
             ctx.bkproj_host(geom, np_fproj, np_img)        # KatsevichBkProj_GPU
-        t_e2e = (time.perf_counter() - t0) / e2e_steps
-        t_e2e = max_over_ranks(t_e2e, ws)
-        e2e = {"value": ws * updates / t_e2e / 1e9, "unit": "GUPS",
-               "h2d_bytes_per_step": 8 * (2 * nproj + nvox),
-               "d2h_bytes_per_step": 8 * (nproj + nvox),
-               "s_per_vol": t_e2e, "steps": e2e_steps,
-               "path": "ctrecon_filter_host_f64 + ctrecon_bkproj_host_f64 (MEX-equivalent), "
-                       "pinned FP64 host buffers"}
+        t_mex = max_over_ranks((time.perf_counter() - t0) / e2e_steps, ws)
+        e2e_mex = {"value": ws * updates / t_mex / 1e9, "unit": "GUPS",
+                   "h2d_bytes_per_step": 8 * (2 * nproj + nvox),
+                   "d2h_bytes_per_step": 8 * (nproj + nvox), "s_per_vol": t_mex,
+                   "steps": e2e_steps,
+                   "path": "ctrecon_filter_host_f64 + ctrecon_bkproj_host_f64 (the two MEX "
+                           "calls' C ABI), pinned FP64 host buffers"}
         del h_fproj, h_img
         # the MEX modules themselves, with pageable FP64 arrays as MATLAB passes them
         # (FunctionKat_v6.m:85-113: FProj = Proj then KatsevichFiltering_GPU writes in place)
@@ -1361,7 +1377,8 @@ def run_headline(args):
                 "phase_ms": plain["phase_ms"],
                 "bkproj_gups": updates / (plain["phase_ms"]["bkproj"] / 1e3) / 1e9,
                 "gpu_launches": launches,
-                "e2e": e2e, "e2e_pageable": e2e_pageable, "roofline": roofline,
+                "e2e": e2e, "e2e_mex_pinned": e2e_mex, "e2e_pageable": e2e_pageable,
+                "roofline": roofline,
                 "kernels": kern, "cpu_baseline": cpu, "clocks": clocks,
                 "forms": {k: {kk: vv for kk, vv in v.items() if kk != "kernel_times"}
                           for k, v in forms.items()},

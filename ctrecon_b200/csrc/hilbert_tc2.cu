@@ -154,7 +154,7 @@ __device__ __forceinline__ void tile_coords(const Tc2Params& p, int t, int& vg, 
 }
 
 template <int MODE, int RB>
-__global__ void __launch_bounds__(kThreads2, 1)
+__global__ void __maxnreg__(112)
 k_hilbert_tc2(const __grid_constant__ CUtensorMap tA0, const __grid_constant__ CUtensorMap tA1,
               const __grid_constant__ CUtensorMap tB0, const __grid_constant__ CUtensorMap tB1,
               Tc2Params p) {
@@ -279,12 +279,20 @@ k_hilbert_tc2(const __grid_constant__ CUtensorMap tA0, const __grid_constant__ C
             const int4* bkrow = bk4 + (size_t)par * p.YLhA + ip;
             const size_t zstride = (size_t)2 * p.YLhA;
             const uint32_t acc_base = lane_base + (uint32_t)(b * kAccCols);
+            // the entries of the next kRowsAhead rows are loaded while this batch is processed
+            int4 enext[kRowsAhead];
+#pragma unroll
+            for (int r = 0; r < kRowsAhead; ++r) {
+                const int k = h + 4 * r;
+                enext[r] = k < p.ZL ? __ldg(bkrow + (size_t)k * zstride) : make_int4(0, 0, 0, 0);
+            }
             for (int k0 = h; k0 < p.ZL; k0 += 4 * kRowsAhead) {
                 int4 e[kRowsAhead];
 #pragma unroll
                 for (int r = 0; r < kRowsAhead; ++r) {
-                    const int k = k0 + 4 * r;
-                    e[r] = k < p.ZL ? __ldg(bkrow + (size_t)k * zstride) : make_int4(0, 0, 0, 0);
+                    e[r] = enext[r];
+                    const int k = k0 + 4 * kRowsAhead + 4 * r;
+                    enext[r] = k < p.ZL ? __ldg(bkrow + (size_t)k * zstride) : make_int4(0, 0, 0, 0);
                 }
                 // rows past ZL (warp-uniform) read a harmless window and store nothing
                 int lo[kRowsAhead], hi[kRowsAhead];

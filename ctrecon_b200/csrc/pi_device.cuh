@@ -30,7 +30,10 @@ __device__ __forceinline__ void pi_bisect(double x, double y, double z, double* 
     bmin = bmax - 2 * PI;
     double sb = 0, st = 0;
     int it = 0;
-    while (((bmax - bmin) > kPiTol) && (delta > kPiTol)) {
+    // the reference's loop test ((bmax - bmin) > DeltaMax) && (delta > DeltaMax): the bracket
+    // starts 2 pi wide and halves each step, so its width test holds for the first 25 steps
+    // (2 pi / 2^25 > 1e-7) and is only evaluated from then on
+    while ((it < 25 || (bmax - bmin) > kPiTol) && (delta > kPiTol)) {
         sb = (bmax + bmin) * 0.5;
         double zz = pi_chord(x, y, r2, sb, &st);
         if (zz < z) bmin = sb;
@@ -128,7 +131,8 @@ __device__ __forceinline__ int pi_bisect_replay(double x, double y, double z, do
     double sb = 0, st = 0;
     bool have_st = false;
     int ev = 0;
-    while (((bmax - bmin) > kPiTol) && (delta > kPiTol)) {
+    // the width test holds for the first 25 steps (as in pi_bisect)
+    for (int it = 0; (it < 25 || (bmax - bmin) > kPiTol) && (delta > kPiTol); ++it) {
         sb = (bmax + bmin) * 0.5;
         const double dl = sb - tau;
         double g = dz * dl;  // ~ zz(sb) - z
