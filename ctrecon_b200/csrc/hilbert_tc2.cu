@@ -154,7 +154,7 @@ __device__ __forceinline__ void tile_coords(const Tc2Params& p, int t, int& vg, 
 }
 
 template <int MODE, int RB>
-__global__ void __maxnreg__(112)
+__global__ void __launch_bounds__(kThreads2, 1)
 k_hilbert_tc2(const __grid_constant__ CUtensorMap tA0, const __grid_constant__ CUtensorMap tA1,
               const __grid_constant__ CUtensorMap tB0, const __grid_constant__ CUtensorMap tB1,
               Tc2Params p) {
