@@ -413,6 +413,11 @@ ctrecon_status ctrecon_set_option(ctrecon_ctx* ctx, ctrecon_option opt, int valu
             return finish(ctx, make_status(CTRECON_ERR_INVALID_ARGUMENT, "bad tensor-core form"));
         ctx->opt_tc_form = value;
         break;
+    case CTRECON_OPT_K1_FORM:
+        if (value != CTRECON_K1_STAGED && value != CTRECON_K1_PER_VIEW)
+            return finish(ctx, make_status(CTRECON_ERR_INVALID_ARGUMENT, "bad K1 form"));
+        ctx->opt_k1_form = value;
+        break;
     default: return finish(ctx, make_status(CTRECON_ERR_INVALID_ARGUMENT, "unknown option"));
     }
     return finish(ctx, Status::Ok());
@@ -431,6 +436,7 @@ ctrecon_status ctrecon_get_option(const ctrecon_ctx* ctx, ctrecon_option opt, in
     case CTRECON_OPT_PINET_MODE: *value = ctx->opt_pinet_mode; break;
     case CTRECON_OPT_KERNEL_TIMING: *value = ctx->opt_kernel_timing; break;
     case CTRECON_OPT_TC_FORM: *value = ctx->opt_tc_form; break;
+    case CTRECON_OPT_K1_FORM: *value = ctx->opt_k1_form; break;
     default: return CTRECON_ERR_INVALID_ARGUMENT;
     }
     return CTRECON_OK;

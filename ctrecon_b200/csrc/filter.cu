@@ -401,7 +401,6 @@ Status launch_filter(ctrecon_ctx* ctx, cudaStream_t s, FilterPlan& plan, const f
                      int view_begin, int view_end) {
     const FilterTables& t = plan.t;
     const int YL = t.YL, ZL = t.ZL, AL = t.AL, YLp = plan.YLp, P = t.P;
-    (void)proj_nviews;
     const int mode = ctx->opt_hilbert;
     const int chunk = std::max(1, ctx->opt_filter_chunk);
     // 4 bytes per kappa sample in every format (FP32, TF32, or BF16 hi + lo planes), for the
@@ -425,7 +424,11 @@ Status launch_filter(ctrecon_ctx* ctx, cudaStream_t s, FilterPlan& plan, const f
         dres = plan.dres.as<DresCol>();
     }
 
-    {  // K1 launch shape, checked before any launch
+    // K1: the staged form where it applies (chain-rule derivative), else the per-view form,
+    // whose launch shape is checked before any launch
+    const bool staged = ctx->opt_k1_form == CTRECON_K1_STAGED && !dres &&
+                        k1_staged_fits(YL, ZL, AL, YLp, d_proj);
+    if (!staged) {
         int tj;
         size_t smem1;
         CTR_TRY(k1_shape(ZL, &tj, &smem1));
@@ -441,9 +444,16 @@ Status launch_filter(ctrecon_ctx* ctx, cudaStream_t s, FilterPlan& plan, const f
         const size_t plane = (size_t)n * AL * YLp;
         {
             KernelTimer tm(ctx, s, kKDerivRebin);
-            CTR_TRY(launch_k1(s, d_proj, proj_view0, P, YL, ZL, AL, YLp, c0, n,
-                              plan.fw.as<FwEntry>(), plan.cuy.as<float2>(), plan.zcv.as<float>(),
-                              plan.inv2dl, dres, (float)t.DeltaL, X, plane, mode));
+            if (staged)
+                CTR_TRY(launch_k1_staged(ctx, s, d_proj, proj_view0, proj_nviews, P, YL, ZL, AL,
+                                         YLp, c0, n, plan.fw.as<FwEntry>(),
+                                         plan.cuy.as<float2>(), plan.zcv.as<float>(),
+                                         plan.inv2dl, X, plane, mode));
+            else
+                CTR_TRY(launch_k1(s, d_proj, proj_view0, P, YL, ZL, AL, YLp, c0, n,
+                                  plan.fw.as<FwEntry>(), plan.cuy.as<float2>(),
+                                  plan.zcv.as<float>(), plan.inv2dl, dres, (float)t.DeltaL, X,
+                                  plane, mode));
         }
         float* out = d_fproj + (size_t)(c0 - out_view0) * YL * ZL;
         if (mode == CTRECON_HILBERT_FP32) {

@@ -241,6 +241,7 @@ struct ctrecon_ctx {
     int opt_pinet_mode = CTRECON_PINET_GRID;  // CTRECON_OPT_PINET_MODE
     int opt_kernel_timing = 0;                // CTRECON_OPT_KERNEL_TIMING
     int opt_tc_form = CTRECON_TC_PARITY_SPLIT;  // CTRECON_OPT_TC_FORM
+    int opt_k1_form = CTRECON_K1_STAGED;        // CTRECON_OPT_K1_FORM
     std::vector<ctr::KernelSpan> kspans;      // timed launches since the last query
     std::vector<cudaEvent_t> kev_free;        // timing events for reuse
     cudaStream_t host_stream = nullptr;  // stream for the synchronous host calls
@@ -311,6 +312,14 @@ constexpr int kMaxBPVariant = 12;
 Status selftest_bounded_wait(ctrecon_ctx* ctx, cudaStream_t s, int limit_ms);
 // the driver's cuTensorMapEncodeTiled (nullptr when unavailable), hilbert_tc.cu
 void* tensor_map_encoder();
+// K1 with its projection rows staged by tensor copies (k1_staged.cu): whether it applies to a
+// shape and buffer, and its launch over views [c0, c0 + n) of a buffer holding views
+// [proj_view0, proj_view0 + proj_nviews); the kappa rows are bit-identical to k_deriv_rebin's.
+bool k1_staged_fits(int YL, int ZL, int AL, int YLp, const void* d_proj);
+Status launch_k1_staged(ctrecon_ctx* ctx, cudaStream_t s, const float* d_proj, int proj_view0,
+                        int proj_nviews, int P, int YL, int ZL, int AL, int YLp, int c0, int n,
+                        const FwEntry* fw, const float2* cuy, const float* zcv, float inv2dl,
+                        void* X, size_t plane, int mode);
 // Fifth form building blocks (bkproj2.cu): the box-map table over cell records of `nviews`
 // views (kBoxMaps CUtensorMap entries written to `out`, host memory), the records of views
 // [p0, p0 + nviews) of fproj, and the capacity (records per staged view) of a plan.

@@ -139,7 +139,8 @@ typedef enum ctrecon_option {
     CTRECON_OPT_KERNEL_TIMING = 9,    /* 1: time every kernel launch of the single-scan entry
                                          points with CUDA events on its stream (read with
                                          ctrecon_kernel_times); default 0 */
-    CTRECON_OPT_TC_FORM = 10          /* form of the tensor-core Hilbert: CTRECON_TC_* below */
+    CTRECON_OPT_TC_FORM = 10,         /* form of the tensor-core Hilbert: CTRECON_TC_* below */
+    CTRECON_OPT_K1_FORM = 11          /* form of the derivative + forward rebin: CTRECON_K1_* */
 } ctrecon_option;
 
 /* CTRECON_OPT_TC_FORM. Both forms compute the same sums to FP32 rounding. */
@@ -150,6 +151,16 @@ enum {
                                     with the next tile's MMAs; views of up to 256 kappa rows */
     CTRECON_TC_SINGLE_PASS = 1   /* one full-size product per tile, then its backward rebin; also
                                     the form used for views of more than 256 kappa rows */
+};
+
+/* CTRECON_OPT_K1_FORM. Both forms write the same kappa rows bit for bit. */
+enum {
+    CTRECON_K1_STAGED = 0,  /* default: a CTA per (32-column strip, run of views) walks its
+                               views in order, each view's rows copied in once by a tensor
+                               copy, the strip's rebin entries held in shared memory; used
+                               where it applies (chain-rule derivative, YL a multiple of 4, at
+                               most 256 detector rows), else the per-view form */
+    CTRECON_K1_PER_VIEW = 1 /* a CTA per (view, 128 columns), rows read from device memory */
 };
 
 /* ---- context ---------------------------------------------------------------------- */

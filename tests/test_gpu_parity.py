@@ -150,6 +150,41 @@ def test_filter_tensor_core_forms_agree(torch_mod, oracle_mod, yl, zl, chunk, mo
     assert d < bound
 
 
+@pytest.mark.parametrize("yl,zl,chunk", [(300, 16, 2048), (300, 40, 7), (256, 16, 100),
+                                          (736, 64, 33), (132, 8, 5), (130, 40, 7)])
+@pytest.mark.parametrize("mode", ["fp32", "bf16x3", "tf32"])
+def test_k1_forms_bit_identical(torch_mod, oracle_mod, yl, zl, chunk, mode):
+    """The staged K1 (tensor copies of 32-column strips, views walked in order, default) and
+    the per-view K1 write the same kappa rows bit for bit, so the filtered projections of every
+    Hilbert form agree exactly; both against the FP64 oracle. Shapes: ragged strips (300 and
+    132 columns: a partial last strip and zero-padded columns), chunks of 7, 33 and 5 views
+    (runs of one view, and chunks with fewer views than runs), eight detector rows (half of
+    them under the v stencil's edge rule), 40 rows (a warp's second block of rows holds the
+    last one), the c2 detector width, and 130 columns, where the staged form does not apply
+    (rows of 520 bytes) and both settings run the per-view form."""
+    import ctrecon_b200 as ct
+    from ctrecon_b200 import _lib
+    from ctrecon_b200.geometry import small_config
+    s = small_config(name="ragged", YL=yl, ZL=zl, views_per_turn=90, turns=1.3, NX=24, NY=24,
+                     NZ=8)
+    O = oracle_mod
+    proj = O.project_ellipsoids(oracle_geom(O, s), s.ellipsoids())
+    ref = O.katsevich_filter(oracle_filter_params(O, s), proj)
+    m = {"fp32": ct.HILBERT_FP32, "bf16x3": ct.HILBERT_BF16X3, "tf32": ct.HILBERT_TF32}[mode]
+    bound = {"fp32": 1e-5, "bf16x3": 1e-4, "tf32": 2e-3}[mode]
+    out = {}
+    for form in (_lib.K1_STAGED, _lib.K1_PER_VIEW):
+        with ct.Context(0, hilbert=m) as cx:
+            cx.set_option(_lib.OPT_K1_FORM, form)
+            assert cx.get_option(_lib.OPT_K1_FORM) == form
+            cx.set_option(_lib.OPT_FILTER_CHUNK, chunk)
+            out[form] = cx.filter_host(ct.scan_filter_params(s), proj)
+        err = rel_rmse(out[form], ref)
+        print(f"filter {zl}x{yl} {mode} K1 form {form}: rel RMSE {err:.3e}")
+        assert err < bound
+    assert np.array_equal(out[_lib.K1_STAGED], out[_lib.K1_PER_VIEW])
+
+
 def test_chain_c1_bf16x3_matches_oracle(torch_mod, c1_case):
     import ctrecon_b200 as ct
     s = c1_case["s"]
