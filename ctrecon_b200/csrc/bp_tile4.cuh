@@ -126,6 +126,9 @@ struct Shared4 {
     // (kMagicBits + v0) * W16, W16 = row stride in bytes}, so that a consumer's cell base is
     // bits(u + kMagic) * 16 + kb
     int2 kw[S][NB];
+    // per consumer warp and slice: warp-wide view ranges {lo, hi} (some lane's voxel has a PI
+    // interval there) and {flo, fhi} (every lane's voxel has weight 1 there)
+    int4 sr[8][8];
     Foot3 pfoot[2][NB];  // producer side: footprints of the blocks being staged
     float4 pvg[2][NB];
     int s_pmin, s_pmax, s_abort;
@@ -384,39 +387,37 @@ __device__ __forceinline__ uint32_t tile4(const BPParams& kp, const float* __res
         }
     } else {
         // ------------------------------------------------------------------ consumers
-        const float X = col_ok ? xc[x] : 0.f, Y = col_ok ? yc[y] : 0.f;
+        // a lane past the volume's edge takes the nearest column of the tile: its reads stay in
+        // the staged footprint, and its voxels are never written
+        const float X = xc[min(x, NX - 1)], Y = yc[min(y, NY - 1)];
         const float z0 = zc[zb];
         const float dzf = kp.dzf;
         const float HalfYm = HalfY - 0.5f, HalfZm = HalfZ - 0.5f;
-        // Slices 4h .. 4h + 3 form group h. A group takes the unweighted path at a view when
-        // every voxel of the group, in every lane of the warp, has weight 1 there: [gflo[h],
-        // gfhi[h]] is that warp-wide view range (empty if any voxel of the group has no PI
-        // interval). A block whose views all lie in both groups' ranges skips the per-view
-        // tests. Deciding per group halves the views whose weights are tested: the PI ranges of
-        // a column's slices are shifted against each other.
-        constexpr int GS = 4, NG = TZ / GS;
-        int gflo[NG], gfhi[NG];
+        // Per slice k, warp-wide view ranges: [lo, hi] where some lane's voxel of the slice has
+        // its PI interval (p in [bi, ti + 1]), [flo, fhi] where every lane's voxel has weight 1
+        // (p in [bi + 2, ti - 1], both ramp views of each end excluded). Each block of views then gives every slice one of three warp-uniform
+        // classes: no update, the unweighted update, or the checked (weighted) one. Deciding
+        // per slice and per block keeps the blocks at the ends of the PI intervals close to the
+        // unweighted blocks' cost: the PI ranges of a column's slices are shifted against each
+        // other, so in those blocks most slices are wholly inside or wholly outside.
+        // Only lanes whose voxel has an interval count: the others (outside the reconstructed
+        // cylinder or the volume) are never written, so whatever they accumulate is dropped.
 #pragma unroll
-        for (int h = 0; h < NG; ++h) {
-            int lo = INT_MIN, hi = INT_MAX;
-            bool ok = col_ok;
-#pragma unroll
-            for (int k = h * GS; k < (h + 1) * GS; ++k) {
-                ok = ok && vr.bi[k] != kPiInvalid;
-                if (ok) {
-                    lo = max(lo, vr.bi[k] + 2);  // past both B-side ramp views
-                    hi = min(hi, vr.ti[k] - 1);  // before both T-side ramp views
-                }
-            }
-            if (!ok) { lo = INT_MAX; hi = INT_MIN; }
+        for (int k = 0; k < TZ; ++k) {
+            const bool v = col_ok && vr.bi[k] != kPiInvalid;
+            int lo = v ? vr.bi[k] : INT_MAX, hi = v ? vr.ti[k] + 1 : INT_MIN;
+            int flo = v ? vr.bi[k] + 2 : INT_MIN, fhi = v ? vr.ti[k] - 1 : INT_MAX;
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) {
-                lo = max(lo, __shfl_xor_sync(0xffffffffu, lo, o));
-                hi = min(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+                lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+                hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+                flo = max(flo, __shfl_xor_sync(0xffffffffu, flo, o));
+                fhi = min(fhi, __shfl_xor_sync(0xffffffffu, fhi, o));
             }
-            gflo[h] = lo;
-            gfhi[h] = hi;
+            if (lo > hi) { flo = INT_MAX; fhi = INT_MIN; }  // no lane with an interval
+            if (lane == 0) sh.sr[warp][k] = make_int4(lo, hi, flo, fhi);
         }
+        __syncwarp();
         // one voxel's update from cell records, weighted (w) or not
         auto cell_update = [&](int k, float dz0, float kv, float r2, uint64_t a2, uint32_t W16,
                                uint32_t cbase) {
@@ -452,8 +453,10 @@ __device__ __forceinline__ uint32_t tile4(const BPParams& kp, const float* __res
             const int d1 = vr.ti[k] + 1 - p;
             if ((d0 | d1) < 0) return;
             float w = 1.f;
-            if (d1 <= 1) w = ramp(vr.tf[k] + (float)(d1 - 1));
-            else if (d0 <= 1) w = ramp((float)d0 - vr.bf[k]);
+            // the two views at each end of the interval (the fractions reread from the PI table,
+            // which keeps them out of registers)
+            if (d1 <= 1) w = ramp(__ldg(&pit[colbase + zb + k].tf) + (float)(d1 - 1));
+            else if (d0 <= 1) w = ramp((float)d0 - __ldg(&pit[colbase + zb + k].bf));
             const float dz = fmaf((float)k, dzf, dz0);
             const float v = fmaf(dz, kv, HalfZm);
             const float rinv = rsqrt_approx(fmaf(dz, dz, r2));
@@ -468,15 +471,21 @@ __device__ __forceinline__ uint32_t tile4(const BPParams& kp, const float* __res
                 sh.s_abort = 1;
                 break;
             }
-            const int pb = pmin + ib * NB;
-            bool blk = pb + NB - 1 <= pmax;  // a whole block of views with cell records
+            const int pb = pmin + ib * NB, pe = pb + NB - 1;
+            bool blk = pe <= pmax;  // a whole block of views with cell records
 #pragma unroll
             for (int j = 0; j < NB; ++j) blk = blk && (sh.foot[slot][j].W > 0);
-            bool all_fast = blk;  // every group unweighted for the whole block (warp-uniform)
+            // 2 bits per slice: 0 no update in this block, 1 unweighted, 2 weighted
+            uint32_t cls = 0;
+            if (blk) {
 #pragma unroll
-            for (int h = 0; h < NG; ++h)
-                all_fast = all_fast && pb >= gflo[h] && pb + NB - 1 <= gfhi[h];
-            if (all_fast) {
+                for (int k = 0; k < TZ; ++k) {
+                    const int4 r = sh.sr[warp][k];
+                    const uint32_t c = (pe < r.x || pb > r.y) ? 0u : ((pb >= r.z && pe <= r.w) ? 1u : 2u);
+                    cls |= c << (2 * k);
+                }
+            }
+            if (blk && cls == 0x5555u) {
                 // every view of the block has cell records and weight 1 for all voxels of the
                 // warp: no per-view tests
 #pragma unroll
@@ -505,7 +514,45 @@ __device__ __forceinline__ uint32_t tile4(const BPParams& kp, const float* __res
                         for (int k = 0; k < TZ; ++k) cell_update(k, dz0, kv, r2, a2, W16, cbase);
                     }
                 }
+            } else if (blk) {
+                // a block at an end of some slices' PI intervals: per slice its class
+                if (cls != 0) {
+#pragma unroll 1
+                    for (int j = 0; j < NB; ++j) {
+                        const int p = pb + j;
+                        const float4 gv = sh.vg[slot][j];
+                        const int2 kw = sh.kw[slot][j];
+                        const float fen = R - (X * gv.x + Y * gv.y);
+                        const float YY = Y * gv.x - X * gv.y;
+                        const float inv = rcp_approx(fen);
+                        const float kv = DdV * inv;
+                        const float r2 = fen * fen + YY * YY;
+                        const float dz0 = z0 - gv.z;
+                        const float u = fmaf(YY * DdU, inv, HalfYm);  // u - 1/2
+                        const float tu = u + kMagic;
+                        const float a = u - (tu - kMagic);           // alpha - 1/2
+                        const uint64_t a2 = pk2(a, a);
+                        const uint32_t W16 = (uint32_t)kw.y;
+                        const uint32_t cbase = (uint32_t)__float_as_int(tu) * 16u + (uint32_t)kw.x;
+#pragma unroll
+                        for (int k = 0; k < TZ; k += 2) {
+                            const uint32_t c0 = (cls >> (2 * k)) & 3u, c1 = (cls >> (2 * k + 2)) & 3u;
+                            if (PK2 && c0 == 1u && c1 == 1u) {
+                                if constexpr (PK2)
+                                    cell_update2(k, pk2(dz0, dz0), pk2(kv, kv), pk2(r2, r2), a2,
+                                                 W16, cbase);
+                            } else {
+                                if (c0 == 1u) cell_update(k, dz0, kv, r2, a2, W16, cbase);
+                                else if (c0 == 2u) cell_update_w(k, p, dz0, kv, r2, a2, W16, cbase);
+                                if (c1 == 1u) cell_update(k + 1, dz0, kv, r2, a2, W16, cbase);
+                                else if (c1 == 2u)
+                                    cell_update_w(k + 1, p, dz0, kv, r2, a2, W16, cbase);
+                            }
+                        }
+                    }
+                }
             } else if (col_ok && wmin <= wmax && !(pb + NB - 1 < wmin || pb > wmax)) {
+                // a partial block, or views without cell records: every update checked
 #pragma unroll 1
                 for (int j = 0; j < NB; ++j) {
                     const int p = pb + j;
@@ -529,26 +576,8 @@ __device__ __forceinline__ uint32_t tile4(const BPParams& kp, const float* __res
                         const uint32_t cbase =
                             (uint32_t)__float_as_int(tu) * 16u + (uint32_t)kw.x;
 #pragma unroll
-                        for (int h = 0; h < NG; ++h) {
-                            // group h unweighted at this view for every lane (warp-uniform)
-                            if (p >= gflo[h] && p <= gfhi[h]) {
-                                if constexpr (PK2) {
-                                    const uint64_t dz02 = pk2(dz0, dz0), kv2 = pk2(kv, kv),
-                                                   r22 = pk2(r2, r2);
-#pragma unroll
-                                    for (int k = h * GS; k < (h + 1) * GS; k += 2)
-                                        cell_update2(k, dz02, kv2, r22, a2, W16, cbase);
-                                } else {
-#pragma unroll
-                                    for (int k = h * GS; k < (h + 1) * GS; ++k)
-                                        cell_update(k, dz0, kv, r2, a2, W16, cbase);
-                                }
-                            } else {
-#pragma unroll
-                                for (int k = h * GS; k < (h + 1) * GS; ++k)
-                                    cell_update_w(k, p, dz0, kv, r2, a2, W16, cbase);
-                            }
-                        }
+                        for (int k = 0; k < TZ; ++k)
+                            cell_update_w(k, p, dz0, kv, r2, a2, W16, cbase);
                     } else {
                         // direct reads with the clamped indices of the first form
                         const float u = YY * DdU * inv + HalfY;
@@ -561,8 +590,8 @@ __device__ __forceinline__ uint32_t tile4(const BPParams& kp, const float* __res
                             const int d1 = vr.ti[k] + 1 - p;
                             if ((d0 | d1) < 0) continue;
                             float w = 1.f;
-                            if (d1 <= 1) w = ramp(vr.tf[k] + (float)(d1 - 1));
-                            else if (d0 <= 1) w = ramp((float)d0 - vr.bf[k]);
+                            if (d1 <= 1) w = ramp(__ldg(&pit[colbase + zb + k].tf) + (float)(d1 - 1));
+                            else if (d0 <= 1) w = ramp((float)d0 - __ldg(&pit[colbase + zb + k].bf));
                             const float dz = fmaf((float)k, dzf, dz0);
                             const float v = fmaf(dz, kv, HalfZ);
                             const float rinv = rsqrt_approx(fmaf(dz, dz, r2));
