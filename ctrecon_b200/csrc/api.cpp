@@ -743,34 +743,6 @@ static Status check_filter_bp_shapes(const ctrecon_filter_params& p, const BPGeo
     return Status::Ok();
 }
 
-// PI solve (on the down stream, overlapping the uploads), then the backprojection of d_fproj
-// into the FP64 image (uploaded, written in place, downloaded). `ready` is the event after
-// which d_fproj is complete (recorded by the caller), or NULL if it already is.
-static Status host_bkproj_pipeline(ctrecon_ctx* ctx, BPPlan& plan, const float* d_fproj,
-                                   cudaEvent_t ready, double* image) {
-    cudaStream_t up = ctx->up_stream, comp = ctx->host_stream, side = ctx->down_stream;
-    const size_t nvox = (size_t)plan.kp.NX * plan.kp.NY * plan.kp.NZ;
-    CTR_TRY(ctx->ws_pitab.ensure(nvox * sizeof(PiRecord), "PI table"));
-    CTR_TRY(ctx->ws_e.ensure(nvox * sizeof(double), "FP64 image"));
-    CTR_TRY(launch_pi(ctx, side, plan, ctx->ws_pitab.as<PiRecord>(), nullptr));
-    cudaEvent_t pi_done = nullptr, img_up = nullptr;
-    CTR_TRY(event_at(ctx, 0, &pi_done));
-    CTR_TRY(event_at(ctx, 1, &img_up));
-    CTR_CUDA(cudaEventRecord(pi_done, side));
-    CTR_CUDA(cudaMemcpyAsync(ctx->ws_e.ptr, image, nvox * sizeof(double), cudaMemcpyHostToDevice, up));
-    CTR_CUDA(cudaEventRecord(img_up, up));
-    if (ready) CTR_CUDA(cudaStreamWaitEvent(comp, ready, 0));
-    CTR_CUDA(cudaStreamWaitEvent(comp, pi_done, 0));
-    CTR_CUDA(cudaStreamWaitEvent(comp, img_up, 0));
-    CTR_TRY(launch_bkproj_f64out(ctx, comp, plan, d_fproj, ctx->ws_pitab.as<PiRecord>(),
-                                 ctx->ws_e.as<double>()));
-    CTR_CUDA(cudaMemcpyAsync(image, ctx->ws_e.ptr, nvox * sizeof(double), cudaMemcpyDeviceToHost, comp));
-    CTR_CUDA(cudaStreamSynchronize(comp));
-    CTR_CUDA(cudaStreamSynchronize(side));
-    CTR_CUDA(cudaStreamSynchronize(up));
-    return check_device_flag(ctx);
-}
-
 ctrecon_status ctrecon_filter_host_f64(ctrecon_ctx* ctx, const ctrecon_filter_params* p,
                                        const double* proj, double* fproj) {
     if (!ctx) return CTRECON_ERR_INVALID_ARGUMENT;
@@ -870,6 +842,91 @@ ctrecon_status ctrecon_bkproj_host_f64(ctrecon_ctx* ctx, const ctrecon_bp_geom* 
     API_END(ctx)
 }
 
+// The whole chain with FP64 host buffers (FunctionKat_v6.m:85-113 without the FProj round
+// trip), pipelined so that the host copies hide the work: the image goes up first and the PI
+// solve runs beside the uploads; the projections go up in chunks, each chunk is converted and
+// filtered as soon as it and its neighbour view are resident, and each window of about 2048
+// views is backprojected (accumulating into the zeroed valid voxels) as soon as its views are
+// filtered, while later chunks are still on their way; the image comes down at the end.
+static Status host_recon_pipeline(ctrecon_ctx* ctx, const ctrecon_filter_params& p, BPPlan& plan,
+                                  const double* proj, double* image) {
+    FilterPlan* fplan = nullptr;
+    CTR_TRY(get_filter_plan(ctx, p, &fplan));
+    cudaStream_t up = ctx->up_stream, comp = ctx->host_stream, side = ctx->down_stream;
+    const int P = p.proj_number;
+    const size_t S = (size_t)p.yl * p.zl, n = S * P;
+    const size_t nvox = (size_t)plan.kp.NX * plan.kp.NY * plan.kp.NZ;
+    CTR_TRY(ctx->ws_a.ensure(n * sizeof(double), "FP64 staging"));
+    CTR_TRY(ctx->ws_b.ensure(n * sizeof(float), "projections"));
+    CTR_TRY(ctx->ws_c.ensure(n * sizeof(float), "filtered projections"));
+    CTR_TRY(ctx->ws_pitab.ensure(nvox * sizeof(PiRecord), "PI table"));
+    CTR_TRY(ctx->ws_e.ensure(nvox * sizeof(double), "FP64 image"));
+    const int nch = (P + kHostChunkViews - 1) / kHostChunkViews;
+    cudaEvent_t pi_done = nullptr, img_up = nullptr;
+    CTR_TRY(event_at(ctx, 0, &pi_done));
+    CTR_TRY(event_at(ctx, 1, &img_up));
+    // image first (the first window needs it), then the projection chunks
+    CTR_CUDA(cudaMemcpyAsync(ctx->ws_e.ptr, image, nvox * sizeof(double), cudaMemcpyHostToDevice, up));
+    CTR_CUDA(cudaEventRecord(img_up, up));
+    for (int c = 0; c < nch; ++c) {
+        const size_t v0 = (size_t)c * kHostChunkViews, v1 = std::min<size_t>(P, v0 + kHostChunkViews);
+        CTR_CUDA(cudaMemcpyAsync(ctx->ws_a.as<double>() + v0 * S, proj + v0 * S,
+                                 (v1 - v0) * S * sizeof(double), cudaMemcpyHostToDevice, up));
+        cudaEvent_t e = nullptr;
+        CTR_TRY(event_at(ctx, 2 + (size_t)c, &e));
+        CTR_CUDA(cudaEventRecord(e, up));
+    }
+    CTR_TRY(launch_pi(ctx, side, plan, ctx->ws_pitab.as<PiRecord>(), nullptr));
+    CTR_CUDA(cudaEventRecord(pi_done, side));
+    CTR_CUDA(cudaStreamWaitEvent(comp, pi_done, 0));
+    CTR_CUDA(cudaStreamWaitEvent(comp, img_up, 0));
+    CTR_TRY(launch_zero_valid_f64(comp, ctx->ws_pitab.as<PiRecord>(), ctx->ws_e.as<double>(), nvox));
+    // windows of whole chunks, about 2048 views each
+    const int cpw = std::max(1, 2048 / kHostChunkViews);
+    const BPParams saved = plan.kp;
+    Status st;
+    int converted = 0;  // chunks [0, converted) are in FP32
+    for (int w0 = 0; st.ok() && w0 < nch; w0 += cpw) {
+        const int w1 = std::min(nch, w0 + cpw);
+        for (int c = w0; st.ok() && c < w1; ++c) {
+            const int v0 = c * kHostChunkViews, v1 = std::min(P, v0 + kHostChunkViews);
+            // this chunk and the first view of the next (derivative neighbour)
+            const int need = std::min(c + 1, nch - 1);
+            for (; st.ok() && converted <= need; ++converted) {
+                cudaEvent_t e = nullptr;
+                st = event_at(ctx, 2 + (size_t)converted, &e);
+                if (st.ok()) {
+                    const cudaError_t ce = cudaStreamWaitEvent(comp, e, 0);
+                    if (ce != cudaSuccess) st = cuda_status(ce, "chunk event");
+                }
+                const size_t x0 = (size_t)converted * kHostChunkViews;
+                const size_t x1 = std::min<size_t>(P, x0 + kHostChunkViews);
+                if (st.ok())
+                    st = launch_convert_f64_to_f32(comp, ctx->ws_a.as<double>() + x0 * S,
+                                                   ctx->ws_b.as<float>() + x0 * S, (x1 - x0) * S);
+            }
+            if (st.ok())
+                st = launch_filter(ctx, comp, *fplan, ctx->ws_b.as<float>(), 0, P,
+                                   ctx->ws_c.as<float>(), 0, v0, v1);
+        }
+        if (st.ok()) {
+            plan.kp.win0 = w0 * kHostChunkViews;
+            plan.kp.win1 = std::min(P, w1 * kHostChunkViews) - 1;
+            plan.kp.accum = 1;
+            st = launch_bkproj_f64out(ctx, comp, plan, ctx->ws_c.as<float>(),
+                                      ctx->ws_pitab.as<PiRecord>(), ctx->ws_e.as<double>());
+            plan.kp = saved;
+        }
+    }
+    plan.kp = saved;
+    CTR_TRY(st);
+    CTR_CUDA(cudaMemcpyAsync(image, ctx->ws_e.ptr, nvox * sizeof(double), cudaMemcpyDeviceToHost, comp));
+    CTR_CUDA(cudaStreamSynchronize(comp));
+    CTR_CUDA(cudaStreamSynchronize(side));
+    CTR_CUDA(cudaStreamSynchronize(up));
+    return check_device_flag(ctx);
+}
+
 ctrecon_status ctrecon_recon_host_f64(ctrecon_ctx* ctx, const ctrecon_filter_params* p,
                                       const ctrecon_bp_geom* g, const double* proj,
                                       double* image) {
@@ -882,9 +939,7 @@ ctrecon_status ctrecon_recon_host_f64(ctrecon_ctx* ctx, const ctrecon_filter_par
     if (s.ok()) s = get_bp_plan(ctx, *g, &plan);
     if (s.ok()) s = check_filter_bp_shapes(*p, plan->g);
     if (s.ok()) s = host_reset(ctx);
-    if (s.ok()) s = host_filter_pipeline(ctx, *p, proj, nullptr);
-    // the filter's work is ordered on the host stream, where the backprojection runs too
-    if (s.ok()) s = host_bkproj_pipeline(ctx, *plan, ctx->ws_c.as<float>(), nullptr, image);
+    if (s.ok()) s = host_recon_pipeline(ctx, *p, *plan, proj, image);
     return finish(ctx, s);
     API_END(ctx)
 }
