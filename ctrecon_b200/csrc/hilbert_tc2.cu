@@ -141,6 +141,12 @@ __device__ __forceinline__ void tmem_wait_ld16(uint32_t* r) {
 __device__ __forceinline__ float pick4(int d, float v0, float v1, float v2, float v3) {
     return d == 0 ? v0 : d == 1 ? v1 : d == 2 ? v2 : v3;
 }
+// the same for d in [0, 3] known: two levels of selects on its bits
+__device__ __forceinline__ float sel4(int d, float v0, float v1, float v2, float v3) {
+    const float a = (d & 1) ? v1 : v0;
+    const float b = (d & 1) ? v3 : v2;
+    return (d & 2) ? b : a;
+}
 
 template <int MODE>
 __host__ __device__ constexpr int planes2() { return MODE == CTRECON_HILBERT_BF16X3 ? 2 : 1; }
@@ -301,7 +307,43 @@ k_hilbert_tc2(const __grid_constant__ CUtensorMap tA0, const __grid_constant__ C
                     lo[r] = (int)__reduce_min_sync(0xffffffffu, (unsigned)min(e[r].x, e[r].y));
                     hi[r] = (int)__reduce_max_sync(0xffffffffu, (unsigned)max(e[r].x, e[r].y));
                 }
-                for (int vl = 0; vl < nv; ++vl) {
+                // every row of the batch spans at most four kappa rows over the warp (the usual
+                // case): one window per row, selects without range checks
+                bool narrow = true;
+#pragma unroll
+                for (int r = 0; r < kRowsAhead; ++r) narrow = narrow && hi[r] - lo[r] < 4;
+                for (int vl = 0; vl < nv && narrow; ++vl) {
+                    const int cbase = vl * p.AL;  // this view's first accumulator column
+                    float* ov = p.out + (size_t)(vg * p.vpt + vl) * vstride + (size_t)k0 * p.YL + i;
+                    const size_t rstep = (size_t)4 * p.YL;  // rows k0, k0 + 4, ... of this warp
+#pragma unroll
+                    for (int r4 = 0; r4 < kRowsAhead; r4 += 4) {
+                        uint32_t w[16];
+                        int c0[4];
+#pragma unroll
+                        for (int r = 0; r < 4; ++r) {
+                            c0[r] = min(cbase + lo[r4 + r], kAccCols - 4);
+                            tmem_ld4_nowait(acc_base + (uint32_t)c0[r], w + 4 * r);
+                        }
+                        tmem_wait_ld16(w);
+#pragma unroll
+                        for (int r = 0; r < 4; ++r) {
+                            const int k = k0 + 4 * (r4 + r);
+                            const int4 er = e[r4 + r];
+                            const int db = cbase + er.x - c0[r], de = cbase + er.y - c0[r];
+                            const float v0 = __uint_as_float(w[4 * r]);
+                            const float v1 = __uint_as_float(w[4 * r + 1]);
+                            const float v2 = __uint_as_float(w[4 * r + 2]);
+                            const float v3 = __uint_as_float(w[4 * r + 3]);
+                            const float vb = sel4(db, v0, v1, v2, v3);
+                            const float ve = sel4(de, v0, v1, v2, v3);
+                            if (valid && k < p.ZL)
+                                ov[(size_t)(r4 + r) * rstep] =
+                                    fmaf(__int_as_float(er.z), vb, __int_as_float(er.w) * ve);
+                        }
+                    }
+                }
+                for (int vl = 0; vl < nv && !narrow; ++vl) {
                     const int cbase = vl * p.AL;  // this view's first accumulator column
 #pragma unroll
                     for (int r4 = 0; r4 < kRowsAhead; r4 += 4) {
