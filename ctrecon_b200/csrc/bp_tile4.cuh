@@ -188,8 +188,8 @@ __device__ __forceinline__ uint32_t tile4(const BPParams& kp, const float* __res
     // a 4 x 2 patch (lane bits 0-1: x, 2: y, 3: x, 4: y), whose cells on the detector lie closer
     // together than 8 columns of one row, so fewer of them share a bank group
     const int lane_ = tid & 31, w_ = (tid >> 5) & 7;
-    const int tx = (w_ & 1) * 8 + (lane_ & 3) + ((lane_ >> 3) & 1) * 4;
-    const int ty = (w_ >> 1) * 4 + ((lane_ >> 2) & 1) + ((lane_ >> 4) & 1) * 2;
+    const int tx = (w_ & 1) * 8 + (lane_ & 1) + ((lane_ >> 3) & 3) * 2;
+    const int ty = (w_ >> 1) * 4 + ((lane_ >> 1) & 3);
     const int x = bx * kTXY + tx, y = by * kTXY + ty;
     const bool col_ok = consumer && (x < NX) && (y < NY);
     const size_t colbase = ((size_t)x * NY + y) * NZ;

@@ -21,8 +21,9 @@
 // SM and clock in every precision).
 //
 // CTRECON_PINET_GRID (the default): the network's inputs depend on (r, psi = phi - 2 pi z)
-// only, so k_pinet_infer evaluates it once per point of a 256 x 1024 grid of (r, psi) and the
-// Newton kernel (pi.cu) starts every voxel from the bilinear interpolation of those outputs.
+// only, so k_pinet_infer evaluates it once per point of a 256 x 4096 grid of (r, psi), an FP64
+// Newton solve refines each grid point from the network's output (k_grid_refine), and the Newton
+// kernel (pi.cu) starts every voxel from the bilinear interpolation of the refined grid.
 #include "internal.h"
 #include "pi_device.cuh"
 #include "pinet.h"
@@ -463,7 +464,32 @@ __global__ void k_grid_feat(float* __restrict__ feat, int nr, int np, double r_m
     feat[3 * q + 2] = (float)sp;
 }
 
-constexpr int kGridNR = 256, kGridNP = 1024;
+// The network's predictions at the grid points refined by the FP64 Newton solve (pi_device.cuh)
+// of the grid point itself, (x, y, z) = r (cos psi, sin psi) / ScanR at z = 0, from the network's
+// start: by the screw symmetry of the PI lines (a turn of the helix by psi lifts every chord by
+// psi / 2 pi) each voxel's interpolated start is then within the grid's interpolation error of its
+// root (~3e-7 rad on this grid), under the 1e-6 rad at which Newton accepts a step, so a voxel's
+// solve takes one Newton evaluation before the replayed bisection; the grid points whose Newton
+// solve does not converge keep the network's prediction.
+__global__ void k_grid_refine(float2* __restrict__ out, int nr, int np, double r_max) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nr * np) return;
+    const int i = q / np, j = q % np;
+    double sp, cp;
+    sincospi(2.0 * j / np, &sp, &cp);
+    const double r = r_max * i / (nr - 1);
+    const float2 o = out[q];
+    double sb, st;
+    int it = 0;
+    bool conv = false;
+    pi_newton(r * cp, r * sp, 0.0, (double)o.x / kPinetOutScale - 0.5 * kRefPi, &sb, &st, &it,
+              nullptr, &conv);
+    if (conv)
+        out[q] = make_float2((float)((sb + 0.5 * kRefPi) * kPinetOutScale),
+                             (float)((st - 0.5 * kRefPi) * kPinetOutScale));
+}
+
+constexpr int kGridNR = 256, kGridNP = 4096;
 
 Status launch_pi_learned(ctrecon_ctx* ctx, cudaStream_t s, BPPlan& plan, PiRecord* d_pitab,
                          unsigned long long* d_updates, unsigned long long* d_iters) {
@@ -480,6 +506,9 @@ Status launch_pi_learned(ctrecon_ctx* ctx, cudaStream_t s, BPPlan& plan, PiRecor
         CTR_CUDA(cudaGetLastError());
         CTR_TRY(launch_infer(ctx, s, plan.kp, ng, ctx->pinet.grid_feat.as<float>(),
                              ctx->pinet.grid_out.as<float2>(), nullptr));
+        k_grid_refine<<<(ng + 127) / 128, 128, 0, s>>>(ctx->pinet.grid_out.as<float2>(), kGridNR,
+                                                       kGridNP, r_max);
+        CTR_CUDA(cudaGetLastError());
         return launch_pi_guess(ctx, s, plan, d_pitab, d_updates, d_iters, nullptr,
                                ctx->pinet.grid_out.ptr, kGridNR, kGridNP, r_max);
     }

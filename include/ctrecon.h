@@ -109,8 +109,10 @@ enum {
 enum {
     CTRECON_PINET_VOXEL_FP32 = 0, /* per voxel, FP32 SiLU (as ctrecon_pinet_predict) */
     CTRECON_PINET_VOXEL_BF16 = 1, /* per voxel, packed BF16 SiLU */
-    CTRECON_PINET_GRID = 2        /* default: the network (FP32 SiLU) on a 256 x 1024 grid of
-                                     (r, psi) each solve, bilinear in (r, psi) per voxel */
+    CTRECON_PINET_GRID = 2        /* default: the network (FP32 SiLU) on a 256 x 4096 grid of
+                                     (r, psi) each solve, each grid point refined by the FP64
+                                     Newton solve from the network's output, bilinear in
+                                     (r, psi) per voxel */
 };
 
 typedef enum ctrecon_option {

@@ -158,6 +158,10 @@ def test_pinet_training_inference_and_gain(torch_mod):
         assert r["iters"] < newt["iters"]
     # the grid interpolates the same network: as good a start as evaluating it per voxel
     assert lrn["grid"]["iters"] <= 1.02 * lrn["voxel-fp32"]["iters"]
+    # and its points are refined by the FP64 Newton solve, so a voxel's interpolated start is
+    # within the 1e-6 rad at which Newton accepts: one Newton evaluation and the replayed
+    # bisection's final one per voxel (2.00 measured at c1)
+    assert lrn["grid"]["iters"] <= 2.1 * nv
 
 
 @pytest.mark.parametrize("name", ["c1", "c2s", "ragged"])
