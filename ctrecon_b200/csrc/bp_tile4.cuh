@@ -185,7 +185,7 @@ __device__ __forceinline__ uint32_t tile4(const BPParams& kp, const float* __res
     // consumer state
     // warp w holds the 8 x 4 columns x in 8 (w & 1) + [0, 8), y in 4 (w >> 1) + [0, 4) (compact,
     // so its voxels' PI intervals differ little); each quarter-warp of its 16-byte record loads is
-    // a 4 x 2 patch (lane bits 0-1: x, 2: y, 3: x, 4: y), whose cells on the detector lie closer
+    // a 2 x 4 patch (lane bit 0: x, bits 1-2: y, bits 3-4: x), whose cells on the detector lie closer
     // together than 8 columns of one row, so fewer of them share a bank group
     const int lane_ = tid & 31, w_ = (tid >> 5) & 7;
     const int tx = (w_ & 1) * 8 + (lane_ & 1) + ((lane_ >> 3) & 3) * 2;
