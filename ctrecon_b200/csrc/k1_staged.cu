@@ -14,14 +14,14 @@
 // The derivative of view p reads views pc - 1, pc, pc + 1 (pc = p clamped to [1, P - 2]) and p
 // itself, so walking the views in order, each view of the strip is copied in ONCE (rows
 // 0 .. ZL - 1, the strip's 32 columns plus 4 each side for the u stencil: the copies start on
-// a 16-byte boundary) into a ring of kSlots slots, up to kSlots - 3 views ahead of the view
+// a 16-byte boundary) into a ring of SLOTS slots, up to SLOTS - 3 views ahead of the view
 // being computed. The forward-rebin entries (the two weights and the two derivative rows of
 // each (kappa line, column)) of a thread's column and its warp's kappa lines stay in registers
 // for the whole run: the only global traffic of the loop is the tensor copies in and the
 // kappa-row stores out, and shared memory carries only the staged rows and the derivative.
 //
 // Per view: wait for the view the window gains; the derivative of the strip's ZL x 32 samples
-// into one of two shared buffers (a warp per 8 rows, a lane per column, the v stencil's rows
+// into one of two shared buffers (a warp per ROWS rows, a lane per column, the v stencil's rows
 // in registers); ONE barrier; the copies of the views the next window frees; the AL x 32
 // kappa samples from that buffer (a warp per kappa line, the entries in registers),
 // stored de-interleaved as every Hilbert form reads them. The next view's derivative writes
@@ -45,10 +45,18 @@ constexpr int kHalo = 4;                   // staged columns each side (16 bytes
 constexpr int kRowW = kStrip + 2 * kHalo;  // floats per staged row
 constexpr int kThreadsK1 = 512;
 constexpr int kWarpsK1 = kThreadsK1 / 32;
-constexpr int kRowsPerWarp = 8;            // derivative rows a warp takes at a time
-constexpr int kSlots = 5;                  // ring of staged views
-constexpr int kRegLines = 11;              // kappa lines per warp, entries held in registers
-constexpr size_t kSmemBudget = 227 * 1024 - 128 - 64;  // less alignment slack and barriers
+constexpr size_t kSmemBudget = 227 * 1024 - 128 - 128;  // less alignment slack and barriers
+
+// The two shapes of the kernel: derivative rows a warp takes at a time (ROWS), kappa lines per
+// warp with their entries in registers (LINES), views in the ring (SLOTS). Tall detectors (up
+// to 176 kappa lines) take 8 rows and 11 lines a warp; short ones (at most 64 rows and 96
+// kappa lines) 4 rows and 6 lines, so that all 16 warps share the derivative, no warp loads
+// entries of lines past AL, and the smaller staged views allow a deeper ring.
+struct K1Shape {
+    int rows, lines, slots;
+};
+constexpr K1Shape kTall{8, 11, 5};
+constexpr K1Shape kShort{4, 6, 8};
 
 struct K1sParams {
     int P, YL, ZL, AL, YLp;
@@ -105,19 +113,19 @@ __device__ __forceinline__ float deriv_sample(float pp, float pm, float ur, floa
     return fmaf(zc, vr - vl, g);
 }
 
-template <int MODE>
+template <int MODE, int ROWS, int LINES, int SLOTS>
 __global__ void __launch_bounds__(kThreadsK1, 1)
 k_deriv_rebin_staged(const __grid_constant__ CUtensorMap pmap, const K1sParams k) {
     extern __shared__ __align__(128) unsigned char k1dyn[];
-    __shared__ __align__(8) uint64_t full[kSlots];
+    __shared__ __align__(8) uint64_t full[SLOTS];
     unsigned char* base = k1dyn + ((128u - (tcu::smem_u32(k1dyn) & 127u)) & 127u);
     const int ZL = k.ZL, AL = k.AL, YL = k.YL, P = k.P;
     float* ring = reinterpret_cast<float*>(base);
-    float* gfb = ring + (size_t)kSlots * k.slot_floats;  // two buffers of ZL x 32 samples
+    float* gfb = ring + (size_t)SLOTS * k.slot_floats;  // two buffers of ZL x 32 samples
     float* zs = gfb + (size_t)2 * ZL * kStrip;             // zcv
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (tid == 0) {
-        for (int s = 0; s < kSlots; ++s) tcu::mbar_init(&full[s], 1);
+        for (int s = 0; s < SLOTS; ++s) tcu::mbar_init(&full[s], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     for (int i = tid; i < ZL; i += kThreadsK1) zs[i] = k.zcv[i];
@@ -133,9 +141,9 @@ k_deriv_rebin_staged(const __grid_constant__ CUtensorMap pmap, const K1sParams k
     // the forward-rebin entries of this thread's column and the warp's kappa lines
     // a = warp + 16 i, for the whole run: {wa, wb, byte offsets of gf[r0][lane], gf[r1][lane]};
     // columns past YL get zero weights (zero padding)
-    float4 te[kRegLines];
+    float4 te[LINES];
 #pragma unroll
-    for (int i = 0; i < kRegLines; ++i) {
+    for (int i = 0; i < LINES; ++i) {
         const int a = warp + i * kWarpsK1;
         FwEntry e{0, 0, 0.f, 0.f};
         if (a < AL && real) e = k.fw[(size_t)a * YL + j];
@@ -144,21 +152,21 @@ k_deriv_rebin_staged(const __grid_constant__ CUtensorMap pmap, const K1sParams k
     }
     __syncthreads();  // barriers initialised, zcv in place
 
-    // views staged for the run, in order: L0 .. L1 (copy c = v - L0 fills slot c % kSlots)
+    // views staged for the run, in order: L0 .. L1 (copy c = v - L0 fills slot c % SLOTS)
     const int L0 = clamp_view(pfirst, P) - 1, L1 = clamp_view(plast, P) + 1;
     int next = L0;  // next view to copy in (the same in every thread)
     auto issue_upto = [&](int vmax) {
         vmax = vmax < L1 ? vmax : L1;
         for (; next <= vmax; ++next) {
             if (tid == 0) {
-                const int s = (next - L0) % kSlots;
+                const int s = (next - L0) % SLOTS;
                 mbar_arrive_expect_tx(&full[s], k.box_bytes);
                 tma_load_rows(tcu::smem_u32(ring + (size_t)s * k.slot_floats), &pmap, j0 - kHalo,
                               0, next - k.proj_view0, &full[s]);
             }
         }
     };
-    issue_upto(L0 + kSlots - 1);  // fill the ring
+    issue_upto(L0 + SLOTS - 1);  // fill the ring
 
     const float2 cy = real ? __ldg(k.cuy + j) : make_float2(0.f, 0.f);
     // u stencil with the reference's edge rule (:63-78), as offsets into a staged row; columns
@@ -169,10 +177,10 @@ k_deriv_rebin_staged(const __grid_constant__ CUtensorMap pmap, const K1sParams k
     const int oc = lane + kHalo;
     const int ol = real ? jl - j0 + kHalo : oc, orr = real ? jr - j0 + kHalo : oc;
     // the first block of rows of this warp: its (zcv[k] * cy) factors for the whole run
-    const int kb = warp * kRowsPerWarp;
-    float zcy[kRowsPerWarp];
+    const int kb = warp * ROWS;
+    float zcy[ROWS];
 #pragma unroll
-    for (int i = 0; i < kRowsPerWarp; ++i) zcy[i] = kb + i < ZL ? zs[kb + i] * cy.y : 0.f;
+    for (int i = 0; i < ROWS; ++i) zcy[i] = kb + i < ZL ? zs[kb + i] * cy.y : 0.f;
     // kappa lines of this warp, and the 32-bit shared addresses the loop works with
     const int nl = AL > warp ? (AL - warp + kWarpsK1 - 1) / kWarpsK1 : 0;
     const size_t jx = (size_t)((j & 1) * (k.YLp >> 1) + (j >> 1));
@@ -191,24 +199,24 @@ k_deriv_rebin_staged(const __grid_constant__ CUtensorMap pmap, const K1sParams k
         // ring runs
         bool ok = true;
         while (ok && waited <= pc + 1 - L0) {
-            ok = tcu::mbar_wait(&full[waited % kSlots], (uint32_t)(waited / kSlots) & 1u, k.err, 31);
+            ok = tcu::mbar_wait(&full[waited % SLOTS], (uint32_t)(waited / SLOTS) & 1u, k.err, 31);
             if (ok) ++waited;
         }
         const uint32_t gcur = gf_s + (uint32_t)((p - pfirst) & 1) * gf_b;
         if (ok) {
-            const uint32_t Tm = ring_s + (uint32_t)((pc - 1 - L0) % kSlots) * slot_b;
-            const uint32_t Tp = ring_s + (uint32_t)((pc + 1 - L0) % kSlots) * slot_b;
-            const uint32_t Tv = ring_s + (uint32_t)((p - L0) % kSlots) * slot_b;
+            const uint32_t Tm = ring_s + (uint32_t)((pc - 1 - L0) % SLOTS) * slot_b;
+            const uint32_t Tp = ring_s + (uint32_t)((pc + 1 - L0) % SLOTS) * slot_b;
+            const uint32_t Tv = ring_s + (uint32_t)((p - L0) % SLOTS) * slot_b;
             const uint32_t tv = Tv + (uint32_t)oc * 4u, tp = Tp + (uint32_t)oc * 4u;
             const uint32_t tm = Tm + (uint32_t)oc * 4u;
             const uint32_t tl = Tv + (uint32_t)ol * 4u, tq = Tv + (uint32_t)orr * 4u;
             const uint32_t gw = gcur + (uint32_t)lane * 4u;
-            for (int k0 = kb; k0 < ZL; k0 += kWarpsK1 * kRowsPerWarp) {
-                if (k0 == kb && k0 >= 1 && k0 + kRowsPerWarp + 1 <= ZL) {
+            for (int k0 = kb; k0 < ZL; k0 += kWarpsK1 * ROWS) {
+                if (k0 == kb && k0 >= 1 && k0 + ROWS + 1 <= ZL) {
                     // no edge row: the v stencil is rows k - 1, k + 1; each half block loads
                     // all its operands before it computes
 #pragma unroll
-                    for (int h = 0; h < kRowsPerWarp; h += 4) {
+                    for (int h = 0; h < ROWS; h += 4) {
                         const uint32_t r0 = (uint32_t)(k0 + h) * kRowB;
                         float w[6], fp[4], fm[4], fl[4], fq[4];
 #pragma unroll
@@ -229,7 +237,7 @@ k_deriv_rebin_staged(const __grid_constant__ CUtensorMap pmap, const K1sParams k
                     }
                 } else {
                     // the first or the last row (edge rule, :85-95), rows past 128, or past ZL
-                    for (int i = 0; i < kRowsPerWarp; ++i) {
+                    for (int i = 0; i < ROWS; ++i) {
                         const int kk = k0 + i;
                         if (kk >= ZL) break;
                         int kl = kk - 1, kr = kk + 1;
@@ -247,26 +255,26 @@ k_deriv_rebin_staged(const __grid_constant__ CUtensorMap pmap, const K1sParams k
         }
         // every thread's derivative is in place and its reads of the ring are done
         if (!__syncthreads_and(ok)) { good = false; break; }
-        if (p < plast) issue_upto(clamp_view(p + 1, P) - 1 + kSlots - 1);
+        if (p < plast) issue_upto(clamp_view(p + 1, P) - 1 + SLOTS - 1);
         // forward rebin + pre-weight (:131-153) into the chunk's kappa rows: every line's two
         // derivative samples loaded first (lines past AL read row 0 with zero weights), then
         // the sums, then the stores
-        float v[kRegLines];
+        float v[LINES];
         {
-            float g0[kRegLines], g1[kRegLines];
+            float g0[LINES], g1[LINES];
 #pragma unroll
-            for (int i = 0; i < kRegLines; ++i) {
+            for (int i = 0; i < LINES; ++i) {
                 g0[i] = lds_f32(gcur + __float_as_uint(te[i].z));
                 g1[i] = lds_f32(gcur + __float_as_uint(te[i].w));
             }
 #pragma unroll
-            for (int i = 0; i < kRegLines; ++i) v[i] = fmaf(te[i].x, g0[i], te[i].y * g1[i]);
+            for (int i = 0; i < LINES; ++i) v[i] = fmaf(te[i].x, g0[i], te[i].y * g1[i]);
         }
         const size_t x0 = (size_t)(p - k.c0) * AL * k.YLp + (size_t)warp * k.YLp + jx;
         if constexpr (MODE == CTRECON_HILBERT_BF16X3) {
             __nv_bfloat16* o = static_cast<__nv_bfloat16*>(k.X) + x0;
 #pragma unroll
-            for (int i = 0; i < kRegLines; ++i, o += ostep) {
+            for (int i = 0; i < LINES; ++i, o += ostep) {
                 const __nv_bfloat16 hi = __float2bfloat16_rn(v[i]);
                 const __nv_bfloat16 lo = __float2bfloat16_rn(v[i] - __bfloat162float(hi));
                 if (i < nl) {
@@ -277,7 +285,7 @@ k_deriv_rebin_staged(const __grid_constant__ CUtensorMap pmap, const K1sParams k
         } else {
             float* o = static_cast<float*>(k.X) + x0;
 #pragma unroll
-            for (int i = 0; i < kRegLines; ++i, o += ostep) {
+            for (int i = 0; i < LINES; ++i, o += ostep) {
                 float r = v[i];
                 if constexpr (MODE == CTRECON_HILBERT_TF32) {
                     uint32_t t;
@@ -292,16 +300,22 @@ k_deriv_rebin_staged(const __grid_constant__ CUtensorMap pmap, const K1sParams k
         // no copy may still be writing shared memory when the CTA exits: wait (bounded) for
         // the copies not known complete
         for (int c = waited; c < next - L0; ++c)
-            tcu::mbar_drain(&full[c % kSlots], (uint32_t)(c / kSlots) & 1u);
+            tcu::mbar_drain(&full[c % SLOTS], (uint32_t)(c / SLOTS) & 1u);
     }
+}
+
+// the kernel's shape for a detector of ZL rows and AL kappa lines
+K1Shape staged_shape(int ZL, int AL) {
+    return (ZL <= kWarpsK1 * kShort.rows && AL <= kWarpsK1 * kShort.lines) ? kShort : kTall;
 }
 
 // dynamic shared memory of the staged form, or 0 when it does not apply
 size_t staged_smem(int ZL, int AL, int* slot_floats) {
     if (ZL < 3 || ZL > 256 || AL < 1) return 0;
+    const K1Shape sh = staged_shape(ZL, AL);
     *slot_floats = (ZL * kRowW + 31) / 32 * 32;
-    if (AL > kRegLines * kWarpsK1) return 0;
-    const size_t bytes = (size_t)kSlots * *slot_floats * 4 + (size_t)2 * ZL * kStrip * 4 +
+    if (AL > sh.lines * kWarpsK1) return 0;
+    const size_t bytes = (size_t)sh.slots * *slot_floats * 4 + (size_t)2 * ZL * kStrip * 4 +
                          (size_t)ZL * 4;
     return bytes <= kSmemBudget ? bytes + 128 : 0;
 }
@@ -331,11 +345,21 @@ Status make_proj_map(CUtensorMap* m, const float* base, int YL, int ZL, int nvie
     return Status::Ok();
 }
 
+template <int MODE, bool TALL>
+Status run_staged(const CUtensorMap& map, const K1sParams& k, int grid, size_t smem,
+                  cudaStream_t s) {
+    constexpr K1Shape sh = TALL ? kTall : kShort;
+    auto kern = k_deriv_rebin_staged<MODE, sh.rows, sh.lines, sh.slots>;
+    CTR_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<grid, kThreadsK1, smem, s>>>(map, k);
+    return Status::Ok();
+}
+
 }  // namespace
 
 // Whether the staged K1 applies: rows of whole 16-byte units (YL a multiple of 4: the copies'
 // row stride), at most 256 detector rows (one box), at most 176 kappa lines (11 per warp, their
-// entries in registers), two derivative buffers and the ring in shared memory, a 16-byte
+// entries in registers; 96 for the short shape), two derivative buffers and the ring in shared memory, a 16-byte
 // aligned buffer.
 bool k1_staged_fits(int YL, int ZL, int AL, int YLp, const void* d_proj) {
     int sf = 0;
@@ -371,21 +395,19 @@ Status launch_k1_staged(ctrecon_ctx* ctx, cudaStream_t s, const float* d_proj, i
     k.X = X;
     k.err = ctx->ws_flag.as<int>();
     const int grid = k.nstrips * k.ngroups;
+    const bool tall = staged_shape(ZL, AL).rows == kTall.rows;
     switch (mode) {
     case CTRECON_HILBERT_BF16X3:
-        CTR_CUDA(cudaFuncSetAttribute(k_deriv_rebin_staged<CTRECON_HILBERT_BF16X3>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_deriv_rebin_staged<CTRECON_HILBERT_BF16X3><<<grid, kThreadsK1, smem, s>>>(map, k);
+        if (tall) CTR_TRY((run_staged<CTRECON_HILBERT_BF16X3, true>(map, k, grid, smem, s)));
+        else CTR_TRY((run_staged<CTRECON_HILBERT_BF16X3, false>(map, k, grid, smem, s)));
         break;
     case CTRECON_HILBERT_TF32:
-        CTR_CUDA(cudaFuncSetAttribute(k_deriv_rebin_staged<CTRECON_HILBERT_TF32>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_deriv_rebin_staged<CTRECON_HILBERT_TF32><<<grid, kThreadsK1, smem, s>>>(map, k);
+        if (tall) CTR_TRY((run_staged<CTRECON_HILBERT_TF32, true>(map, k, grid, smem, s)));
+        else CTR_TRY((run_staged<CTRECON_HILBERT_TF32, false>(map, k, grid, smem, s)));
         break;
     default:
-        CTR_CUDA(cudaFuncSetAttribute(k_deriv_rebin_staged<CTRECON_HILBERT_FP32>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_deriv_rebin_staged<CTRECON_HILBERT_FP32><<<grid, kThreadsK1, smem, s>>>(map, k);
+        if (tall) CTR_TRY((run_staged<CTRECON_HILBERT_FP32, true>(map, k, grid, smem, s)));
+        else CTR_TRY((run_staged<CTRECON_HILBERT_FP32, false>(map, k, grid, smem, s)));
         break;
     }
     CTR_CUDA(cudaGetLastError());

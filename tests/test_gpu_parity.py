@@ -151,7 +151,8 @@ def test_filter_tensor_core_forms_agree(torch_mod, oracle_mod, yl, zl, chunk, mo
 
 
 @pytest.mark.parametrize("yl,zl,chunk", [(300, 16, 2048), (300, 40, 7), (256, 16, 100),
-                                          (736, 64, 33), (132, 8, 5), (130, 40, 7)])
+                                          (736, 64, 33), (132, 8, 5), (130, 40, 7),
+                                          (256, 80, 9), (160, 132, 40)])
 @pytest.mark.parametrize("mode", ["fp32", "bf16x3", "tf32"])
 def test_k1_forms_bit_identical(torch_mod, oracle_mod, yl, zl, chunk, mode):
     """The staged K1 (tensor copies of 32-column strips, views walked in order, default) and
@@ -159,9 +160,11 @@ def test_k1_forms_bit_identical(torch_mod, oracle_mod, yl, zl, chunk, mode):
     Hilbert form agree exactly; both against the FP64 oracle. Shapes: ragged strips (300 and
     132 columns: a partial last strip and zero-padded columns), chunks of 7, 33 and 5 views
     (runs of one view, and chunks with fewer views than runs), eight detector rows (half of
-    them under the v stencil's edge rule), 40 rows (a warp's second block of rows holds the
-    last one), the c2 detector width, and 130 columns, where the staged form does not apply
-    (rows of 520 bytes) and both settings run the per-view form."""
+    them under the v stencil's edge rule), 40 rows, 64 rows and the c2 detector width (the
+    short shape: 4 rows and 6 kappa lines a warp), 80 rows (105 kappa lines: the tall shape, 8
+    rows and 11 lines a warp), 132 rows (173 kappa lines: warp 0 takes a second block of rows,
+    the last four), and 130 columns, where the staged form does not apply (rows of 520 bytes)
+    and both settings run the per-view form."""
     import ctrecon_b200 as ct
     from ctrecon_b200 import _lib
     from ctrecon_b200.geometry import small_config
