@@ -3,13 +3,13 @@
 // with the pre-weight (:131-153), the same arithmetic in the same order as k_deriv_rebin
 // (filter.cu), so the kappa rows are bit-identical to that kernel's.
 //
-// Layout of the work: the detector is cut into strips of 32 columns. CTA b (one per SM, all
-// resident at once) takes strip b % strips and the (b / strips)-th of as many equal runs of
-// the chunk's views as whole sets of strips fit on the SMs, and walks its views in order. The
-// strips of one run are neighbouring CTAs working on the same views at the same time, so the
-// 128-byte lines a strip's halo columns share with its neighbours, and the lines of the kappa
-// rows the strips write side by side, meet in L2: DRAM sees each projection line read once
-// and each kappa-row line written whole.
+// Layout of the work: the detector is cut into strips of 32 columns. CTA b (one per SM at a
+// time) takes strip b % strips and the (b / strips)-th of the equal runs of the chunk's views
+// (as many runs as fill the SMs in the fewest waves, staged_runs), and walks its views in
+// order. The strips of one run are neighbouring CTAs working on the same views at the same
+// time (they start in the same wave), so the 128-byte lines a strip's halo columns share with
+// its neighbours, and the lines of the kappa rows the strips write side by side, meet in L2:
+// DRAM sees each projection line read once and each kappa-row line written whole.
 //
 // The derivative of view p reads views pc - 1, pc, pc + 1 (pc = p clamped to [1, P - 2]) and p
 // itself, so walking the views in order, each view of the strip is copied in ONCE (rows
@@ -272,15 +272,22 @@ k_deriv_rebin_staged(const __grid_constant__ CUtensorMap pmap, const K1sParams k
         }
         const size_t x0 = (size_t)(p - k.c0) * AL * k.YLp + (size_t)warp * k.YLp + jx;
         if constexpr (MODE == CTRECON_HILBERT_BF16X3) {
-            __nv_bfloat16* o = static_cast<__nv_bfloat16*>(k.X) + x0;
+            // lanes l and l + 2 hold neighbouring elements of a de-interleaved row: lanes with
+            // bit 1 clear store the two hi values at their own element, the others the two lo
+            // values at the element before theirs (4-byte aligned: YLp and the plane offset are
+            // even)
+            const bool hi_lane = (lane & 2) == 0;
+            __nv_bfloat16* o = static_cast<__nv_bfloat16*>(k.X) + x0 + (hi_lane ? 0 : k.plane - 1);
 #pragma unroll
             for (int i = 0; i < LINES; ++i, o += ostep) {
                 const __nv_bfloat16 hi = __float2bfloat16_rn(v[i]);
                 const __nv_bfloat16 lo = __float2bfloat16_rn(v[i] - __bfloat162float(hi));
-                if (i < nl) {
-                    o[0] = hi;
-                    o[k.plane] = lo;
-                }
+                const uint32_t u = (uint32_t)__bfloat16_as_ushort(hi) |
+                                   ((uint32_t)__bfloat16_as_ushort(lo) << 16);
+                const uint32_t dn = __shfl_down_sync(0xffffffffu, u, 2);
+                const uint32_t up = __shfl_up_sync(0xffffffffu, u, 2);
+                const uint32_t w = hi_lane ? __byte_perm(u, dn, 0x5410) : __byte_perm(up, u, 0x7632);
+                if (i < nl) *reinterpret_cast<uint32_t*>(o) = w;
             }
         } else {
             float* o = static_cast<float*>(k.X) + x0;
@@ -318,6 +325,26 @@ size_t staged_smem(int ZL, int AL, int* slot_floats) {
     const size_t bytes = (size_t)sh.slots * *slot_floats * 4 + (size_t)2 * ZL * kStrip * 4 +
                          (size_t)ZL * 4;
     return bytes <= kSmemBudget ? bytes + 128 : 0;
+}
+
+// Runs of views per strip. One CTA fits on an SM, so strips x runs CTAs take ceil(strips x runs
+// / SMs) waves, each as long as a run (its views, plus about four views' worth of start-up: the
+// two halo views copied in and the first copies' latency). The count that minimises waves x
+// (views per run + 4): 32 strips of 2048 views take 9 runs in two waves of 148 SMs (288 CTAs)
+// rather than 4 runs in one wave of 128.
+int staged_runs(int nstrips, int n, int nsm) {
+    int best = 1;
+    long long best_cost = -1;
+    const int gmax = std::min(n, 64);
+    for (int g = 1; g <= gmax; ++g) {
+        const long long waves = ((long long)nstrips * g + nsm - 1) / nsm;
+        const long long cost = waves * ((n + g - 1) / g + 4);
+        if (best_cost < 0 || cost < best_cost) {
+            best_cost = cost;
+            best = g;
+        }
+    }
+    return best;
 }
 
 int k1_sm_count() {
@@ -386,8 +413,7 @@ Status launch_k1_staged(ctrecon_ctx* ctx, cudaStream_t s, const float* d_proj, i
     k.proj_view0 = proj_view0;
     k.c0 = c0; k.n = n;
     k.nstrips = YLp / kStrip;
-    // as many runs of views per strip as whole sets of strips fit on the SMs (one CTA each)
-    k.ngroups = std::max(1, std::min(n, k1_sm_count() / k.nstrips));
+    k.ngroups = staged_runs(k.nstrips, n, k1_sm_count());
     k.box_bytes = (uint32_t)(kRowW * ZL * 4);
     k.inv2dl = inv2dl;
     k.plane = plane;
