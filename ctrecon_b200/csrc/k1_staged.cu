@@ -14,18 +14,20 @@
 // The derivative of view p reads views pc - 1, pc, pc + 1 (pc = p clamped to [1, P - 2]) and p
 // itself, so walking the views in order, each view of the strip is copied in ONCE (rows
 // 0 .. ZL - 1, the strip's 32 columns plus 4 each side for the u stencil: the copies start on
-// a 16-byte boundary) into a ring of SLOTS slots, up to SLOTS - 3 views ahead of the view
-// being computed. The forward-rebin entries (the two weights and the two derivative rows of
+// a 16-byte boundary) into a ring of SLOTS slots, up to SLOTS - VIEWS - 2 views ahead of the
+// step being computed. The forward-rebin entries (the two weights and the two derivative rows of
 // each (kappa line, column)) of a thread's column and its warp's kappa lines stay in registers
 // for the whole run: the only global traffic of the loop is the tensor copies in and the
 // kappa-row stores out, and shared memory carries only the staged rows and the derivative.
 //
-// Per view: wait for the view the window gains; the derivative of the strip's ZL x 32 samples
-// into one of two shared buffers (a warp per ROWS rows, a lane per column, the v stencil's rows
-// in registers); ONE barrier; the copies of the views the next window frees; the AL x 32
-// kappa samples from that buffer (a warp per kappa line, the entries in registers),
-// stored de-interleaved as every Hilbert form reads them. The next view's derivative writes
-// the other buffer, so the rebin needs no barrier of its own.
+// A step takes VIEWS consecutive views: wait for the views its window gains; the derivative of
+// the strip's ZL x 32 samples of each view into one of two sets of VIEWS shared buffers (a warp
+// per ROWS rows, a lane per column, the v stencil's rows in registers); ONE barrier; the copies
+// of the views the next window frees; the AL x 32 kappa samples of each view from its buffer
+// (a warp per kappa line, the entries in registers), stored de-interleaved as every Hilbert
+// form reads them. The next step's derivatives write the other set, so the rebins need no
+// barrier of their own; taking several views a step shares the wait, the barrier and the loop
+// among them.
 #include "internal.h"
 #include "tc_util.cuh"
 
@@ -48,15 +50,16 @@ constexpr int kWarpsK1 = kThreadsK1 / 32;
 constexpr size_t kSmemBudget = 227 * 1024 - 128 - 128;  // less alignment slack and barriers
 
 // The two shapes of the kernel: derivative rows a warp takes at a time (ROWS), kappa lines per
-// warp with their entries in registers (LINES), views in the ring (SLOTS). Tall detectors (up
-// to 176 kappa lines) take 8 rows and 11 lines a warp; short ones (at most 64 rows and 96
-// kappa lines) 4 rows and 6 lines, so that all 16 warps share the derivative, no warp loads
-// entries of lines past AL, and the smaller staged views allow a deeper ring.
+// warp with their entries in registers (LINES), views in the ring (SLOTS), views a step
+// (VIEWS). Tall detectors (up to 176 kappa lines) take 8 rows and 11 lines a warp, 2 views a
+// step; short ones (at most 64 rows and 96 kappa lines) 4 rows and 6 lines, so that all 16
+// warps share the derivative and no warp loads entries of lines past AL, and 4 views a step,
+// which their smaller staged views leave room for.
 struct K1Shape {
-    int rows, lines, slots;
+    int rows, lines, slots, views;
 };
-constexpr K1Shape kTall{8, 11, 5};
-constexpr K1Shape kShort{4, 6, 8};
+constexpr K1Shape kTall{8, 11, 6, 2};
+constexpr K1Shape kShort{4, 6, 10, 4};
 
 struct K1sParams {
     int P, YL, ZL, AL, YLp;
@@ -113,16 +116,18 @@ __device__ __forceinline__ float deriv_sample(float pp, float pm, float ur, floa
     return fmaf(zc, vr - vl, g);
 }
 
-template <int MODE, int ROWS, int LINES, int SLOTS>
+template <int MODE, int ROWS, int LINES, int SLOTS, int VIEWS>
 __global__ void __launch_bounds__(kThreadsK1, 1)
 k_deriv_rebin_staged(const __grid_constant__ CUtensorMap pmap, const K1sParams k) {
+    // a step's window (VIEWS + 2 views) fits in the ring, so every wait has its copy issued
+    static_assert(SLOTS >= VIEWS + 2, "ring too small for a step");
     extern __shared__ __align__(128) unsigned char k1dyn[];
     __shared__ __align__(8) uint64_t full[SLOTS];
     unsigned char* base = k1dyn + ((128u - (tcu::smem_u32(k1dyn) & 127u)) & 127u);
     const int ZL = k.ZL, AL = k.AL, YL = k.YL, P = k.P;
     float* ring = reinterpret_cast<float*>(base);
-    float* gfb = ring + (size_t)SLOTS * k.slot_floats;  // two buffers of ZL x 32 samples
-    float* zs = gfb + (size_t)2 * ZL * kStrip;             // zcv
+    float* gfb = ring + (size_t)SLOTS * k.slot_floats;  // 2 x VIEWS buffers of ZL x 32 samples
+    float* zs = gfb + (size_t)2 * VIEWS * ZL * kStrip;     // zcv
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (tid == 0) {
         for (int s = 0; s < SLOTS; ++s) tcu::mbar_init(&full[s], 1);
@@ -188,77 +193,65 @@ k_deriv_rebin_staged(const __grid_constant__ CUtensorMap pmap, const K1sParams k
     const uint32_t ring_s = tcu::smem_u32(ring);
     const uint32_t slot_b = (uint32_t)k.slot_floats * 4u;
     const uint32_t gf_s = tcu::smem_u32(gfb);
-    const uint32_t gf_b = (uint32_t)(ZL * kStrip) * 4u;  // bytes between the two buffers
+    const uint32_t gf_b = (uint32_t)(ZL * kStrip) * 4u;  // bytes per derivative buffer
     constexpr uint32_t kRowB = kRowW * 4;                  // bytes per staged row
 
-    int waited = 0;  // copies (c = v - L0) below this are known complete
-    bool good = true;
-    for (int p = pfirst; p <= plast; ++p) {
-        const int pc = clamp_view(p, P);
-        // views pc - 1 .. pc + 1 (p is one of them) have landed: one new copy per view once the
-        // ring runs
-        bool ok = true;
-        while (ok && waited <= pc + 1 - L0) {
-            ok = tcu::mbar_wait(&full[waited % SLOTS], (uint32_t)(waited / SLOTS) & 1u, k.err, 31);
-            if (ok) ++waited;
-        }
-        const uint32_t gcur = gf_s + (uint32_t)((p - pfirst) & 1) * gf_b;
-        if (ok) {
-            const uint32_t Tm = ring_s + (uint32_t)((pc - 1 - L0) % SLOTS) * slot_b;
-            const uint32_t Tp = ring_s + (uint32_t)((pc + 1 - L0) % SLOTS) * slot_b;
-            const uint32_t Tv = ring_s + (uint32_t)((p - L0) % SLOTS) * slot_b;
-            const uint32_t tv = Tv + (uint32_t)oc * 4u, tp = Tp + (uint32_t)oc * 4u;
-            const uint32_t tm = Tm + (uint32_t)oc * 4u;
-            const uint32_t tl = Tv + (uint32_t)ol * 4u, tq = Tv + (uint32_t)orr * 4u;
-            const uint32_t gw = gcur + (uint32_t)lane * 4u;
-            for (int k0 = kb; k0 < ZL; k0 += kWarpsK1 * ROWS) {
-                if (k0 == kb && k0 >= 1 && k0 + ROWS + 1 <= ZL) {
-                    // no edge row: the v stencil is rows k - 1, k + 1; each half block loads
-                    // all its operands before it computes
+    // the derivative of view q (:52-95) into the buffer at gcur
+    auto derive = [&](int q, uint32_t gcur) {
+        const int qc = clamp_view(q, P);
+        const uint32_t Tm = ring_s + (uint32_t)((qc - 1 - L0) % SLOTS) * slot_b;
+        const uint32_t Tp = ring_s + (uint32_t)((qc + 1 - L0) % SLOTS) * slot_b;
+        const uint32_t Tv = ring_s + (uint32_t)((q - L0) % SLOTS) * slot_b;
+        const uint32_t tv = Tv + (uint32_t)oc * 4u, tp = Tp + (uint32_t)oc * 4u;
+        const uint32_t tm = Tm + (uint32_t)oc * 4u;
+        const uint32_t tl = Tv + (uint32_t)ol * 4u, tq = Tv + (uint32_t)orr * 4u;
+        const uint32_t gw = gcur + (uint32_t)lane * 4u;
+        for (int k0 = kb; k0 < ZL; k0 += kWarpsK1 * ROWS) {
+            if (k0 == kb && k0 >= 1 && k0 + ROWS + 1 <= ZL) {
+                // no edge row: the v stencil is rows k - 1, k + 1; each half block loads all
+                // its operands before it computes
 #pragma unroll
-                    for (int h = 0; h < ROWS; h += 4) {
-                        const uint32_t r0 = (uint32_t)(k0 + h) * kRowB;
-                        float w[6], fp[4], fm[4], fl[4], fq[4];
+                for (int h = 0; h < ROWS; h += 4) {
+                    const uint32_t r0 = (uint32_t)(k0 + h) * kRowB;
+                    float w[6], fp[4], fm[4], fl[4], fq[4];
 #pragma unroll
-                        for (int i = 0; i < 6; ++i) w[i] = lds_f32(tv + r0 - kRowB + i * kRowB);
+                    for (int i = 0; i < 6; ++i) w[i] = lds_f32(tv + r0 - kRowB + i * kRowB);
 #pragma unroll
-                        for (int i = 0; i < 4; ++i) {
-                            fp[i] = lds_f32(tp + r0 + i * kRowB);
-                            fm[i] = lds_f32(tm + r0 + i * kRowB);
-                            fq[i] = lds_f32(tq + r0 + i * kRowB);
-                            fl[i] = lds_f32(tl + r0 + i * kRowB);
-                        }
-#pragma unroll
-                        for (int i = 0; i < 4; ++i) {
-                            const float g = deriv_sample(fp[i], fm[i], fq[i], fl[i], cy.x,
-                                                         zcy[h + i], w[i + 2], w[i], k.inv2dl);
-                            sts_f32(gw + (uint32_t)((k0 + h + i) * kStrip) * 4u, real ? g : 0.f);
-                        }
+                    for (int i = 0; i < 4; ++i) {
+                        fp[i] = lds_f32(tp + r0 + i * kRowB);
+                        fm[i] = lds_f32(tm + r0 + i * kRowB);
+                        fq[i] = lds_f32(tq + r0 + i * kRowB);
+                        fl[i] = lds_f32(tl + r0 + i * kRowB);
                     }
-                } else {
-                    // the first or the last row (edge rule, :85-95), rows past 128, or past ZL
-                    for (int i = 0; i < ROWS; ++i) {
-                        const int kk = k0 + i;
-                        if (kk >= ZL) break;
-                        int kl = kk - 1, kr = kk + 1;
-                        if (kk < 2) { kl = 0; kr = 2; }
-                        else if (kk > ZL - 3) { kl = ZL - 3; kr = ZL - 1; }
-                        const uint32_t r = (uint32_t)kk * kRowB;
-                        const float g = deriv_sample(lds_f32(tp + r), lds_f32(tm + r),
-                                                     lds_f32(tq + r), lds_f32(tl + r), cy.x,
-                                                     zs[kk] * cy.y, lds_f32(tv + (uint32_t)kr * kRowB),
-                                                     lds_f32(tv + (uint32_t)kl * kRowB), k.inv2dl);
-                        sts_f32(gw + (uint32_t)(kk * kStrip) * 4u, real ? g : 0.f);
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) {
+                        const float g = deriv_sample(fp[i], fm[i], fq[i], fl[i], cy.x, zcy[h + i],
+                                                     w[i + 2], w[i], k.inv2dl);
+                        sts_f32(gw + (uint32_t)((k0 + h + i) * kStrip) * 4u, real ? g : 0.f);
                     }
+                }
+            } else {
+                // the first or the last row (edge rule, :85-95), rows past 128, or past ZL
+                for (int i = 0; i < ROWS; ++i) {
+                    const int kk = k0 + i;
+                    if (kk >= ZL) break;
+                    int kl = kk - 1, kr = kk + 1;
+                    if (kk < 2) { kl = 0; kr = 2; }
+                    else if (kk > ZL - 3) { kl = ZL - 3; kr = ZL - 1; }
+                    const uint32_t r = (uint32_t)kk * kRowB;
+                    const float g = deriv_sample(lds_f32(tp + r), lds_f32(tm + r), lds_f32(tq + r),
+                                                 lds_f32(tl + r), cy.x, zs[kk] * cy.y,
+                                                 lds_f32(tv + (uint32_t)kr * kRowB),
+                                                 lds_f32(tv + (uint32_t)kl * kRowB), k.inv2dl);
+                    sts_f32(gw + (uint32_t)(kk * kStrip) * 4u, real ? g : 0.f);
                 }
             }
         }
-        // every thread's derivative is in place and its reads of the ring are done
-        if (!__syncthreads_and(ok)) { good = false; break; }
-        if (p < plast) issue_upto(clamp_view(p + 1, P) - 1 + SLOTS - 1);
-        // forward rebin + pre-weight (:131-153) into the chunk's kappa rows: every line's two
-        // derivative samples loaded first (lines past AL read row 0 with zero weights), then
-        // the sums, then the stores
+    };
+    // the forward rebin + pre-weight (:131-153) of view q from the buffer at gcur into the
+    // chunk's kappa rows: every line's two derivative samples loaded first (lines past AL read
+    // row 0 with zero weights), then the sums, then the stores
+    auto rebin = [&](int q, uint32_t gcur) {
         float v[LINES];
         {
             float g0[LINES], g1[LINES];
@@ -270,7 +263,7 @@ k_deriv_rebin_staged(const __grid_constant__ CUtensorMap pmap, const K1sParams k
 #pragma unroll
             for (int i = 0; i < LINES; ++i) v[i] = fmaf(te[i].x, g0[i], te[i].y * g1[i]);
         }
-        const size_t x0 = (size_t)(p - k.c0) * AL * k.YLp + (size_t)warp * k.YLp + jx;
+        const size_t x0 = (size_t)(q - k.c0) * AL * k.YLp + (size_t)warp * k.YLp + jx;
         if constexpr (MODE == CTRECON_HILBERT_BF16X3) {
             // lanes l and l + 2 hold neighbouring elements of a de-interleaved row: lanes with
             // bit 1 clear store the two hi values at their own element, the others the two lo
@@ -302,6 +295,33 @@ k_deriv_rebin_staged(const __grid_constant__ CUtensorMap pmap, const K1sParams k
                 if (i < nl) *o = r;
             }
         }
+    };
+
+    // VIEWS views a step: their derivatives into one set of VIEWS buffers, one barrier, the
+    // copies the next step's window frees, their rebins; the next step's derivatives write the
+    // other set, so the rebins need no barrier of their own
+    int waited = 0;  // copies (c = v - L0) below this are known complete
+    bool good = true;
+    for (int p = pfirst; p <= plast; p += VIEWS) {
+        const int pe = p + VIEWS - 1 < plast ? p + VIEWS - 1 : plast;  // the step's last view
+        // views clamp(p) - 1 .. clamp(pe) + 1 have landed
+        bool ok = true;
+        while (ok && waited <= clamp_view(pe, P) + 1 - L0) {
+            ok = tcu::mbar_wait(&full[waited % SLOTS], (uint32_t)(waited / SLOTS) & 1u, k.err, 31);
+            if (ok) ++waited;
+        }
+        const uint32_t gset = gf_s + (uint32_t)(((p - pfirst) / VIEWS) & 1) * VIEWS * gf_b;
+        if (ok) {
+#pragma unroll
+            for (int v = 0; v < VIEWS; ++v)
+                if (p + v <= pe) derive(p + v, gset + v * gf_b);
+        }
+        // every thread's derivatives are in place and its reads of the ring are done
+        if (!__syncthreads_and(ok)) { good = false; break; }
+        if (pe < plast) issue_upto(clamp_view(pe + 1, P) - 1 + SLOTS - 1);
+#pragma unroll
+        for (int v = 0; v < VIEWS; ++v)
+            if (p + v <= pe) rebin(p + v, gset + v * gf_b);
     }
     if (!good && tid == 0) {
         // no copy may still be writing shared memory when the CTA exits: wait (bounded) for
@@ -322,7 +342,8 @@ size_t staged_smem(int ZL, int AL, int* slot_floats) {
     const K1Shape sh = staged_shape(ZL, AL);
     *slot_floats = (ZL * kRowW + 31) / 32 * 32;
     if (AL > sh.lines * kWarpsK1) return 0;
-    const size_t bytes = (size_t)sh.slots * *slot_floats * 4 + (size_t)2 * ZL * kStrip * 4 +
+    const size_t bytes = (size_t)sh.slots * *slot_floats * 4 +
+                         (size_t)2 * sh.views * ZL * kStrip * 4 +
                          (size_t)ZL * 4;
     return bytes <= kSmemBudget ? bytes + 128 : 0;
 }
@@ -376,7 +397,7 @@ template <int MODE, bool TALL>
 Status run_staged(const CUtensorMap& map, const K1sParams& k, int grid, size_t smem,
                   cudaStream_t s) {
     constexpr K1Shape sh = TALL ? kTall : kShort;
-    auto kern = k_deriv_rebin_staged<MODE, sh.rows, sh.lines, sh.slots>;
+    auto kern = k_deriv_rebin_staged<MODE, sh.rows, sh.lines, sh.slots, sh.views>;
     CTR_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     kern<<<grid, kThreadsK1, smem, s>>>(map, k);
     return Status::Ok();
