@@ -988,7 +988,8 @@ def kernel_rooflines(s, kt, steps, updates, peaks, sm_mhz, hil):
         if kind == "deriv_rebin":
             b = P * (4 * YL * ZL + 4 * AL * YLp)
             r.update(bound="hbm", achieved_gbs=b / t / 1e9, peak_gbs=peaks["hbm_gbs"],
-                     frac=b / t / 1e9 / peaks["hbm_gbs"], algorithmic_bytes=b)
+                     frac=b / t / 1e9 / peaks["hbm_gbs"], algorithmic_bytes=b,
+                     peak_source=peaks["source"])
         elif kind == "hilbert_tc":
             f = 2.0 * YL * YL * AL * P
             # the parity-split form: two products of (YLp/2 rows padded to 128) x YLp/2 per
@@ -1005,8 +1006,8 @@ def kernel_rooflines(s, kt, steps, updates, peaks, sm_mhz, hil):
             r.update(bound="tensor", achieved_tflops=f / t / 1e12, peak_tflops=pk,
                      frac=f / t / 1e12 / pk, executed_tflops=ex / t / 1e12,
                      executed_frac=ex / t / 1e12 / pk, algorithmic_flop=f,
-                     peak_note="BF16 burst of measured" if hil == "bf16x3" else
-                     "half the BF16 burst of measured (TF32 rate)")
+                     peak_note=(f"BF16 burst of {peaks['source']}" if hil == "bf16x3" else
+                                f"half the BF16 burst of {peaks['source']} (TF32 rate)"))
         elif kind == "hilbert_simt":
             fma = AL * YL * (YL / 2.0) * P
             pk = SMS * FP32_LANES_PER_SM * clk
@@ -1015,7 +1016,8 @@ def kernel_rooflines(s, kt, steps, updates, peaks, sm_mhz, hil):
         elif kind == "cell_records":
             b = P * (YL - 1) * (ZL - 1) * 20
             r.update(bound="hbm", achieved_gbs=b / t / 1e9, peak_gbs=peaks["hbm_gbs"],
-                     frac=b / t / 1e9 / peaks["hbm_gbs"], algorithmic_bytes=b)
+                     frac=b / t / 1e9 / peaks["hbm_gbs"], algorithmic_bytes=b,
+                     peak_source=peaks["source"])
         elif kind == "backproject":
             r.update(gups=updates / t / 1e9,
                      gather_equivalent_gbs=BYTES_PER_UPDATE * updates / t / 1e9)
@@ -1338,7 +1340,7 @@ def run_headline(args):
                                  "KatsevichBkProj.cpp:253-256); the taps come from shared "
                                  "memory, so this is not an HBM bound",
                         "achieved_gbs": BYTES_PER_UPDATE * updates / t_bp / 1e9,
-                        "hbm_peak_gbs": peaks["hbm_gbs"]}}
+                        "hbm_peak_gbs": peaks["hbm_gbs"], "hbm_peak_source": peaks["source"]}}
 
     # ---- CPU baseline (rank 0, N = 1): the FP64 oracle restatement on a bounded sample -----------
     cpu = None
