@@ -1254,12 +1254,20 @@ def run_headline(args):
         for _ in range(e2e_steps):
             ctx.recon_host(fpar, geom, np_proj, np_img)
         t_e2e = max_over_ranks((time.perf_counter() - t0) / e2e_steps, ws)
+        # the FP64 projections cross to the device as FP32 when host threads convert them
+        # (CTRECON_OPT_HOST_THREADS, default: the host's threads, at most 16)
+        host_threads = ctx.get_option(_lib.OPT_HOST_THREADS)
+        if host_threads < 0:
+            host_threads = min(16, os.cpu_count() or 4)
+        proj_bytes = (4 if host_threads > 0 else 8) * nproj
         e2e = {"value": ws * updates / t_e2e / 1e9, "unit": "GUPS",
-               "h2d_bytes_per_step": 8 * (nproj + nvox), "d2h_bytes_per_step": 8 * nvox,
-               "s_per_vol": t_e2e, "steps": e2e_steps,
+               "h2d_bytes_per_step": proj_bytes + 8 * nvox, "d2h_bytes_per_step": 8 * nvox,
+               "s_per_vol": t_e2e, "steps": e2e_steps, "host_threads": host_threads,
                "path": "ctrecon_recon_host_f64 (filter + backprojection in one call, "
                        "FunctionKat_v6.m:85-113 without the FProj round trip), pinned FP64 host "
-                       "buffers"}
+                       "buffers, the projections converted to FP32 by host threads slot by slot "
+                       "as they go up (FP64 copies converted on the device when host_threads "
+                       "is 0)"}
         # the two MEX-equivalent calls, FProj through the host in between
         ctx.filter_host(fpar, np_proj, np_fproj)
         ctx.bkproj_host(geom, np_fproj, np_img)

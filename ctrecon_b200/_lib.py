@@ -34,6 +34,7 @@ OPT_KERNEL_TIMING = 9
 OPT_TC_FORM = 10
 TC_PARITY_SPLIT, TC_SINGLE_PASS = 0, 1
 OPT_K1_FORM = 11
+OPT_HOST_THREADS = 12
 K1_STAGED, K1_PER_VIEW = 0, 1
 KERNEL_KINDS = ("deriv_rebin", "hilbert_simt", "hilbert_tc", "pi_solve", "cell_records",
                 "backproject")

@@ -50,6 +50,18 @@ struct DevBuf {
     void release();
     template <class T> T* as() const { return static_cast<T*>(ptr); }
 };
+// Page-locked host memory of the library (cudaHostAlloc), kept for reuse like a DevBuf.
+struct PinnedBuf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    PinnedBuf() = default;
+    PinnedBuf(const PinnedBuf&) = delete;
+    PinnedBuf& operator=(const PinnedBuf&) = delete;
+    ~PinnedBuf();
+    Status ensure(size_t b, const char* what);
+    void release();
+    template <class T> T* as() const { return static_cast<T*>(ptr); }
+};
 // Number of device allocations made by DevBuf::ensure so far (process-wide); a captured CUDA
 // graph that baked in work-buffer pointers is stale once this has moved.
 unsigned long long devbuf_epoch();
@@ -242,11 +254,13 @@ struct ctrecon_ctx {
     int opt_kernel_timing = 0;                // CTRECON_OPT_KERNEL_TIMING
     int opt_tc_form = CTRECON_TC_PARITY_SPLIT;  // CTRECON_OPT_TC_FORM
     int opt_k1_form = CTRECON_K1_STAGED;        // CTRECON_OPT_K1_FORM
+    int opt_host_threads = -1;                  // CTRECON_OPT_HOST_THREADS
     std::vector<ctr::KernelSpan> kspans;      // timed launches since the last query
     std::vector<cudaEvent_t> kev_free;        // timing events for reuse
     cudaStream_t host_stream = nullptr;  // stream for the synchronous host calls
     cudaStream_t up_stream = nullptr;    // host -> device copies of the host calls
     cudaStream_t down_stream = nullptr;  // device -> host copies of the host calls
+    cudaStream_t up2_stream = nullptr;   // host -> device copies of host-converted projections
     std::vector<cudaEvent_t> events;     // reusable (timing-disabled) events of the host calls
     // plans by geometry, most recently used first; a plan is never rebuilt in place (kernels
     // still queued may read it) and evicting one synchronises the device first
@@ -257,6 +271,7 @@ struct ctrecon_ctx {
     ctr::DevBuf ws_count;    // update counter
     ctr::DevBuf ws_a, ws_b, ws_c, ws_d;  // host-call staging (f64 in, f32, f32 out, f64 out)
     ctr::DevBuf ws_e;        // FP64 image of the host backprojection
+    ctr::PinnedBuf pin_ring; // FP32 projection slots of the one-call path's host conversion
     ctr::DevBuf ws_panel;    // arc-to-flat rebin table
     ctr::DevBuf ws_dual;     // second filter result of FilteringMode 1
     ctr::DevBuf ws_ell;      // phantom ellipsoids

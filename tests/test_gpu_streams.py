@@ -110,6 +110,41 @@ def test_host_calls_pinned_equal_pageable(torch_mod):
         assert rel < 1e-6
 
 
+@pytest.mark.parametrize("cfg", ["c1", "tiny"])
+def test_recon_host_conversion_forms_equal(torch_mod, cfg):
+    """ctrecon_recon_host_f64 converts the FP64 projections to FP32 either with host threads
+    (CTRECON_OPT_HOST_THREADS > 0, default: slots of 64 views copied up as they are converted)
+    or on the device (0); the casts round alike, so the image is the same bit for bit, for
+    thread counts that do and do not divide a slot, pinned and pageable, on repeated calls."""
+    torch = torch_mod
+    import ctrecon_b200 as ct
+    from ctrecon_b200 import _lib
+    from ctrecon_b200.geometry import config, small_config
+    s = config("c1") if cfg == "c1" else small_config(name="tiny")
+    with ct.Context(0) as cx:
+        assert cx.get_option(_lib.OPT_HOST_THREADS) == -1
+        d = torch.empty(s.proj_shape, dtype=torch.float32, device="cuda")
+        cx.phantom_dev(s.geom_struct(), s.ellipsoids(), d)
+        torch.cuda.synchronize()
+        proj = d.cpu().numpy().astype(np.float64)
+        proj_pin = torch.from_numpy(proj).pin_memory().numpy()
+        p = ct.scan_filter_params(s)
+        out = {}
+        for th in (0, -1, 1, 3, 7, 16):
+            cx.set_option(_lib.OPT_HOST_THREADS, th)
+            assert cx.get_option(_lib.OPT_HOST_THREADS) == th
+            for src in (proj, proj_pin):
+                for _ in range(2):
+                    img = np.full(s.vol_shape, 7.25)
+                    cx.recon_host(p, s.geom_struct(), src, img)
+                    out.setdefault(th, img)
+                    assert np.array_equal(img, out[th]), th
+        for th in out:
+            assert np.array_equal(out[th], out[0]), th
+        with pytest.raises(_lib.CtreconError):
+            cx.set_option(_lib.OPT_HOST_THREADS, -2)
+
+
 def test_host_bkproj_fifth_form(torch_mod):
     """The host backprojection accumulates ~2048-view windows; with the fifth form each
     window's cell records are built for that window only."""
