@@ -14,6 +14,10 @@
 #include <thread>
 #include <vector>
 
+#if defined(__SSE2__)
+#include <emmintrin.h>
+#endif
+
 namespace ctr {
 
 DevBuf::~DevBuf() { release(); }
@@ -892,6 +896,25 @@ ctrecon_status ctrecon_bkproj_host_f64(ctrecon_ctx* ctx, const ctrecon_bp_geom* 
 constexpr int kSlotViews = 64;
 constexpr int kRingSlots = 8;
 
+// dst[i] = (float)src[i], the FP32 results written around the caches (they only go on to
+// the device): no read for ownership of the slot lines, a quarter less memory traffic. The
+// SSE2 conversion rounds to nearest even, as the cast does.
+static void convert_stream(const double* src, float* dst, size_t n) {
+#if defined(__SSE2__)
+    size_t i = 0;
+    for (; i < n && ((uintptr_t)(dst + i) & 15u) != 0; ++i) dst[i] = (float)src[i];
+    for (; i + 4 <= n; i += 4) {
+        const __m128 lo = _mm_cvtpd_ps(_mm_loadu_pd(src + i));
+        const __m128 hi = _mm_cvtpd_ps(_mm_loadu_pd(src + i + 2));
+        _mm_stream_ps(dst + i, _mm_movelh_ps(lo, hi));
+    }
+    for (; i < n; ++i) dst[i] = (float)src[i];
+    _mm_sfence();  // the streamed stores are visible before the slot is handed to the copy
+#else
+    for (size_t i = 0; i < n; ++i) dst[i] = (float)src[i];
+#endif
+}
+
 class HostConverter {
 public:
     ~HostConverter() { stop(); }
@@ -988,7 +1011,7 @@ private:
             const size_t a = n * t / nthreads_, b = n * (t + 1) / nthreads_;
             const double* s = src_ + v0 * S_;
             float* d = slot(q);
-            for (size_t i = a; i < b; ++i) d[i] = (float)s[i];
+            convert_stream(s + a, d + a, b - a);
             {
                 std::lock_guard<std::mutex> lk(mu_);
                 if (stopping_) return;
