@@ -715,184 +715,14 @@ static Status event_at(ctrecon_ctx* ctx, size_t i, cudaEvent_t* out) {
     return Status::Ok();
 }
 
-// Uploads proj (FP64 host) and filters it into ctx->ws_c (FP32, device); if fproj_host is not
-// NULL the result also comes down into it (FP64). Returns after enqueueing, except that it
-// waits for the down copies when fproj_host is given. The host stream holds the filter work.
-static Status host_filter_pipeline(ctrecon_ctx* ctx, const ctrecon_filter_params& p,
-                                   const double* proj, double* fproj_host) {
-    FilterPlan* plan = nullptr;
-    CTR_TRY(get_filter_plan(ctx, p, &plan));
-    const int P = p.proj_number;
-    const size_t S = (size_t)p.yl * p.zl, n = S * P;
-    CTR_TRY(ctx->ws_a.ensure(n * sizeof(double), "FP64 staging"));
-    CTR_TRY(ctx->ws_b.ensure(n * sizeof(float), "projections"));
-    CTR_TRY(ctx->ws_c.ensure(n * sizeof(float), "filtered projections"));
-    if (fproj_host) CTR_TRY(ctx->ws_d.ensure(n * sizeof(double), "FP64 result staging"));
-    const int nch = (P + kHostChunkViews - 1) / kHostChunkViews;
-    cudaStream_t up = ctx->up_stream, comp = ctx->host_stream, down = ctx->down_stream;
-    // the up stream carries copies only: a conversion kernel there would wait for SMs behind
-    // the filter and stall the copy engine; each chunk is converted on the compute stream
-    for (int c = 0; c < nch; ++c) {
-        const size_t v0 = (size_t)c * kHostChunkViews, v1 = std::min<size_t>(P, v0 + kHostChunkViews);
-        CTR_CUDA(cudaMemcpyAsync(ctx->ws_a.as<double>() + v0 * S, proj + v0 * S,
-                                 (v1 - v0) * S * sizeof(double), cudaMemcpyHostToDevice, up));
-        cudaEvent_t e = nullptr;
-        CTR_TRY(event_at(ctx, c, &e));
-        CTR_CUDA(cudaEventRecord(e, up));
-    }
-    int converted = 0;  // chunks [0, converted) are in FP32
-    for (int c = 0; c < nch; ++c) {
-        const int v0 = c * kHostChunkViews, v1 = std::min(P, v0 + kHostChunkViews);
-        // this chunk and the first view of the next (derivative neighbour)
-        const int need = std::min(c + 1, nch - 1);
-        for (; converted <= need; ++converted) {
-            cudaEvent_t e = nullptr;
-            CTR_TRY(event_at(ctx, converted, &e));
-            CTR_CUDA(cudaStreamWaitEvent(comp, e, 0));
-            const size_t w0 = (size_t)converted * kHostChunkViews;
-            const size_t w1 = std::min<size_t>(P, w0 + kHostChunkViews);
-            CTR_TRY(launch_convert_f64_to_f32(comp, ctx->ws_a.as<double>() + w0 * S,
-                                              ctx->ws_b.as<float>() + w0 * S, (w1 - w0) * S));
-        }
-        CTR_TRY(launch_filter(ctx, comp, *plan, ctx->ws_b.as<float>(), 0, P,
-                              ctx->ws_c.as<float>(), 0, v0, v1));
-        if (fproj_host) {
-            const size_t o = (size_t)v0 * S, m = (size_t)(v1 - v0) * S;
-            CTR_TRY(launch_convert_f32_to_f64(comp, ctx->ws_c.as<float>() + o,
-                                              ctx->ws_d.as<double>() + o, m));
-            cudaEvent_t done = nullptr;
-            CTR_TRY(event_at(ctx, nch + c, &done));
-            CTR_CUDA(cudaEventRecord(done, comp));
-            CTR_CUDA(cudaStreamWaitEvent(down, done, 0));
-            CTR_CUDA(cudaMemcpyAsync(fproj_host + o, ctx->ws_d.as<double>() + o,
-                                     m * sizeof(double), cudaMemcpyDeviceToHost, down));
-        }
-    }
-    if (fproj_host) {
-        CTR_CUDA(cudaStreamSynchronize(down));
-        CTR_CUDA(cudaStreamSynchronize(comp));
-    }
-    return Status::Ok();
-}
-
-static Status check_filter_bp_shapes(const ctrecon_filter_params& p, const BPGeom& g) {
-    if (p.yl != g.YL || p.zl != g.ZL || p.proj_number != g.ProjNum)
-        return make_status(CTRECON_ERR_INVALID_ARGUMENT,
-                           "filter and backprojection geometries disagree on YL/ZL/views");
-    return Status::Ok();
-}
-
-ctrecon_status ctrecon_filter_host_f64(ctrecon_ctx* ctx, const ctrecon_filter_params* p,
-                                       const double* proj, double* fproj) {
-    if (!ctx) return CTRECON_ERR_INVALID_ARGUMENT;
-    API_BEGIN
-    if (!p || !proj || !fproj)
-        return finish(ctx, make_status(CTRECON_ERR_INVALID_ARGUMENT, "NULL argument"));
-    Status s = use_device(ctx);
-    if (s.ok()) s = host_reset(ctx);
-    if (s.ok()) s = host_filter_pipeline(ctx, *p, proj, fproj);
-    if (s.ok()) s = check_device_flag(ctx);
-    return finish(ctx, s);
-    API_END(ctx)
-}
-
-// KatsevichBkProj with FProj from host memory, with the transfer overlapping the work: the
-// image goes up first, the PI solve runs meanwhile, the valid voxels are zeroed, then the views
-// go up in windows of about 2048 and each window is backprojected (accumulating) as soon as it
-// is resident; the image comes down at the end. Summing per window reorders the FP32 sums of a
-// voxel (the windows' partial sums are added in FP64).
-static Status host_bkproj_windowed(ctrecon_ctx* ctx, BPPlan& plan, const double* fproj,
-                                   double* image) {
-    cudaStream_t up = ctx->up_stream, comp = ctx->host_stream, side = ctx->down_stream;
-    const int P = plan.g.ProjNum;
-    const size_t S = (size_t)plan.g.YL * plan.g.ZL, n = S * P;
-    const size_t nvox = (size_t)plan.kp.NX * plan.kp.NY * plan.kp.NZ;
-    CTR_TRY(ctx->ws_a.ensure(n * sizeof(double), "FP64 staging"));
-    CTR_TRY(ctx->ws_c.ensure(n * sizeof(float), "filtered projections"));
-    CTR_TRY(ctx->ws_pitab.ensure(nvox * sizeof(PiRecord), "PI table"));
-    CTR_TRY(ctx->ws_e.ensure(nvox * sizeof(double), "FP64 image"));
-    cudaEvent_t pi_done = nullptr, img_up = nullptr;
-    CTR_TRY(event_at(ctx, 0, &pi_done));
-    CTR_TRY(event_at(ctx, 1, &img_up));
-    CTR_TRY(launch_pi(ctx, side, plan, ctx->ws_pitab.as<PiRecord>(), nullptr));
-    CTR_CUDA(cudaEventRecord(pi_done, side));
-    CTR_CUDA(cudaMemcpyAsync(ctx->ws_e.ptr, image, nvox * sizeof(double), cudaMemcpyHostToDevice, up));
-    CTR_CUDA(cudaEventRecord(img_up, up));
-    CTR_CUDA(cudaStreamWaitEvent(comp, pi_done, 0));
-    CTR_CUDA(cudaStreamWaitEvent(comp, img_up, 0));
-    CTR_TRY(launch_zero_valid_f64(comp, ctx->ws_pitab.as<PiRecord>(), ctx->ws_e.as<double>(), nvox));
-    // windows: whole upload chunks, about 2048 views each
-    const int per_win = std::max(kHostChunkViews, (2048 / kHostChunkViews) * kHostChunkViews);
-    const BPParams saved = plan.kp;
-    Status st;
-    int w = 0;
-    for (int v0 = 0; st.ok() && v0 < P; v0 += per_win, ++w) {
-        const int v1 = std::min(P, v0 + per_win);
-        for (int c0 = v0; st.ok() && c0 < v1; c0 += kHostChunkViews) {
-            const size_t m = (size_t)(std::min(v1, c0 + kHostChunkViews) - c0) * S;
-            cudaError_t e = cudaMemcpyAsync(ctx->ws_a.as<double>() + (size_t)c0 * S,
-                                            fproj + (size_t)c0 * S, m * sizeof(double),
-                                            cudaMemcpyHostToDevice, up);
-            if (e != cudaSuccess) st = cuda_status(e, "FProj upload");
-        }
-        cudaEvent_t ev = nullptr;
-        if (st.ok()) st = event_at(ctx, 2 + (size_t)w, &ev);
-        if (st.ok()) {
-            cudaError_t e = cudaEventRecord(ev, up);
-            if (e == cudaSuccess) e = cudaStreamWaitEvent(comp, ev, 0);
-            if (e != cudaSuccess) st = cuda_status(e, "window event");
-        }
-        // the window's conversion on the compute stream (copies only on the up stream: a
-        // kernel there would wait for SMs behind the backprojection and stall the copy engine)
-        if (st.ok())
-            st = launch_convert_f64_to_f32(comp, ctx->ws_a.as<double>() + (size_t)v0 * S,
-                                           ctx->ws_c.as<float>() + (size_t)v0 * S,
-                                           (size_t)(v1 - v0) * S);
-        if (st.ok()) {
-            plan.kp.win0 = v0;
-            plan.kp.win1 = v1 - 1;
-            plan.kp.accum = 1;
-            st = launch_bkproj_f64out(ctx, comp, plan, ctx->ws_c.as<float>(),
-                                      ctx->ws_pitab.as<PiRecord>(), ctx->ws_e.as<double>());
-            plan.kp = saved;
-        }
-    }
-    plan.kp = saved;
-    CTR_TRY(st);
-    CTR_CUDA(cudaMemcpyAsync(image, ctx->ws_e.ptr, nvox * sizeof(double), cudaMemcpyDeviceToHost, comp));
-    CTR_CUDA(cudaStreamSynchronize(comp));
-    CTR_CUDA(cudaStreamSynchronize(side));
-    CTR_CUDA(cudaStreamSynchronize(up));
-    return check_device_flag(ctx);
-}
-
-ctrecon_status ctrecon_bkproj_host_f64(ctrecon_ctx* ctx, const ctrecon_bp_geom* g,
-                                       const double* fproj, double* image) {
-    if (!ctx) return CTRECON_ERR_INVALID_ARGUMENT;
-    API_BEGIN
-    if (!g || !fproj || !image)
-        return finish(ctx, make_status(CTRECON_ERR_INVALID_ARGUMENT, "NULL argument"));
-    Status s = use_device(ctx);
-    BPPlan* plan = nullptr;
-    if (s.ok()) s = get_bp_plan(ctx, *g, &plan);
-    if (s.ok()) s = host_reset(ctx);
-    if (s.ok()) s = host_bkproj_windowed(ctx, *plan, fproj, image);
-    return finish(ctx, s);
-    API_END(ctx)
-}
-
-// The whole chain with FP64 host buffers (FunctionKat_v6.m:85-113 without the FProj round
-// trip), pipelined so that the host copies hide the work: the image goes up first and the PI
-// solve runs beside the uploads; the projections go up in chunks, each chunk is converted and
-// filtered as soon as it and its neighbour view are resident, and each window of about 2048
-// views is backprojected (accumulating into the zeroed valid voxels) as soon as its views are
-// filtered, while later chunks are still on their way; the image comes down at the end.
-// Host-side FP64 -> FP32 conversion of the one-call path's projections. Worker threads convert
-// slots of kSlotViews views into a ring of kRingSlots page-locked FP32 slots (ctx->pin_ring),
-// each worker a fixed share of every slot; the calling thread copies each slot to the device
-// as soon as every worker is done with it (issue_upto), and a worker reuses a slot only after
-// the copy out of it has completed. The FP32 values are the round-to-nearest casts the device
-// conversion makes, so the result is the same bit for bit; half the bytes cross the host link.
+// Host-side FP64 -> FP32 conversion of the host calls' views (projections, or filtered
+// projections for the backprojection). Worker threads convert slots of kSlotViews views into a
+// ring of kRingSlots page-locked FP32 slots (ctx->pin_ring), each worker a fixed share of every
+// slot; the calling thread copies each slot to the device as soon as every worker is done with
+// it (issue_upto), and a worker reuses a slot only after the copy out of it has completed. The
+// FP32 values are the round-to-nearest casts the device conversion makes, so the result is the
+// same bit for bit; half the bytes cross the host link, and pageable host arrays are read by
+// the threads at memory speed instead of going through the driver's staged copies.
 constexpr int kSlotViews = 64;
 constexpr int kRingSlots = 8;
 
@@ -1038,11 +868,382 @@ private:
     std::string why_;
 };
 
+// dst[i] = (double)src[i] (exact), the FP64 results written around the caches.
+static void widen_stream(const float* src, double* dst, size_t n) {
+#if defined(__SSE2__)
+    size_t i = 0;
+    if (((uintptr_t)dst & 7u) == 0) {
+        for (; i < n && ((uintptr_t)(dst + i) & 15u) != 0; ++i) dst[i] = (double)src[i];
+        for (; i + 2 <= n; i += 2) {
+            const __m128 f = _mm_castpd_ps(_mm_load_sd(reinterpret_cast<const double*>(src + i)));
+            _mm_stream_pd(dst + i, _mm_cvtps_pd(f));
+        }
+    }
+    for (; i < n; ++i) dst[i] = (double)src[i];
+    _mm_sfence();
+#else
+    for (size_t i = 0; i < n; ++i) dst[i] = (double)src[i];
+#endif
+}
+
+// The reverse of HostConverter, for results going to pageable host arrays: each slot of
+// kSlotViews FP32 views comes down from the device into a ring of kRingSlots page-locked slots
+// (ctx->pin_ring_down) on the down stream, and worker threads widen it to FP64 into the
+// caller's array; the calling thread reuses a slot only after the workers are done with it.
+// Half the bytes cross the host link, and the pageable array is written by the threads at
+// memory speed instead of through the driver's staged copies.
+class HostWidener {
+public:
+    ~HostWidener() { stop(); }
+
+    Status start(ctrecon_ctx* ctx, const float* d_src, double* dst, size_t S, int nviews,
+                 int threads, cudaStream_t down) {
+        src_ = d_src;
+        dst_ = dst;
+        S_ = S;
+        down_ = down;
+        device_ = ctx->device;
+        for (int v = 0; v < nviews; v += kSlotViews)
+            slots_.push_back({v, std::min(kSlotViews, nviews - v)});
+        nslot_ = (int)slots_.size();
+        CTR_TRY(ctx->pin_ring_down.ensure((size_t)kRingSlots * kSlotViews * S * sizeof(float),
+                                          "widening ring"));
+        ring_ = ctx->pin_ring_down.as<float>();
+        for (cudaEvent_t& e : ev_) {
+            if (!e) CTR_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        }
+        parts_.assign(nslot_, 0);
+        nthreads_ = threads;
+        for (int t = 0; t < threads; ++t) workers_.emplace_back([this, t] { work(t); });
+        return Status::Ok();
+    }
+
+    // enqueues on the down stream, after `ready` (recorded where views [0, v) of d_src are
+    // final), the copies of every slot below view v, each once its ring slot is free again
+    Status issue_upto(int v, cudaEvent_t ready) {
+        bool waited = false;
+        while (issued_ < nslot_ && slots_[issued_].first < v) {
+            const int q = issued_;
+            if (q >= kRingSlots) {
+                std::unique_lock<std::mutex> lk(mu_);
+                cv_.wait(lk, [&] { return parts_[q - kRingSlots] == nthreads_ || failed_; });
+                if (failed_) return make_status(CTRECON_ERR_CUDA, "host widening: " + why_);
+            }
+            if (!waited) {
+                CTR_CUDA(cudaStreamWaitEvent(down_, ready, 0));
+                waited = true;
+            }
+            const size_t v0 = (size_t)slots_[q].first, nv = (size_t)slots_[q].second;
+            CTR_CUDA(cudaMemcpyAsync(slot(q), src_ + v0 * S_, nv * S_ * sizeof(float),
+                                     cudaMemcpyDeviceToHost, down_));
+            CTR_CUDA(cudaEventRecord(ev_[q % kRingSlots], down_));
+            {
+                std::lock_guard<std::mutex> lk(mu_);
+                ++issued_;
+            }
+            cv_.notify_all();
+        }
+        return Status::Ok();
+    }
+
+    // waits until every slot is widened into the caller's array
+    Status finish() {
+        {
+            std::unique_lock<std::mutex> lk(mu_);
+            cv_.wait(lk, [&] {
+                return failed_ || nslot_ == 0 || parts_[nslot_ - 1] == nthreads_;
+            });
+            if (failed_) return make_status(CTRECON_ERR_CUDA, "host widening: " + why_);
+        }
+        stop();
+        return Status::Ok();
+    }
+
+    // joins the workers (abandoning what they have not widened)
+    void stop() {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            stopping_ = true;
+        }
+        cv_.notify_all();
+        for (std::thread& w : workers_) w.join();
+        workers_.clear();
+        for (cudaEvent_t& e : ev_) {
+            if (e) {
+                cudaEventSynchronize(e);  // no copy may still write the ring
+                cudaEventDestroy(e);
+            }
+            e = nullptr;
+        }
+    }
+
+private:
+    float* slot(int q) const { return ring_ + (size_t)(q % kRingSlots) * kSlotViews * S_; }
+
+    void work(int t) {
+        cudaSetDevice(device_);
+        for (int q = 0; q < nslot_; ++q) {
+            {
+                std::unique_lock<std::mutex> lk(mu_);
+                cv_.wait(lk, [&] { return issued_ > q || stopping_ || failed_; });
+                if (stopping_ || failed_) return;
+            }
+            const cudaError_t e = cudaEventSynchronize(ev_[q % kRingSlots]);
+            if (e != cudaSuccess) {
+                std::lock_guard<std::mutex> lk(mu_);
+                failed_ = true;
+                why_ = cudaGetErrorString(e);
+                cv_.notify_all();
+                return;
+            }
+            const size_t v0 = (size_t)slots_[q].first, n = (size_t)slots_[q].second * S_;
+            const size_t a = n * t / nthreads_, b = n * (t + 1) / nthreads_;
+            widen_stream(slot(q) + a, dst_ + v0 * S_ + a, b - a);
+            {
+                std::lock_guard<std::mutex> lk(mu_);
+                ++parts_[q];
+            }
+            cv_.notify_all();
+        }
+    }
+
+    const float* src_ = nullptr;
+    double* dst_ = nullptr;
+    float* ring_ = nullptr;
+    size_t S_ = 0;
+    std::vector<std::pair<int, int>> slots_;
+    int nslot_ = 0, nthreads_ = 0, device_ = 0;
+    cudaStream_t down_ = nullptr;
+    cudaEvent_t ev_[kRingSlots] = {};
+    std::vector<std::thread> workers_;
+    std::mutex mu_;
+    std::condition_variable cv_;
+    std::vector<int> parts_;
+    int issued_ = 0;
+    bool stopping_ = false, failed_ = false;
+    std::string why_;
+};
+
+// Host memory the driver copies through staging buffers (not page-locked or registered).
+static bool is_pageable(const void* p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return true;
+    }
+    return a.type == cudaMemoryTypeUnregistered;
+}
+
 static int host_threads(const ctrecon_ctx* ctx) {
     if (ctx->opt_host_threads >= 0) return ctx->opt_host_threads;
     const unsigned hw = std::thread::hardware_concurrency();
     return hw == 0 ? 4 : (int)std::min(16u, hw);
 }
+
+// Uploads proj (FP64 host) and filters it into ctx->ws_c (FP32, device); if fproj_host is not
+// NULL the result also comes down into it (FP64). Returns after enqueueing, except that it
+// waits for the down copies when fproj_host is given. The host stream holds the filter work.
+static Status host_filter_pipeline(ctrecon_ctx* ctx, const ctrecon_filter_params& p,
+                                   const double* proj, double* fproj_host) {
+    FilterPlan* plan = nullptr;
+    CTR_TRY(get_filter_plan(ctx, p, &plan));
+    const int P = p.proj_number;
+    const size_t S = (size_t)p.yl * p.zl, n = S * P;
+    const int threads = host_threads(ctx);
+    if (threads == 0) CTR_TRY(ctx->ws_a.ensure(n * sizeof(double), "FP64 staging"));
+    CTR_TRY(ctx->ws_b.ensure(n * sizeof(float), "projections"));
+    CTR_TRY(ctx->ws_c.ensure(n * sizeof(float), "filtered projections"));
+    // results for a pageable array come down in FP32 and are widened by host threads
+    const bool widen = fproj_host && threads > 0 && is_pageable(fproj_host);
+    if (fproj_host && !widen) CTR_TRY(ctx->ws_d.ensure(n * sizeof(double), "FP64 result staging"));
+    const int nch = (P + kHostChunkViews - 1) / kHostChunkViews;
+    cudaStream_t up = ctx->up_stream, comp = ctx->host_stream, down = ctx->down_stream;
+    HostWidener wid;
+    if (widen) CTR_TRY(wid.start(ctx, ctx->ws_c.as<float>(), fproj_host, S, P, threads, down));
+    // the projections go up converted to FP32 by host threads (slots on the second up stream),
+    // or in FP64 on the up stream, converted on the compute stream (a conversion kernel on the
+    // up stream would wait for SMs behind the filter and stall the copy engine)
+    HostConverter cvt;
+    if (threads > 0) {
+        CTR_TRY(cvt.start(ctx, proj, ctx->ws_b.as<float>(), S, {{0, P}}, threads, ctx->up2_stream));
+    } else {
+        for (int c = 0; c < nch; ++c) {
+            const size_t v0 = (size_t)c * kHostChunkViews, v1 = std::min<size_t>(P, v0 + kHostChunkViews);
+            CTR_CUDA(cudaMemcpyAsync(ctx->ws_a.as<double>() + v0 * S, proj + v0 * S,
+                                     (v1 - v0) * S * sizeof(double), cudaMemcpyHostToDevice, up));
+            cudaEvent_t e = nullptr;
+            CTR_TRY(event_at(ctx, c, &e));
+            CTR_CUDA(cudaEventRecord(e, up));
+        }
+    }
+    int converted = 0;  // chunks [0, converted) are in FP32 once the compute stream gets there
+    for (int c = 0; c < nch; ++c) {
+        const int v0 = c * kHostChunkViews, v1 = std::min(P, v0 + kHostChunkViews);
+        // this chunk and the first view of the next (derivative neighbour)
+        const int need = std::min(c + 1, nch - 1);
+        for (; converted <= need; ++converted) {
+            const size_t w0 = (size_t)converted * kHostChunkViews;
+            const size_t w1 = std::min<size_t>(P, w0 + kHostChunkViews);
+            cudaEvent_t e = nullptr;
+            CTR_TRY(event_at(ctx, converted, &e));
+            if (threads > 0) {
+                CTR_TRY(cvt.issue_upto((int)w1));
+                CTR_CUDA(cudaEventRecord(e, ctx->up2_stream));
+            }
+            CTR_CUDA(cudaStreamWaitEvent(comp, e, 0));
+            if (threads == 0)
+                CTR_TRY(launch_convert_f64_to_f32(comp, ctx->ws_a.as<double>() + w0 * S,
+                                                  ctx->ws_b.as<float>() + w0 * S, (w1 - w0) * S));
+        }
+        CTR_TRY(launch_filter(ctx, comp, *plan, ctx->ws_b.as<float>(), 0, P,
+                              ctx->ws_c.as<float>(), 0, v0, v1));
+        if (widen) {
+            cudaEvent_t done = nullptr;
+            CTR_TRY(event_at(ctx, nch + c, &done));
+            CTR_CUDA(cudaEventRecord(done, comp));
+            CTR_TRY(wid.issue_upto(v1, done));
+        } else if (fproj_host) {
+            const size_t o = (size_t)v0 * S, m = (size_t)(v1 - v0) * S;
+            CTR_TRY(launch_convert_f32_to_f64(comp, ctx->ws_c.as<float>() + o,
+                                              ctx->ws_d.as<double>() + o, m));
+            cudaEvent_t done = nullptr;
+            CTR_TRY(event_at(ctx, nch + c, &done));
+            CTR_CUDA(cudaEventRecord(done, comp));
+            CTR_CUDA(cudaStreamWaitEvent(down, done, 0));
+            CTR_CUDA(cudaMemcpyAsync(fproj_host + o, ctx->ws_d.as<double>() + o,
+                                     m * sizeof(double), cudaMemcpyDeviceToHost, down));
+        }
+    }
+    cvt.stop();
+    if (widen) CTR_TRY(wid.finish());
+    if (fproj_host) {
+        CTR_CUDA(cudaStreamSynchronize(down));
+        CTR_CUDA(cudaStreamSynchronize(comp));
+    }
+    return Status::Ok();
+}
+
+static Status check_filter_bp_shapes(const ctrecon_filter_params& p, const BPGeom& g) {
+    if (p.yl != g.YL || p.zl != g.ZL || p.proj_number != g.ProjNum)
+        return make_status(CTRECON_ERR_INVALID_ARGUMENT,
+                           "filter and backprojection geometries disagree on YL/ZL/views");
+    return Status::Ok();
+}
+
+ctrecon_status ctrecon_filter_host_f64(ctrecon_ctx* ctx, const ctrecon_filter_params* p,
+                                       const double* proj, double* fproj) {
+    if (!ctx) return CTRECON_ERR_INVALID_ARGUMENT;
+    API_BEGIN
+    if (!p || !proj || !fproj)
+        return finish(ctx, make_status(CTRECON_ERR_INVALID_ARGUMENT, "NULL argument"));
+    Status s = use_device(ctx);
+    if (s.ok()) s = host_reset(ctx);
+    if (s.ok()) s = host_filter_pipeline(ctx, *p, proj, fproj);
+    if (s.ok()) s = check_device_flag(ctx);
+    return finish(ctx, s);
+    API_END(ctx)
+}
+
+// KatsevichBkProj with FProj from host memory, with the transfer overlapping the work: the
+// image goes up first, the PI solve runs meanwhile, the valid voxels are zeroed, then the views
+// go up in windows of about 2048 and each window is backprojected (accumulating) as soon as it
+// is resident; the image comes down at the end. Summing per window reorders the FP32 sums of a
+// voxel (the windows' partial sums are added in FP64).
+static Status host_bkproj_windowed(ctrecon_ctx* ctx, BPPlan& plan, const double* fproj,
+                                   double* image) {
+    cudaStream_t up = ctx->up_stream, comp = ctx->host_stream, side = ctx->down_stream;
+    const int P = plan.g.ProjNum;
+    const size_t S = (size_t)plan.g.YL * plan.g.ZL, n = S * P;
+    const size_t nvox = (size_t)plan.kp.NX * plan.kp.NY * plan.kp.NZ;
+    const int threads = host_threads(ctx);
+    if (threads == 0) CTR_TRY(ctx->ws_a.ensure(n * sizeof(double), "FP64 staging"));
+    CTR_TRY(ctx->ws_c.ensure(n * sizeof(float), "filtered projections"));
+    CTR_TRY(ctx->ws_pitab.ensure(nvox * sizeof(PiRecord), "PI table"));
+    CTR_TRY(ctx->ws_e.ensure(nvox * sizeof(double), "FP64 image"));
+    cudaEvent_t pi_done = nullptr, img_up = nullptr;
+    CTR_TRY(event_at(ctx, 0, &pi_done));
+    CTR_TRY(event_at(ctx, 1, &img_up));
+    CTR_TRY(launch_pi(ctx, side, plan, ctx->ws_pitab.as<PiRecord>(), nullptr));
+    CTR_CUDA(cudaEventRecord(pi_done, side));
+    CTR_CUDA(cudaMemcpyAsync(ctx->ws_e.ptr, image, nvox * sizeof(double), cudaMemcpyHostToDevice, up));
+    CTR_CUDA(cudaEventRecord(img_up, up));
+    // the views go up converted to FP32 by host threads (slots on the second up stream), or
+    // in FP64, converted per window on the compute stream
+    HostConverter cvt;
+    if (threads > 0)
+        CTR_TRY(cvt.start(ctx, fproj, ctx->ws_c.as<float>(), S, {{0, P}}, threads, ctx->up2_stream));
+    CTR_CUDA(cudaStreamWaitEvent(comp, pi_done, 0));
+    CTR_CUDA(cudaStreamWaitEvent(comp, img_up, 0));
+    CTR_TRY(launch_zero_valid_f64(comp, ctx->ws_pitab.as<PiRecord>(), ctx->ws_e.as<double>(), nvox));
+    // windows: whole upload chunks, about 2048 views each
+    const int per_win = std::max(kHostChunkViews, (2048 / kHostChunkViews) * kHostChunkViews);
+    const BPParams saved = plan.kp;
+    Status st;
+    int w = 0;
+    for (int v0 = 0; st.ok() && v0 < P; v0 += per_win, ++w) {
+        const int v1 = std::min(P, v0 + per_win);
+        for (int c0 = v0; st.ok() && threads == 0 && c0 < v1; c0 += kHostChunkViews) {
+            const size_t m = (size_t)(std::min(v1, c0 + kHostChunkViews) - c0) * S;
+            cudaError_t e = cudaMemcpyAsync(ctx->ws_a.as<double>() + (size_t)c0 * S,
+                                            fproj + (size_t)c0 * S, m * sizeof(double),
+                                            cudaMemcpyHostToDevice, up);
+            if (e != cudaSuccess) st = cuda_status(e, "FProj upload");
+        }
+        if (st.ok() && threads > 0) st = cvt.issue_upto(v1);
+        cudaEvent_t ev = nullptr;
+        if (st.ok()) st = event_at(ctx, 2 + (size_t)w, &ev);
+        if (st.ok()) {
+            cudaError_t e = cudaEventRecord(ev, threads > 0 ? ctx->up2_stream : up);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(comp, ev, 0);
+            if (e != cudaSuccess) st = cuda_status(e, "window event");
+        }
+        // the window's conversion on the compute stream (copies only on the up stream: a
+        // kernel there would wait for SMs behind the backprojection and stall the copy engine)
+        if (st.ok() && threads == 0)
+            st = launch_convert_f64_to_f32(comp, ctx->ws_a.as<double>() + (size_t)v0 * S,
+                                           ctx->ws_c.as<float>() + (size_t)v0 * S,
+                                           (size_t)(v1 - v0) * S);
+        if (st.ok()) {
+            plan.kp.win0 = v0;
+            plan.kp.win1 = v1 - 1;
+            plan.kp.accum = 1;
+            st = launch_bkproj_f64out(ctx, comp, plan, ctx->ws_c.as<float>(),
+                                      ctx->ws_pitab.as<PiRecord>(), ctx->ws_e.as<double>());
+            plan.kp = saved;
+        }
+    }
+    plan.kp = saved;
+    cvt.stop();
+    CTR_TRY(st);
+    CTR_CUDA(cudaMemcpyAsync(image, ctx->ws_e.ptr, nvox * sizeof(double), cudaMemcpyDeviceToHost, comp));
+    CTR_CUDA(cudaStreamSynchronize(comp));
+    CTR_CUDA(cudaStreamSynchronize(side));
+    CTR_CUDA(cudaStreamSynchronize(up));
+    CTR_CUDA(cudaStreamSynchronize(ctx->up2_stream));
+    return check_device_flag(ctx);
+}
+
+ctrecon_status ctrecon_bkproj_host_f64(ctrecon_ctx* ctx, const ctrecon_bp_geom* g,
+                                       const double* fproj, double* image) {
+    if (!ctx) return CTRECON_ERR_INVALID_ARGUMENT;
+    API_BEGIN
+    if (!g || !fproj || !image)
+        return finish(ctx, make_status(CTRECON_ERR_INVALID_ARGUMENT, "NULL argument"));
+    Status s = use_device(ctx);
+    BPPlan* plan = nullptr;
+    if (s.ok()) s = get_bp_plan(ctx, *g, &plan);
+    if (s.ok()) s = host_reset(ctx);
+    if (s.ok()) s = host_bkproj_windowed(ctx, *plan, fproj, image);
+    return finish(ctx, s);
+    API_END(ctx)
+}
+
+// The whole chain with FP64 host buffers (FunctionKat_v6.m:85-113 without the FProj round
+// trip), pipelined so that the host copies hide the work: the image goes up first and the PI
+// solve runs beside the uploads; the projections go up in chunks, each chunk is converted and
+// filtered as soon as it and its neighbour view are resident, and each window of about 2048
+// views is backprojected (accumulating into the zeroed valid voxels) as soon as its views are
+// filtered, while later chunks are still on their way; the image comes down at the end.
 
 static Status host_recon_pipeline(ctrecon_ctx* ctx, const ctrecon_filter_params& p, BPPlan& plan,
                                   const double* proj, double* image) {

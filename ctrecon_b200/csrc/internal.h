@@ -271,7 +271,8 @@ struct ctrecon_ctx {
     ctr::DevBuf ws_count;    // update counter
     ctr::DevBuf ws_a, ws_b, ws_c, ws_d;  // host-call staging (f64 in, f32, f32 out, f64 out)
     ctr::DevBuf ws_e;        // FP64 image of the host backprojection
-    ctr::PinnedBuf pin_ring; // FP32 projection slots of the one-call path's host conversion
+    ctr::PinnedBuf pin_ring; // FP32 slots of the host calls' input conversion
+    ctr::PinnedBuf pin_ring_down;  // FP32 slots of the results widened on the host
     ctr::DevBuf ws_panel;    // arc-to-flat rebin table
     ctr::DevBuf ws_dual;     // second filter result of FilteringMode 1
     ctr::DevBuf ws_ell;      // phantom ellipsoids

@@ -3,7 +3,7 @@
 * Several scan geometries used one after the other on one context, on a non-blocking stream
   and without host synchronisation in between, must give exactly the images that separate
   contexts give: a geometry change must never touch tables that queued kernels still read.
-* The host (MEX-equivalent) calls pipeline their copies on three streams; with pinned host
+* The host (MEX-equivalent) calls pipeline their copies on their own streams; with pinned host
   buffers the copies overlap the kernels, with pageable ones they do not. Both must give the
   same bits. The host backprojection accumulates view windows as they arrive: equal to the
   one-pass backprojection up to the order of the FP32 sums.
@@ -112,10 +112,13 @@ def test_host_calls_pinned_equal_pageable(torch_mod):
 
 @pytest.mark.parametrize("cfg", ["c1", "tiny"])
 def test_recon_host_conversion_forms_equal(torch_mod, cfg):
-    """ctrecon_recon_host_f64 converts the FP64 projections to FP32 either with host threads
+    """The host calls convert their FP64 inputs to FP32 either with host threads
     (CTRECON_OPT_HOST_THREADS > 0, default: slots of 64 views copied up as they are converted)
-    or on the device (0); the casts round alike, so the image is the same bit for bit, for
-    thread counts that do and do not divide a slot, pinned and pageable, on repeated calls."""
+    or on the device (0), and the filter's results for a pageable array come down in FP32 and
+    are widened by host threads; the casts round alike and widening is exact, so
+    ctrecon_recon_host_f64's image, ctrecon_filter_host_f64's FProj and ctrecon_bkproj_host_f64's
+    image are the same bit for bit, for thread counts that do and do not divide a slot, pinned
+    and pageable arrays, on repeated calls."""
     torch = torch_mod
     import ctrecon_b200 as ct
     from ctrecon_b200 import _lib
@@ -129,7 +132,8 @@ def test_recon_host_conversion_forms_equal(torch_mod, cfg):
         proj = d.cpu().numpy().astype(np.float64)
         proj_pin = torch.from_numpy(proj).pin_memory().numpy()
         p = ct.scan_filter_params(s)
-        out = {}
+        out, fout, bout = {}, {}, {}
+        f_pin = torch.empty(proj.shape, dtype=torch.float64).pin_memory().numpy()
         for th in (0, -1, 1, 3, 7, 16):
             cx.set_option(_lib.OPT_HOST_THREADS, th)
             assert cx.get_option(_lib.OPT_HOST_THREADS) == th
@@ -139,8 +143,20 @@ def test_recon_host_conversion_forms_equal(torch_mod, cfg):
                     cx.recon_host(p, s.geom_struct(), src, img)
                     out.setdefault(th, img)
                     assert np.array_equal(img, out[th]), th
+            for f in (np.empty_like(proj), f_pin):
+                for _ in range(2):
+                    f[...] = -1.0
+                    cx.filter_host(p, proj_pin if f is f_pin else proj, f)
+                    fout.setdefault(th, f.copy())
+                    assert np.array_equal(f, fout[th]), th
+                    img = np.full(s.vol_shape, 7.25)
+                    cx.bkproj_host(s.geom_struct(), f, img)
+                    bout.setdefault(th, img)
+                    assert np.array_equal(img, bout[th]), th
         for th in out:
             assert np.array_equal(out[th], out[0]), th
+            assert np.array_equal(fout[th], fout[0]), th
+            assert np.array_equal(bout[th], bout[0]), th
         with pytest.raises(_lib.CtreconError):
             cx.set_option(_lib.OPT_HOST_THREADS, -2)
 
