@@ -1277,8 +1277,11 @@ def run_headline(args):
             ctx.filter_host(fpar, np_proj, np_fproj)       # KatsevichFiltering_GPU
             ctx.bkproj_host(geom, np_fproj, np_img)        # KatsevichBkProj_GPU
         t_mex = max_over_ranks((time.perf_counter() - t0) / e2e_steps, ws)
+        # inputs cross as FP32 when host threads convert them; the pinned FProj comes down
+        # in FP64
+        in_b = 4 if host_threads > 0 else 8
         e2e_mex = {"value": ws * updates / t_mex / 1e9, "unit": "GUPS",
-                   "h2d_bytes_per_step": 8 * (2 * nproj + nvox),
+                   "h2d_bytes_per_step": 2 * in_b * nproj + 8 * nvox,
                    "d2h_bytes_per_step": 8 * (nproj + nvox), "s_per_vol": t_mex,
                    "steps": e2e_steps,
                    "path": "ctrecon_filter_host_f64 + ctrecon_bkproj_host_f64 (the two MEX "
@@ -1308,9 +1311,10 @@ def run_headline(args):
         for _ in range(pg_steps):
             mex_step()
         t_pg = max_over_ranks((time.perf_counter() - t0) / pg_steps, ws)
+        # the pageable FProj comes down in FP32 and is widened by host threads
         e2e_pageable = {"value": ws * updates / t_pg / 1e9, "unit": "GUPS",
-                        "h2d_bytes_per_step": 8 * (2 * nproj + nvox),
-                        "d2h_bytes_per_step": 8 * (nproj + nvox), "s_per_vol": t_pg,
+                        "h2d_bytes_per_step": 2 * in_b * nproj + 8 * nvox,
+                        "d2h_bytes_per_step": in_b * nproj + 8 * nvox, "s_per_vol": t_pg,
                         "steps": pg_steps,
                         "path": "KatsevichFiltering_GPU + KatsevichBkProj_GPU MEX modules "
                                 "(mex.h shim), pageable FP64 arrays"}

@@ -143,13 +143,14 @@ typedef enum ctrecon_option {
                                          ctrecon_kernel_times); default 0 */
     CTRECON_OPT_TC_FORM = 10,         /* form of the tensor-core Hilbert: CTRECON_TC_* below */
     CTRECON_OPT_K1_FORM = 11,         /* form of the derivative + forward rebin: CTRECON_K1_* */
-    CTRECON_OPT_HOST_THREADS = 12     /* host threads with which ctrecon_recon_host_f64 converts
-                                         the FP64 projections to FP32 before they cross to the
+    CTRECON_OPT_HOST_THREADS = 12     /* host threads with which the host (FP64) calls convert
+                                         their input views to FP32 before they cross to the
                                          device (half the bytes over the host link), each slot of
-                                         views copied up as soon as it is converted; 0: copy the
-                                         FP64 views and convert them on the device; default -1:
-                                         as many as the host has, at most 16. The result is the
-                                         same bit for bit. */
+                                         views copied up as soon as it is converted, and widen
+                                         ctrecon_filter_host_f64's FP32 results on the host when
+                                         FProj is pageable; 0: copy FP64 and convert on the
+                                         device; default -1: as many as the host has, at most
+                                         16. The results are the same bit for bit. */
 } ctrecon_option;
 
 /* CTRECON_OPT_TC_FORM. Both forms compute the same sums to FP32 rounding. */
