@@ -32,6 +32,27 @@ def test_library_exports_every_declared_symbol():
     assert set(syms) <= bound, set(syms) - bound
 
 
+def header_enum_values():
+    """Every `CTRECON_NAME = value` enumerator of include/ctrecon.h."""
+    txt = open(os.path.join(ROOT, "include", "ctrecon.h")).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return {m.group(1): int(m.group(2))
+            for m in re.finditer(r"\bCTRECON_([A-Z0-9_]+)\s*=\s*(-?\d+)\b", txt)}
+
+
+def test_python_option_constants_match_header():
+    """The ctypes mirror's option numbers and option values are the header's, so an option
+    added on one side only is caught here."""
+    h = header_enum_values()
+    opts = {k: v for k, v in h.items() if k.startswith("OPT_")}
+    assert len(opts) >= 12
+    for name, value in opts.items():
+        assert getattr(_lib, name) == value, name
+    for name in ("HILBERT_FP32", "HILBERT_BF16X3", "HILBERT_TF32", "PI_BISECT", "PI_NEWTON",
+                 "PI_LEARNED", "TC_PARITY_SPLIT", "TC_SINGLE_PASS", "K1_STAGED", "K1_PER_VIEW"):
+        assert getattr(_lib, name) == h[name], name
+
+
 def test_abi_version_and_status_strings():
     L = _lib.lib()
     assert L.ctrecon_abi_version() == 1
