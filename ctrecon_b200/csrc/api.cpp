@@ -1,6 +1,7 @@
 // api.cpp -- the C ABI of include/ctrecon.h: contexts, plan caching and the host (FP64,
 // MEX-equivalent) and device (FP32) entry points.
 #include "internal.h"
+#include "host_convert.h"
 
 #include <algorithm>
 #include <atomic>
@@ -14,9 +15,6 @@
 #include <thread>
 #include <vector>
 
-#if defined(__SSE2__)
-#include <emmintrin.h>
-#endif
 
 namespace ctr {
 
@@ -726,25 +724,6 @@ static Status event_at(ctrecon_ctx* ctx, size_t i, cudaEvent_t* out) {
 constexpr int kSlotViews = 64;
 constexpr int kRingSlots = 8;
 
-// dst[i] = (float)src[i], the FP32 results written around the caches (they only go on to
-// the device): no read for ownership of the slot lines, a quarter less memory traffic. The
-// SSE2 conversion rounds to nearest even, as the cast does.
-static void convert_stream(const double* src, float* dst, size_t n) {
-#if defined(__SSE2__)
-    size_t i = 0;
-    for (; i < n && ((uintptr_t)(dst + i) & 15u) != 0; ++i) dst[i] = (float)src[i];
-    for (; i + 4 <= n; i += 4) {
-        const __m128 lo = _mm_cvtpd_ps(_mm_loadu_pd(src + i));
-        const __m128 hi = _mm_cvtpd_ps(_mm_loadu_pd(src + i + 2));
-        _mm_stream_ps(dst + i, _mm_movelh_ps(lo, hi));
-    }
-    for (; i < n; ++i) dst[i] = (float)src[i];
-    _mm_sfence();  // the streamed stores are visible before the slot is handed to the copy
-#else
-    for (size_t i = 0; i < n; ++i) dst[i] = (float)src[i];
-#endif
-}
-
 class HostConverter {
 public:
     ~HostConverter() { stop(); }
@@ -867,24 +846,6 @@ private:
     bool stopping_ = false, failed_ = false;
     std::string why_;
 };
-
-// dst[i] = (double)src[i] (exact), the FP64 results written around the caches.
-static void widen_stream(const float* src, double* dst, size_t n) {
-#if defined(__SSE2__)
-    size_t i = 0;
-    if (((uintptr_t)dst & 7u) == 0) {
-        for (; i < n && ((uintptr_t)(dst + i) & 15u) != 0; ++i) dst[i] = (double)src[i];
-        for (; i + 2 <= n; i += 2) {
-            const __m128 f = _mm_castpd_ps(_mm_load_sd(reinterpret_cast<const double*>(src + i)));
-            _mm_stream_pd(dst + i, _mm_cvtps_pd(f));
-        }
-    }
-    for (; i < n; ++i) dst[i] = (double)src[i];
-    _mm_sfence();
-#else
-    for (size_t i = 0; i < n; ++i) dst[i] = (double)src[i];
-#endif
-}
 
 // The reverse of HostConverter, for results going to pageable host arrays: each slot of
 // kSlotViews FP32 views comes down from the device into a ring of kRingSlots page-locked slots
