@@ -120,7 +120,7 @@ __device__ __forceinline__ void pi_newton(double x, double y, double z, double s
 // error there is ~1e-12, far below the bisection's 1e-7). The chord is evaluated exactly -- the
 // same pi_chord call as the bisection's -- only where either decision lies within 1e-10 of its
 // threshold, and once at the final midpoint for st. The midpoints are the bisection's own
-// arithmetic, so (sb, st) equal pi_bisect's bit for bit: the bisection remains the judge of the
+// arithmetic, so (sb, st) equal pi_bisect's bit for bit: the bisection still decides the
 // endpoints, Newton only finds where it will end. Returns the chord evaluations made (~1).
 __device__ __forceinline__ int pi_bisect_replay(double x, double y, double z, double tau,
                                                 double dz, double* B, double* T) {
